@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""Benchmark: grid-point updates per second of the FP64 Teukolsky step.
+
+Workload (the configuration the headline metric is quoted on): FP64
+plunge-driven ringdown, s=-2, m=2, a=0.9, M=1, r* (grid coordinate) in
+[-200, 600] with N_r=8192, N_theta=128, dt = 0.25 min(dx, r_min dtheta),
+source from a prograde equatorial plunge worldline sampled at dt/2 (a
+seeded synthetic stand-in for GenOT output: no GenOT inputs exist here).
+
+A step is one full time step (source patch, three SSP-RK3 stages,
+extraction) over the whole grid.  The solver's working set (three states
+of 32 MB plus tables) fits in the 126 MB L2, so L2 is flushed by writing a
+256 MB buffer between timed steps; each step is timed with CUDA events on
+the solver's stream and the per-kernel durations are summed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N>1 (torchrun, one process per GPU) every rank advances its own
+independent solve (replicas: solves share nothing), timing is the max over
+ranks and value is the sum of all ranks' updates over that time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "grid-pt updates/s (%HBM roofline); solves/s, p99 latency vs FP64 plain @1e-6"
+UNIT = "grid-pt updates/s"
+WORKLOADS = {
+    # the headline configuration: plunge-driven ringdown, 8192 x 128
+    "plunge": dict(N=8192, M=128, Xmin=-200.0, Xmax=600.0, a=0.9, m=2.0, T=1000.0, courant=0.25),
+    # the size the HBM-roofline target is quoted at (16384 x 256), source-free
+    "grid16k": dict(N=16384, M=256, Xmin=-200.0, Xmax=600.0, a=0.9, m=2.0, T=1000.0, courant=0.25),
+}
+WORKLOAD = WORKLOADS["plunge"]
+BYTES_PER_PT = 256.0  # FP64 SSP-RK3 algorithmic bytes per point per step (coefficients recomputed)
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per stage-kernel launch per grid point from the committed
+    ncu summary, if there is one (profiles/stage_kernel_plunge8192x128.txt,
+    line 'dram_bytes_per_point_per_step: X')."""
+    path = os.path.join(ROOT, "profiles", "stage_kernel_plunge8192x128.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_point_per_step:"):
+                return float(line.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"bhr_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=clocks.sm,clocks.max.sm,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None:
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 6:
+                    continue
+                try:
+                    sm.append(float(parts[0]))
+                    mx.append(float(parts[1]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[2:6]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            os.remove(self.path)
+        except Exception:
+            return None
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def source_available():
+    import bh_ringdown_b200 as bhr
+    try:
+        bhr.source_coefficients(bhr.Particle(rp=6.0, tp=np.pi / 2, E=0.9, lz=3.0), 0.5, 1.0, 2.0)
+        return True
+    except bhr.BhrError:
+        return False
+
+
+def make_params(device=0, dt=None):
+    import bh_ringdown_b200 as bhr
+    w = WORKLOAD
+    return bhr.Params(N=w["N"], M=w["M"], Xmin=w["Xmin"], Xmax=w["Xmax"], a=w["a"], m=w["m"], T=w["T"],
+                      dt=0.0 if dt is None else dt, courant=w["courant"], Fr=50, out_start=0.0, device=device,
+                      init_kind=bhr.BHR_INIT_ZERO)
+
+
+def workload_inputs(with_source, device=0):
+    """(params, trajectory rows or None).  Without a source the run starts
+    from a Gaussian pulse instead (psi = exp(-(x-20)^2/8) swsh(2,2))."""
+    import bh_ringdown_b200 as bhr
+    from bh_ringdown_b200.trajectory import synthetic_plunge
+    prm = make_params(device)
+    x, r, th = bhr.grid(prm)
+    dx = (prm.Xmax - prm.Xmin) / prm.N
+    dt = prm.courant * min(dx, r[0] * np.pi / prm.M)
+    prm.dt = dt
+    if with_source:
+        rows = synthetic_plunge(prm.a, dt / 2.0, duration=60.0)
+        return prm, rows
+    prm.init_kind = bhr.BHR_INIT_GAUSSIAN
+    prm.init_center, prm.init_width, prm.init_ell = 20.0, 2.0, 2.0
+    return prm, None
+
+
+def run_ours(args, rank, local_rank, world):
+    import torch
+    import bh_ringdown_b200 as bhr
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    with_source = source_available() and args.workload == "plunge"
+    prm, rows = workload_inputs(with_source, device=local_rank)
+    N, M = prm.N, prm.M
+    solver = bhr.Solver(prm)
+    if rows is not None:
+        solver.set_trajectory(rows)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def one_step():
+        flush.zero_()
+        torch.cuda.synchronize()
+        avg, tot = solver.profile(1)
+        return avg, tot
+
+    for _ in range(args.warmup):
+        one_step()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    per_kernel = np.zeros(5)
+    total_ms = 0.0
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            avg, tot = one_step()
+            per_kernel += avg
+            total_ms += tot
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    clocks = clk.summary()
+    solver.close()
+
+    value = world * N * M * args.steps / (total_ms / 1e3)
+    ms_per_step = total_ms / args.steps
+    stage_ms = per_kernel[1:4] / args.steps
+    peak, peak_kind = measured_peak()
+    achieved = BYTES_PER_PT * N * M / (float(stage_ms.sum()) / 1e3) / 1e9
+    traffic_pp = profile_traffic()
+
+    # End to end through the public API: host params + host trajectory in,
+    # solver set-up (grid, tables, initial data uploaded), n steps, waveform
+    # rows copied back, solver destroyed; wall clock.
+    n_e2e = args.e2e_steps
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s2 = bhr.Solver(prm)
+    if rows is not None:
+        s2.set_trajectory(rows)
+    s2.step(n_e2e)
+    tw, hw, ew = s2.waveform()
+    info = s2.info()
+    s2.close()
+    t_e2e = time.perf_counter() - t0
+    h2d = 4 * N * M * 8 + (13 * N + 4 * M + N + M + 8 * M) * 8 + (0 if rows is None else info["nt"] * 160)
+    d2h = len(tw) * 16 * 8
+    e2e = {"value": N * M * n_e2e / t_e2e * world, "unit": UNIT, "h2d_bytes_per_step": int(h2d / n_e2e),
+           "d2h_bytes_per_step": int(d2h / n_e2e), "steps": n_e2e,
+           "note": "wall clock of create + trajectory upload + steps + waveform readback + destroy"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(prm, rows, args.cpu_seconds)
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: FP64 s=-2 m=2 a=0.9, {N}x{M} on [-200,600]"
+                                   + (", plunge source" if with_source else ", source-free (Gaussian pulse initial data)"),
+                       "N_r": N, "N_theta": M, "dt": prm.dt, "integrator": "SSP-RK3",
+                       "source": "synthetic prograde equatorial plunge from ISCO" if with_source else "none",
+                       "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": None if traffic_pp is None else traffic_pp * N * M,
+                         "kernel": "stage_kernel<1,2,3> (one SSP-RK3 step, 256 B/pt algorithmic)"},
+            "kernel_ms": {"source": per_kernel[0] / args.steps, "stage1": stage_ms[0], "stage2": stage_ms[1],
+                          "stage3": stage_ms[2], "extract": per_kernel[4] / args.steps},
+            "gpu_launches": args.steps * (5 if with_source else 4),
+            "e2e": e2e,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(prm, rows, seconds):
+    """The FP64 oracle on this host's cores, a bounded sample of the same
+    workload (steps of the full grid until about `seconds` elapse)."""
+    from oracle import pyoracle
+    import bh_ringdown_b200 as bhr
+    o = pyoracle.Oracle(prm.N, prm.M, prm.Xmin, prm.Xmax, prm.a, prm.m, prm.dt, T=prm.T, Fr=50, out_start=0.0)
+    coef = None
+    if rows is None:
+        o.init_gaussian(prm.init_center, prm.init_width, prm.init_ell)
+    else:
+        lib = bhr.load_library()
+
+        def _coef(pt, a, mass, m, cr, ci):
+            p = bhr.Particle(*[getattr(pt.contents, n) for n, _ in pyoracle.OrcParticle._fields_])
+            import ctypes
+            lib.bhr_source_coefficients(ctypes.byref(p), a, mass, m, cr, ci)
+        coef = pyoracle.COEF_FN(_coef)
+    t0 = time.perf_counter()
+    n = 0
+    chunk = 5
+    while time.perf_counter() - t0 < seconds:
+        if rows is None:
+            o.step(chunk)
+        else:
+            o.run(traj=rows, coef_fn=coef, nsteps=chunk, max_rows=10)
+        n += chunk
+    el = time.perf_counter() - t0
+    return {"value": prm.N * prm.M * n / el, "unit": UNIT, "cores": pyoracle.num_threads(), "kind": "port",
+            "sample": f"{n} steps of the full {prm.M}x{prm.N} grid in {el:.1f} s (FP64 oracle, OpenMP over theta rows)"}
+
+
+def run_reference(args, rank, world):
+    """The reference's own HighOrder kernels compiled for and run on this
+    host's cores (oracle/_ref/libref_cfg2.so), on the same workload."""
+    if rank != 0:
+        return
+    import ctypes as C
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libref_cfg2.so")
+    if not os.path.exists(lib_path):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_cfg2.so was not built "
+                                                               "(the reference tree was absent at build time)"}))
+        return
+    from oracle import pyoracle
+    D = C.c_double
+    L = C.CDLL(lib_path)
+    L.ref_source.argtypes = [D] * 16
+    N, M = L.ref_N(), L.ref_M()
+    w = WORKLOAD
+    o = pyoracle.Oracle(N, M, w["Xmin"], w["Xmax"], w["a"], w["m"], 0.01)
+    x, r, th = o.grid()  # the reference's grid() with its NaN radii floored at r+
+    o.close()
+    dx = (w["Xmax"] - w["Xmin"]) / N
+    dt = w["courant"] * min(dx, r[0] * np.pi / M)
+    L.ref_init(D(1.0), D(w["a"]), D(w["m"]), D(dt), th.ctypes.data_as(C.c_void_p), r.ctypes.data_as(C.c_void_p))
+    from bh_ringdown_b200.trajectory import synthetic_plunge
+    rows = synthetic_plunge(w["a"], dt / 2.0, duration=60.0)
+    er, ei = np.zeros(M), np.zeros(M)
+
+    # body.cu:97-124 consumption of the trajectory rows, restated.
+    cur = [2]
+    state = {"rp": rows[1, 1], "t11": 0.0, "t22": 0.0, "t33": 0.0, "row": rows[1]}
+
+    def one_step(k, timer):
+        for _ in range(2):
+            if cur[0] < len(rows):
+                state["row"] = rows[cur[0]]
+                state["rp"] = state["row"][1]
+                cur[0] += 1
+        row = state["row"]
+        state["rp"] += 1e-6
+        L.ref_source(D(0.0), D(timer), D(state["rp"]), D(row[6]), D(row[2]), D(row[7]), D(row[8]), D(row[9]),
+                     D(row[3]), D((row[3] - state["t11"]) / dt), D(0.0), D(row[4]), D((row[4] - state["t22"]) / dt),
+                     D(0.0), D(row[5]), D((row[5] - state["t33"]) / dt))
+        state["t11"], state["t22"], state["t33"] = row[3], row[4], row[5]
+        L.ref_step(er.ctypes.data_as(C.c_void_p), ei.ctypes.data_as(C.c_void_p))
+
+    timer = 0.0
+    for k in range(args.warmup):
+        one_step(k, timer)
+        timer += dt
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        one_step(args.warmup + k, timer)
+        timer += dt
+    el = time.perf_counter() - t0
+    value = N * M * args.steps / el
+    threads = os.cpu_count()
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "plunge-driven ringdown FP64, s=-2 m=2 a=0.9, 8192x128 on [-200,600]",
+                      "N_r": N, "N_theta": M, "dt": dt, "integrator": "SSP-RK3",
+                      "source": "synthetic prograde equatorial plunge from ISCO (reference Maple source)"},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                            "sample": f"{args.steps} full steps (reference sourced + 12 step kernels, "
+                                      f"HighOrder/body.cu:108-165 order) on the {M}x{N} grid, host cores"},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=2000)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="plunge")
+    args = ap.parse_args()
+    global WORKLOAD
+    WORKLOAD = WORKLOADS[args.workload]
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, local_rank, world = env_rank()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, local_rank, world)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,265 @@
+"""bh_ringdown_b200: B200-native time-domain Teukolsky solver (Python host mirror).
+
+The compute path is the C ABI of ``include/bhr.h`` implemented in
+``bh_ringdown_b200/libbhr.so`` (sm_100a CUDA kernels plus C++ host code).
+This module binds that library with ctypes and mirrors the reference
+driver surface: the run knobs of TD_GPU_code/HighOrder/parm.h and main.c,
+the .traj trajectory input and the hm*.dat waveform output of body.cu.
+
+There is no fallback: if the library is missing or fails to load, every
+call raises.  Build it with ``python __graft_entry__.py`` or
+``make -C bh_ringdown_b200/csrc``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field, fields
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbhr.so")
+
+D = C.c_double
+I = C.c_int
+
+BHR_OK = 0
+STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OUT_OF_MEMORY", 3: "CUDA_ERROR", 4: "NAN_DETECTED",
+                5: "TIMEOUT", 6: "IO_ERROR", 7: "NO_DEVICE"}
+
+BHR_SSPRK3 = 0
+BHR_FP64, BHR_MIXED = 0, 1
+BHR_INIT_ZERO, BHR_INIT_GAUSSIAN = 0, 1
+
+
+class BhrError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class _Params(C.Structure):
+    _fields_ = [("N", I), ("M", I), ("Xmin", D), ("Xmax", D), ("mass", D), ("a", D), ("m", D), ("dt", D),
+                ("courant", D), ("out_every", D), ("T", D), ("Fr", I), ("out_start", D), ("ext_col", I),
+                ("PTSX", I), ("PTSY", I), ("wr_fac", D), ("wt_fac", D), ("integrator", I), ("precision", I),
+                ("init_kind", I), ("init_center", D), ("init_width", D), ("init_ell", D), ("device", I)]
+
+
+class Particle(C.Structure):
+    """One particle state as HighOrder/body.cu:112-124 hands it to sourced()."""
+    _fields_ = [(n, D) for n in ("rp", "tp", "phip", "E", "lz", "Q", "drdt", "d2rdt2", "d3rdt3", "dthdt",
+                                 "d2thdt2", "d3thdt3", "dphidt", "d2phidt2")]
+
+
+class _Info(C.Structure):
+    _fields_ = [("N", I), ("M", I), ("dx", D), ("dtheta", D), ("dt", D), ("nt", I), ("Fr", I),
+                ("steps_done", I), ("rows_done", I), ("has_source", I), ("r_plus", D), ("device_bytes", C.c_size_t)]
+
+
+@dataclass
+class Params:
+    """Run parameters; defaults are the reference's (HighOrder/parm.h, main.c)."""
+    N: int = 16000
+    M: int = 256
+    Xmin: float = -50.0
+    Xmax: float = 50.0
+    mass: float = 1.0
+    a: float = 1e-8
+    m: float = 2.0
+    dt: float = 0.002
+    courant: float = 0.25
+    out_every: float = 0.0
+    T: float = 1500.0
+    Fr: int = 50
+    out_start: Optional[float] = None  # None -> Xmax + 200 (HighOrder/body.cu:207)
+    ext_col: int = -1
+    PTSX: int = 128
+    PTSY: int = 128
+    wr_fac: float = 2.0
+    wt_fac: float = 6.0
+    integrator: int = BHR_SSPRK3
+    precision: int = BHR_FP64
+    init_kind: int = BHR_INIT_ZERO
+    init_center: float = 20.0
+    init_width: float = 2.0
+    init_ell: float = 2.0
+    device: int = 0
+
+    def to_c(self) -> _Params:
+        p = _Params()
+        for f in fields(self):
+            v = getattr(self, f.name)
+            if f.name == "out_start" and v is None:
+                v = self.Xmax + 200.0
+            setattr(p, f.name, v)
+        return p
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Load libbhr.so (raises if it is missing: there is no CPU fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} not built; run `python __graft_entry__.py` or `make -C bh_ringdown_b200/csrc`")
+    lib = C.CDLL(path)
+    P = C.POINTER
+    vp = C.c_void_p
+    dp = P(D)
+    sigs = {
+        "bhr_abi_version": (I, []),
+        "bhr_last_error_string": (C.c_char_p, []),
+        "bhr_params_default": (I, [P(_Params)]),
+        "bhr_grid": (I, [P(_Params), dp, dp, dp]),
+        "bhr_solver_create": (I, [P(_Params), P(vp)]),
+        "bhr_solver_destroy": (None, [vp]),
+        "bhr_solver_info": (I, [vp, P(_Info)]),
+        "bhr_solver_set_trajectory": (I, [vp, dp, I]),
+        "bhr_solver_load_trajectory": (I, [vp, C.c_char_p]),
+        "bhr_solver_step": (I, [vp, I]),
+        "bhr_solver_run": (I, [vp, C.c_char_p, C.c_char_p]),
+        "bhr_solver_waveform": (I, [vp, dp, dp, dp, I, P(I)]),
+        "bhr_solver_get_state": (I, [vp, dp, dp, dp, dp]),
+        "bhr_solver_set_state": (I, [vp, dp, dp, dp, dp]),
+        "bhr_solver_get_extraction": (I, [vp, dp, dp, dp, dp, dp, dp]),
+        "bhr_solver_get_source": (I, [vp, dp, dp]),
+        "bhr_solver_stream": (vp, [vp]),
+        "bhr_solver_profile": (I, [vp, I, dp, dp]),
+        "bhr_source_coefficients": (I, [P(Particle), D, D, D, dp, dp]),
+        "bhr_swsh": (D, [D, D, D]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(D))
+
+
+def _check(st: int):
+    if st != BHR_OK:
+        raise BhrError(st, load_library().bhr_last_error_string().decode(errors="replace"))
+
+
+def grid(params: Params):
+    """x_c[N], r_c[N], theta[M] of HighOrder/main.c:79-198."""
+    lib = load_library()
+    x, r, t = np.zeros(params.N), np.zeros(params.N), np.zeros(params.M)
+    p = params.to_c()
+    _check(lib.bhr_grid(C.byref(p), _ptr(x), _ptr(r), _ptr(t)))
+    return x, r, t
+
+
+def swsh(ell: float, m: float, theta: float) -> float:
+    return load_library().bhr_swsh(ell, m, theta)
+
+
+def source_coefficients(pt: Particle, a: float, mass: float, m: float):
+    """Six complex coefficients of DelR^(i) DelTH^(j), (i,j) in
+    (0,0) (0,1) (0,2) (1,0) (1,1) (2,0)."""
+    lib = load_library()
+    cr, ci = np.zeros(6), np.zeros(6)
+    _check(lib.bhr_source_coefficients(C.byref(pt), a, mass, m, _ptr(cr), _ptr(ci)))
+    return cr + 1j * ci
+
+
+class Solver:
+    """One solve on one device (replaces HighOrder/body.cu:body())."""
+
+    def __init__(self, params: Params):
+        self.lib = load_library()
+        self.params = params
+        self._p = params.to_c()
+        h = C.c_void_p()
+        _check(self.lib.bhr_solver_create(C.byref(self._p), C.byref(h)))
+        self._h = h
+        self.N, self.M = params.N, params.M
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.bhr_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def info(self) -> dict:
+        inf = _Info()
+        _check(self.lib.bhr_solver_info(self._h, C.byref(inf)))
+        return {f[0]: getattr(inf, f[0]) for f in _Info._fields_}
+
+    def set_trajectory(self, rows: np.ndarray):
+        rows = np.ascontiguousarray(rows, dtype=np.float64)
+        assert rows.ndim == 2 and rows.shape[1] == 10
+        _check(self.lib.bhr_solver_set_trajectory(self._h, _ptr(rows), rows.shape[0]))
+
+    def load_trajectory(self, path: str):
+        _check(self.lib.bhr_solver_load_trajectory(self._h, path.encode()))
+
+    def step(self, nsteps: int = 1):
+        _check(self.lib.bhr_solver_step(self._h, int(nsteps)))
+
+    def run(self, out_dir: Optional[str] = None, name: Optional[str] = None):
+        _check(self.lib.bhr_solver_run(self._h, out_dir.encode() if out_dir else None,
+                                       name.encode() if name else None))
+
+    def waveform(self):
+        n_max = self.info()["rows_done"]
+        t, h, e = np.zeros(n_max), np.zeros(n_max * 14), np.zeros(n_max)
+        n = I(0)
+        _check(self.lib.bhr_solver_waveform(self._h, _ptr(t), _ptr(h), _ptr(e), n_max, C.byref(n)))
+        n = n.value
+        return t[:n], h[: n * 14].reshape(n, 14), e[:n]
+
+    def get_state(self):
+        NM = self.N * self.M
+        out = [np.zeros(NM) for _ in range(4)]
+        _check(self.lib.bhr_solver_get_state(self._h, *[_ptr(x) for x in out]))
+        return [x.reshape(self.M, self.N) for x in out]
+
+    def set_state(self, qre, qim, pre, pim):
+        arrs = [np.ascontiguousarray(x, dtype=np.float64).reshape(-1) for x in (qre, qim, pre, pim)]
+        _check(self.lib.bhr_solver_set_state(self._h, *[_ptr(x) for x in arrs]))
+
+    def get_extraction(self):
+        out = [np.zeros(self.M) for _ in range(6)]
+        _check(self.lib.bhr_solver_get_extraction(self._h, *[_ptr(x) for x in out]))
+        return out
+
+    def get_source(self):
+        tre, tim = np.zeros(self.N * self.M), np.zeros(self.N * self.M)
+        _check(self.lib.bhr_solver_get_source(self._h, _ptr(tre), _ptr(tim)))
+        return tre.reshape(self.M, self.N), tim.reshape(self.M, self.N)
+
+    def stream(self) -> int:
+        return int(self.lib.bhr_solver_stream(self._h) or 0)
+
+    def profile(self, nsteps: int):
+        avg, tot = np.zeros(5), np.zeros(1)
+        _check(self.lib.bhr_solver_profile(self._h, int(nsteps), _ptr(avg), _ptr(tot)))
+        return avg, float(tot[0])
+
+
+__all__ = ["Params", "Particle", "Solver", "BhrError", "grid", "swsh", "source_coefficients", "load_library",
+           "BHR_INIT_ZERO", "BHR_INIT_GAUSSIAN", "BHR_FP64", "BHR_MIXED", "BHR_SSPRK3"]

@@ -1,0 +1,39 @@
+// bhr_host.h -- host-side pieces of the solver shared between translation
+// units: grid, coefficient factor tables, harmonics, trajectory cursor.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "bhr.h"
+
+namespace bhr {
+
+constexpr double kPiParm = 3.14159265358979;  // HighOrder/parm.h:12
+
+struct Grid {
+  int N = 0, M = 0;
+  double dx = 0, dtheta = 0, r_plus = 0, r_minus = 0;
+  std::vector<double> x_c, r_c, theta;
+};
+
+// Grid of HighOrder/main.c:79-198, with a horizon floor where the Newton
+// iteration would step to r <= r+ (see grid.cpp).
+Grid make_grid(const bhr_params &p);
+// Per-column and per-row coefficient factors (layouts of bhr_internal.h).
+void make_tables(const bhr_params &p, const Grid &g, std::vector<double> &coltab, std::vector<double> &rowtab);
+// Spin-weighted harmonic s=-2 (HighOrder/proj.c:16-35).
+double swsh(double ell, double ml, double the);
+// Boole-rule projection weights: h_l = sum_b W[l*M + b] * q[b] for
+// l = |m| + 0..6 (HighOrder/proj.c:37-75, HighOrder/body.cu:189-202).
+void make_projection_weights(const bhr_params &p, const Grid &g, std::vector<double> &w7);
+// Weights of dE/dt = sum_b |int psi|^2 * E[b] (HighOrder/body.cu:174-184).
+void make_dedt_weights(const bhr_params &p, const Grid &g, std::vector<double> &e);
+// Closed initial data planes (q_re, q_im, p_re, p_im) for init_kind.
+void make_initial_data(const bhr_params &p, const Grid &g, std::vector<double> &planes);
+// Reference closure (kernel_boundary2a then 2b) applied on host planes.
+void apply_closure_host(double *planes, int N, int M, bool even_m);
+
+void set_error(const std::string &msg);
+
+}  // namespace bhr

@@ -1,0 +1,106 @@
+// bhr_internal.h -- shared definitions between the host code (bhr_solver.cpp)
+// and the sm_100a kernels (bhr_kernels.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bhr {
+
+// Stage tile: TC radial columns x TR theta rows per CTA.  The loaded window
+// adds 4 columns each side (the Kreiss-Oliger stencil reaches +-4,
+// HighOrder/kern.cu:247-256) and 3 rows each side for q (the 6th-order
+// theta stencils reach +-3, HighOrder/kern.cu:206-222).
+constexpr int TC = 64;
+constexpr int TR = 16;
+constexpr int WC = TC + 8;   // window columns
+constexpr int QR = TR + 6;   // q window rows
+constexpr int STAGE_THREADS = 256;
+
+// Per-column coefficient factors (host-built, FP64).  With bir = B0 +
+// B1*sin^2(theta) every coefficient of HighOrder/kern.cu:132-158 is a
+// per-column numerator, a per-row factor and 1/bir.
+enum ColField {
+  CF_B0 = 0,   // -(2 cL - Om^2) Sg^2 / cL^2
+  CF_B1,       // a^2 Dt
+  CF_ATN,      // 2 (cL - Om^2) Sg^2 / cL^2        Ataurho = ATN / bir
+  CF_ARN,      // -Om^2 Sg^2 / cL^2                Arhorho = ARN / bir
+  CF_CCN,      // -Dt                              Ayy     = CCN / bir
+  CF_XR,       // BtauReal * bir
+  CF_YR,       // BrhoReal * bir
+  CF_CR0,      // CReal * bir, theta-free part
+  CF_CR1,      // Dt: multiplies g(theta) = 4cot^2 - 4m cot csc + m^2 csc^2
+  CF_BI0,      // BtauImag * bir, theta-free part
+  CF_BI1,      // -4 a Dt: multiplies cos(theta)
+  CF_BRI,      // BrhoImag * bir
+  CF_CIN,      // CImag * bir
+  CF_COUNT
+};
+enum RowField { RF_S2 = 0, RF_COS, RF_G, RF_CTAN, RF_COUNT };
+
+// One step's particle source, prepared on the host from the trajectory.
+struct StepRec {
+  double c_re[6], c_im[6];  // bilinear coefficients times the turn-on window
+  double rp, tp, wr;        // particle r, theta and the radial width
+  int col0, row0;           // patch origin: ip - PTSX/2, it - PTSY/2
+};
+
+// Device-side run counters, advanced by the extraction kernel at the end of
+// each step so a captured step graph can be replayed.
+struct RunState {
+  int k;          // steps done
+  int nrow;       // waveform rows written
+  int err;        // bhr_status of the first device-detected failure
+  int pad;
+  double timer;   // accumulated as timer += dt (HighOrder/body.cu:214)
+};
+
+struct StageArgs {
+  const double *vin;    // stage input planes (also the TMA source)
+  const double *un;     // u^n planes (stages 2 and 3)
+  double *out;          // output planes
+  const double *coltab; // [CF_COUNT][N]
+  const double *rowtab; // [RF_COUNT][M]
+  const double *src;    // source patch [2][PTSY][PTSX] or nullptr
+  const StepRec *recs;  // per-step records or nullptr
+  const RunState *rs;
+  int *err;
+  int N, M, PTSX, PTSY;
+  int even_m;
+  double dt, cx, cy, cyy, cko;
+};
+
+struct SourceArgs {
+  double *src;          // [2][PTSY][PTSX]
+  const StepRec *recs;
+  const RunState *rs;
+  const double *r_c;    // [N]
+  const double *theta;  // [M]
+  int N, M, PTSX, PTSY;
+  double a, mass, m, wt;
+};
+
+struct ExtractArgs {
+  const double *u;      // u^n planes after the step
+  double *ext;          // [2][M] psi at ext_col
+  double *integ;        // [4][M] int_re, int_im, dint_re, dint_im
+  const double *wproj;  // [7][M] Boole x swsh projection weights
+  const double *wdedt;  // [M]
+  double *rows;         // [max_rows][16]: t, h+/hx x 7, dedt
+  RunState *rs;
+  int N, M, ext_col, Fr, max_rows, even_m;
+  double dt, out_start, Xmax;
+};
+
+// Launchers (bhr_kernels.cu).
+cudaError_t encode_state_maps(void *planes, int N, int M, CUtensorMap *tm_q, CUtensorMap *tm_p);
+cudaError_t launch_stage(int stage, const CUtensorMap &tm_q, const CUtensorMap &tm_p, const StageArgs &a,
+                         cudaStream_t st);
+cudaError_t launch_source(const SourceArgs &a, cudaStream_t st);
+cudaError_t launch_extract(const ExtractArgs &a, cudaStream_t st);
+cudaError_t launch_closure(double *planes, int N, int M, int even_m, cudaStream_t st);
+size_t stage_smem_bytes();
+cudaError_t prepare_kernels();
+
+}  // namespace bhr

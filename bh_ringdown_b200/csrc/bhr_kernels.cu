@@ -1,0 +1,572 @@
+// bhr_kernels.cu -- sm_100a kernels of the FP64 Teukolsky step.
+//
+// One time step is five launches on the solver stream:
+//   source_patch  the Gaussian-smeared particle source on its PTSX x PTSY patch
+//                 (HighOrder/kern.cu:755-768 reset + 1185-2683 deposit)
+//   stage<1,2,3>  one SSP-RK3 stage each: TMA stages a (q, p) tile with its
+//                 halo into shared memory, the pole and radial-end closures of
+//                 the stage input are rebuilt there, then the 6th-order
+//                 stencils, Kreiss-Oliger dissipation, coefficients, source
+//                 and the Shu-Osher combination are applied and the interior
+//                 of the next stage is written once
+//                 (HighOrder/kern.cu:171-753 as kernel_rhs*/update*/boundary*)
+//   extract       psi at the extraction column, its two time integrals, and
+//                 on output steps the swsh projection and dE/dt
+//                 (HighOrder/body.cu:168-212, HighOrder/proj.c:37-75)
+//
+// Storage: each state is four planes (q_re, q_im, p_re, p_im) of M x N
+// doubles, idx(b,a) = N*b + a.  Only interior points 3 <= b < M-3,
+// 3 <= a < N-3 are stored; the boundary rows and columns of every stage are
+// the reference's extrapolation closure of the interior and are rebuilt by
+// whoever reads them.
+#include "bhr_internal.h"
+
+#include <cudaTypedefs.h>
+
+namespace bhr {
+
+namespace {
+
+constexpr double kThird = 0.33333333333333333;   // HighOrder/kern.cu:46
+constexpr double kPie = 3.141592653589793;       // HighOrder/kern.cu:1188
+constexpr long long kMaxWaitIters = 1LL << 22;   // bounded mbarrier wait
+
+// ---- PTX helpers ---------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase) {
+  for (long long i = 0; i < kMaxWaitIters; i++)
+    if (mbar_try_wait(bar, phase)) return true;
+  return false;
+}
+// 3D tiled TMA load, no multicast.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// ---- stencils (HighOrder/kern.cu:192-261) ---------------------------------
+__device__ __forceinline__ double d1c(const double *v, int c) {
+  return 45.0 * (v[c + 1] - v[c - 1]) - 9.0 * (v[c + 2] - v[c - 2]) + (v[c + 3] - v[c - 3]);
+}
+__device__ __forceinline__ double ko8c(const double *v, int c) {
+  return (v[c + 4] + v[c - 4]) - 8.0 * (v[c + 3] + v[c - 3]) + 28.0 * (v[c + 2] + v[c - 2]) -
+         56.0 * (v[c + 1] + v[c - 1]) + 70.0 * v[c];
+}
+
+struct __align__(128) StageSmem {
+  double q[2][QR][WC];  // TMA box {WC, QR, 2} of planes q_re, q_im
+  double p[2][TR][WC];  // TMA box {WC, TR, 2} of planes p_re, p_im
+  double bb[TR][WC];    // bb on the window columns (for d bb/dx)
+  double ib[TR][WC];    // 1/bir
+  double ee[TR][WC];    // ee = Ataurho + bb
+  uint64_t bar;
+};
+
+template <int STAGE>
+__global__ void __launch_bounds__(STAGE_THREADS, 2)
+    stage_kernel(const __grid_constant__ CUtensorMap tm_q, const __grid_constant__ CUtensorMap tm_p,
+                 const StageArgs A) {
+  extern __shared__ unsigned char smem_raw[];
+  StageSmem &S = *reinterpret_cast<StageSmem *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+  const int c0 = blockIdx.x * TC, b0 = blockIdx.y * TR;
+  const int N = A.N, M = A.M;
+  const size_t NM = static_cast<size_t>(N) * M;
+
+  if (tid == 0) {
+    mbar_init(&S.bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    mbar_expect_tx(&S.bar, static_cast<uint32_t>(sizeof(S.q) + sizeof(S.p)));
+    tma_load_3d(&S.q[0][0][0], &tm_q, c0 - 4, b0 - 3, 0, &S.bar);
+    tma_load_3d(&S.p[0][0][0], &tm_p, c0 - 4, b0, 2, &S.bar);
+  }
+
+  // Coefficient pass while the tile is in flight: bb, 1/bir and ee on the
+  // window columns of the tile rows (HighOrder/kern.cu:132-149).
+  const double *ct = A.coltab;
+  const double *rt = A.rowtab;
+  for (int i = tid; i < TR * WC; i += STAGE_THREADS) {
+    const int r = i / WC, w = i - r * WC;
+    const int b = b0 + r, a = c0 - 4 + w;
+    if (w >= 1 && w < WC - 1 && b >= 3 && b < M - 3 && a >= 0 && a < N) {
+      const double bir = __ldg(ct + CF_B0 * N + a) + __ldg(ct + CF_B1 * N + a) * __ldg(rt + RF_S2 * M + b);
+      const double ib = 1.0 / bir;
+      const double At = __ldg(ct + CF_ATN * N + a) * ib;
+      const double Ar = __ldg(ct + CF_ARN * N + a) * ib;
+      const double bb = -(At + sqrt(At * At + 4.0 * Ar)) * 0.5;
+      S.bb[r][w] = bb;
+      S.ib[r][w] = ib;
+      S.ee[r][w] = At + bb;
+    }
+  }
+
+  const bool ok = mbar_wait_bounded(&S.bar, 0);
+  if (!__syncthreads_and(ok)) {
+    if (tid == 0) atomicCAS(A.err, 0, 5 /* BHR_TIMEOUT */);
+    mbar_wait_bounded(&S.bar, 0);
+    return;
+  }
+
+  // Closure of the stage input rebuilt in shared memory.
+  // Poles, q only (HighOrder/kern.cu:320-409): rows 2,1,0 from 3,4 and
+  // M-3,M-2,M-1 from M-4,M-5 on columns 3..N-4; zero for odd m.
+  const bool lo_rows = (b0 == 0), hi_rows = (b0 + TR + 3 > M - 3);
+  if (lo_rows || hi_rows) {
+    for (int i = tid; i < 2 * WC; i += STAGE_THREADS) {
+      const int pl = i / WC, w = i - pl * WC;
+      const int a = c0 - 4 + w;
+      if (a < 3 || a >= N - 3) continue;
+      double(*q)[WC] = S.q[pl];
+      const int o = 3 - b0;  // window row of global row g is g + o
+      if (lo_rows) {
+        if (A.even_m) {
+          q[2 + o][w] = (4.0 * q[3 + o][w] - q[4 + o][w]) * kThird;
+          q[1 + o][w] = (4.0 * q[2 + o][w] - q[3 + o][w]) * kThird;
+          q[0 + o][w] = (4.0 * q[1 + o][w] - q[2 + o][w]) * kThird;
+        } else {
+          q[2 + o][w] = 0.0; q[1 + o][w] = 0.0; q[0 + o][w] = 0.0;
+        }
+      }
+      if (hi_rows) {
+        if (A.even_m) {
+          q[M - 3 + o][w] = (4.0 * q[M - 4 + o][w] - q[M - 5 + o][w]) * kThird;
+          q[M - 2 + o][w] = (4.0 * q[M - 3 + o][w] - q[M - 4 + o][w]) * kThird;
+          q[M - 1 + o][w] = (4.0 * q[M - 2 + o][w] - q[M - 3 + o][w]) * kThird;
+        } else {
+          q[M - 3 + o][w] = 0.0; q[M - 2 + o][w] = 0.0; q[M - 1 + o][w] = 0.0;
+        }
+      }
+    }
+  }
+  // Radial ends, all four planes, tile rows (HighOrder/kern.cu:412-449).
+  const bool lo_cols = (c0 == 0), hi_cols = (c0 + TC + 4 > N - 3);
+  if (lo_cols || hi_cols) {
+    for (int i = tid; i < 4 * TR; i += STAGE_THREADS) {
+      const int pl = i / TR, r = i - pl * TR;
+      const int b = b0 + r;
+      if (b < 3 || b >= M - 3) continue;
+      double *row = pl < 2 ? &S.q[pl][r + 3][0] : &S.p[pl - 2][r][0];
+      const int o = 4 - c0;  // window column of global column a is a + o
+      if (lo_cols) {
+        row[2 + o] = (4.0 * row[3 + o] - row[4 + o]) * kThird;
+        row[1 + o] = (4.0 * row[2 + o] - row[3 + o]) * kThird;
+        row[0 + o] = (4.0 * row[1 + o] - row[2 + o]) * kThird;
+      }
+      if (hi_cols) {
+        row[N - 3 + o] = (4.0 * row[N - 4 + o] - row[N - 5 + o]) * kThird;
+        row[N - 2 + o] = (4.0 * row[N - 3 + o] - row[N - 4 + o]) * kThird;
+        row[N - 1 + o] = (4.0 * row[N - 2 + o] - row[N - 3 + o]) * kThird;
+      }
+    }
+  }
+  __syncthreads();
+
+  // Source patch placement for this step.
+  int src_c0 = 0, src_r0 = 0;
+  bool tile_src = false;
+  if (A.src != nullptr) {
+    const StepRec &rec = A.recs[A.rs->k];
+    src_c0 = rec.col0;
+    src_r0 = rec.row0;
+    tile_src = (src_c0 < c0 + TC) && (src_c0 + A.PTSX > c0) && (src_r0 < b0 + TR) && (src_r0 + A.PTSY > b0);
+  }
+
+  const int a0 = c0 + 2 * tx;  // this thread's columns a0, a0+1
+  const int w0 = 2 * tx + 4;   // their window column
+  const double dt = A.dt;
+#pragma unroll 1
+  for (int rr = 0; rr < 2; rr++) {
+    const int r = 2 * ty + rr;
+    const int b = b0 + r;
+    if (b < 3 || b >= M - 3) continue;
+    if (a0 + 1 < 3 || a0 >= N - 3) continue;
+
+    // Radial first derivative and dissipation of the four planes.
+    double fx[4][2], fk[4][2], fc[4][2];
+#pragma unroll
+    for (int pl = 0; pl < 4; pl++) {
+      const double *row = pl < 2 ? &S.q[pl][r + 3][0] : &S.p[pl - 2][r][0];
+      double v[10];
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+        const double2 t = *reinterpret_cast<const double2 *>(row + w0 - 4 + 2 * j);
+        v[2 * j] = t.x;
+        v[2 * j + 1] = t.y;
+      }
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const int a = a0 + c;
+        fc[pl][c] = v[4 + c];
+        fx[pl][c] = d1c(v, 4 + c) * A.cx;
+        fk[pl][c] = (a >= 4 && a < N - 4) ? ko8c(v, 4 + c) * A.cko : 0.0;
+      }
+    }
+    // Theta derivatives of q (HighOrder/kern.cu:206-226).
+    const double ctan = __ldg(rt + RF_CTAN * M + b);
+    double ll[2][2];
+#pragma unroll
+    for (int pl = 0; pl < 2; pl++) {
+      double f[7][2];
+#pragma unroll
+      for (int j = 0; j < 7; j++) {
+        const double2 t = *reinterpret_cast<const double2 *>(&S.q[pl][r + j][w0]);
+        f[j][0] = t.x;
+        f[j][1] = t.y;
+      }
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const double y1 = (f[6][c] - f[0][c]) - 9.0 * (f[5][c] - f[1][c]) + 45.0 * (f[4][c] - f[2][c]);
+        const double y2 = 2.0 * (f[6][c] + f[0][c]) - 27.0 * (f[5][c] + f[1][c]) +
+                          270.0 * (f[4][c] + f[2][c]) - 490.0 * f[3][c];
+        ll[pl][c] = y2 * A.cyy + ctan * (y1 * A.cy);
+      }
+    }
+
+    const double cs = __ldg(rt + RF_COS * M + b);
+    const double gth = __ldg(rt + RF_G * M + b);
+    double res[4][2];
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      const int a = a0 + c;
+      const int w = w0 + c;
+      const int ac = (a < N) ? a : N - 1;  // table reads stay in range
+      const double bb = S.bb[r][w], ib = S.ib[r][w], ee = S.ee[r][w];
+      const double dbdx = (45.0 * (S.bb[r][w + 1] - S.bb[r][w - 1]) - 9.0 * (S.bb[r][w + 2] - S.bb[r][w - 2]) +
+                           (S.bb[r][w + 3] - S.bb[r][w - 3])) * A.cx;
+      const double cc = __ldg(ct + CF_CCN * N + ac) * ib;
+      const double btr = __ldg(ct + CF_XR * N + ac) * ib;
+      const double brr = __ldg(ct + CF_YR * N + ac) * ib;
+      const double bti = (__ldg(ct + CF_BI0 * N + ac) + __ldg(ct + CF_BI1 * N + ac) * cs) * ib;
+      const double dim = __ldg(ct + CF_BRI * N + ac) * ib - bb * bti;
+      const double vre = -(__ldg(ct + CF_CR0 * N + ac) + __ldg(ct + CF_CR1 * N + ac) * gth) * ib;
+      const double vim = -__ldg(ct + CF_CIN * N + ac) * ib;
+      const double are = -btr, aim = -bti;
+      const double dre = (brr - bb * btr) - dbdx * ee;
+      double sre = 0.0, sim = 0.0;
+      if (tile_src) {
+        const int sc = a - src_c0, sr = b - src_r0;
+        if (sc >= 0 && sc < A.PTSX && sr >= 0 && sr < A.PTSY) {
+          sre = A.src[static_cast<size_t>(sr) * A.PTSX + sc];
+          sim = A.src[static_cast<size_t>(A.PTSY + sr) * A.PTSX + sc];
+        }
+      }
+      const double qr = fc[0][c], qi = fc[1][c], pr = fc[2][c], pi = fc[3][c];
+      const double qxr = fx[0][c], qxi = fx[1][c], pxr = fx[2][c], pxi = fx[3][c];
+      res[0][c] = -bb * qxr + pr - fk[0][c];
+      res[1][c] = -bb * qxi + pi - fk[1][c];
+      res[2][c] = sre + ee * pxr - fk[2][c] + cc * ll[0][c] + dre * qxr - dim * qxi - are * pr + aim * pi -
+                  vre * qr + vim * qi;
+      res[3][c] = sim + ee * pxi - fk[3][c] + cc * ll[1][c] + dre * qxi + dim * qxr - are * pi - aim * pr -
+                  vre * qi - vim * qr;
+    }
+
+    // Shu-Osher stage combination (HighOrder/kern.cu:301-318, 582-620).
+    const size_t base = static_cast<size_t>(b) * N + a0;
+    const bool both = (a0 >= 3) && (a0 + 1 < N - 3);
+#pragma unroll
+    for (int pl = 0; pl < 4; pl++) {
+      double o[2];
+      if (STAGE == 1) {
+        o[0] = fc[pl][0] + dt * res[pl][0];
+        o[1] = fc[pl][1] + dt * res[pl][1];
+      } else {
+        const double2 u = *reinterpret_cast<const double2 *>(A.un + pl * NM + base);
+        if (STAGE == 2) {
+          o[0] = 0.25 * (3.0 * u.x + fc[pl][0] + dt * res[pl][0]);
+          o[1] = 0.25 * (3.0 * u.y + fc[pl][1] + dt * res[pl][1]);
+        } else {
+          o[0] = kThird * (u.x + 2.0 * fc[pl][0] + 2.0 * dt * res[pl][0]);
+          o[1] = kThird * (u.y + 2.0 * fc[pl][1] + 2.0 * dt * res[pl][1]);
+        }
+      }
+      double *dst = A.out + pl * NM + base;
+      if (both) {
+        *reinterpret_cast<double2 *>(dst) = make_double2(o[0], o[1]);
+      } else {
+        if (a0 >= 3 && a0 < N - 3) dst[0] = o[0];
+        if (a0 + 1 >= 3 && a0 + 1 < N - 3) dst[1] = o[1];
+      }
+    }
+  }
+}
+
+// ---- closure of stored planes (HighOrder/kern.cu:622-753) ------------------
+__device__ __forceinline__ double pole_val(const double *P, int N, int M, int even, int b, int a) {
+  if (b >= 3 && b < M - 3) return P[static_cast<size_t>(b) * N + a];
+  if (!even) return 0.0;
+  if (b < 3) {
+    const double f3 = P[static_cast<size_t>(3) * N + a], f4 = P[static_cast<size_t>(4) * N + a];
+    const double f2 = (4.0 * f3 - f4) * kThird;
+    if (b == 2) return f2;
+    const double f1 = (4.0 * f2 - f3) * kThird;
+    if (b == 1) return f1;
+    return (4.0 * f1 - f2) * kThird;
+  }
+  const double g4 = P[static_cast<size_t>(M - 4) * N + a], g5 = P[static_cast<size_t>(M - 5) * N + a];
+  const double g3 = (4.0 * g4 - g5) * kThird;
+  if (b == M - 3) return g3;
+  const double g2 = (4.0 * g3 - g4) * kThird;
+  if (b == M - 2) return g2;
+  return (4.0 * g2 - g3) * kThird;
+}
+
+__device__ __forceinline__ double closed_val(const double *P, int N, int M, int even, int b, int a) {
+  if (a >= 3 && a < N - 3) return pole_val(P, N, M, even, b, a);
+  if (a < 3) {
+    const double f3 = pole_val(P, N, M, even, b, 3), f4 = pole_val(P, N, M, even, b, 4);
+    const double f2 = (4.0 * f3 - f4) * kThird;
+    if (a == 2) return f2;
+    const double f1 = (4.0 * f2 - f3) * kThird;
+    if (a == 1) return f1;
+    return (4.0 * f1 - f2) * kThird;
+  }
+  const double g4 = pole_val(P, N, M, even, b, N - 4), g5 = pole_val(P, N, M, even, b, N - 5);
+  const double g3 = (4.0 * g4 - g5) * kThird;
+  if (a == N - 3) return g3;
+  const double g2 = (4.0 * g3 - g4) * kThird;
+  if (a == N - 2) return g2;
+  return (4.0 * g2 - g3) * kThird;
+}
+
+__global__ void closure_poles_kernel(double *P, int N, int M, int even) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pl = blockIdx.y;
+  if (a < 3 || a >= N - 3) return;
+  double *Q = P + static_cast<size_t>(pl) * N * M;
+  const double v0 = pole_val(Q, N, M, even, 0, a), v1 = pole_val(Q, N, M, even, 1, a),
+               v2 = pole_val(Q, N, M, even, 2, a);
+  const double w3 = pole_val(Q, N, M, even, M - 3, a), w2 = pole_val(Q, N, M, even, M - 2, a),
+               w1 = pole_val(Q, N, M, even, M - 1, a);
+  Q[a] = v0;
+  Q[static_cast<size_t>(N) + a] = v1;
+  Q[static_cast<size_t>(2) * N + a] = v2;
+  Q[static_cast<size_t>(M - 3) * N + a] = w3;
+  Q[static_cast<size_t>(M - 2) * N + a] = w2;
+  Q[static_cast<size_t>(M - 1) * N + a] = w1;
+}
+
+__global__ void closure_ends_kernel(double *P, int N, int M) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pl = blockIdx.y;
+  if (b >= M) return;
+  double *row = P + static_cast<size_t>(pl) * N * M + static_cast<size_t>(b) * N;
+  row[2] = (4.0 * row[3] - row[4]) * kThird;
+  row[N - 3] = (4.0 * row[N - 4] - row[N - 5]) * kThird;
+  row[1] = (4.0 * row[2] - row[3]) * kThird;
+  row[N - 2] = (4.0 * row[N - 3] - row[N - 4]) * kThird;
+  row[0] = (4.0 * row[1] - row[2]) * kThird;
+  row[N - 1] = (4.0 * row[N - 2] - row[N - 3]) * kThird;
+}
+
+// ---- particle source patch (HighOrder/kern.cu:1185-1227, 2666-2683) ---------
+__global__ void source_patch_kernel(const SourceArgs A) {
+  const int j = blockIdx.x, k = threadIdx.x;
+  if (k >= A.PTSX) return;
+  const StepRec &rec = A.recs[A.rs->k];
+  const int row = j + rec.row0, col = k + rec.col0;
+  double sre = 0.0, sim = 0.0;
+  if (col > 0 && col < A.N && row > 0 && row < A.M) {
+    const double a = A.a, mass = A.mass;
+    const double rpl = mass + sqrt(mass * mass - a * a), rmn = mass - sqrt(mass * mass - a * a);
+    const double g0 = 1.0 / sqrt(2.0 * kPie);
+    const double th = A.theta[row], r = A.r_c[col];
+    const double st = sin(th), ctv = cos(th);
+    const double wt = A.wt, wr = rec.wr;
+    const double dth = th - rec.tp;
+    const double T0 = g0 * exp(-dth * dth / (2.0 * wt * wt)) / wt;
+    const double T1 = -dth / (wt * wt) * T0;
+    const double T2 = (-1.0 / (wt * wt) + dth * dth / (wt * wt * wt * wt)) * T0;
+    const double dr = r - rec.rp;
+    const double R0 = g0 * exp(-dr * dr / (2.0 * wr * wr)) / wr;
+    const double R1 = -dr / (wr * wr) * R0;
+    const double R2 = (-1.0 / (wr * wr) + dr * dr / (wr * wr * wr * wr)) * R0;
+    const double bas[6] = {R0 * T0, R0 * T1, R0 * T2, R1 * T0, R1 * T1, R2 * T0};
+    double tr = 0.0, ti = 0.0;
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+      tr += rec.c_re[i] * bas[i];
+      ti += rec.c_im[i] * bas[i];
+    }
+    // TT = Sigma * t / rho^4 with rho = -1/(r - i a cos): 1/rho^4 = (r - i a cos)^4.
+    const double x = r, y = -a * ctv;
+    const double x2 = x * x - y * y, y2 = 2.0 * x * y;        // (x+iy)^2
+    const double x4 = x2 * x2 - y2 * y2, y4 = 2.0 * x2 * y2;  // (x+iy)^4
+    const double sig = r * r + a * a * ctv * ctv;
+    double Tr = sig * (tr * x4 - ti * y4), Ti = sig * (tr * y4 + ti * x4);
+    const double ph = -A.m * a / (rpl - rmn) * log((r - rpl) / (r - rmn));
+    const double cph = cos(ph), sph = sin(ph);
+    const double Ur = Tr * cph - Ti * sph, Ui = Tr * sph + Ti * cph;
+    const double delta = r * r + a * a - 2.0 * mass * r;
+    const double cs2 = (r * r + a * a) * (r * r + a * a) - a * a * delta * st * st;
+    sre = 8.0 * kPie * delta * Ur / cs2 / (r * r * r);
+    sim = 8.0 * kPie * delta * Ui / cs2 / (r * r * r);
+  }
+  A.src[static_cast<size_t>(j) * A.PTSX + k] = sre;
+  A.src[static_cast<size_t>(A.PTSY + j) * A.PTSX + k] = sim;
+}
+
+// ---- extraction, integration, projection (HighOrder/body.cu:168-212) ------
+constexpr int kExtractThreads = 256;
+constexpr int kSums = 15;
+
+__global__ void __launch_bounds__(kExtractThreads) extract_kernel(const ExtractArgs A) {
+  __shared__ double red[kExtractThreads / 32][kSums];
+  __shared__ int nan_flag;
+  const int tid = threadIdx.x;
+  const int N = A.N, M = A.M;
+  const size_t NM = static_cast<size_t>(N) * M;
+  const int k = A.rs->k;
+  const bool out_step = ((k % A.Fr) == 0) && (static_cast<double>(k) * A.dt >= A.out_start);
+  if (tid == 0) nan_flag = 0;
+  __syncthreads();
+  double acc[kSums];
+#pragma unroll
+  for (int i = 0; i < kSums; i++) acc[i] = 0.0;
+  for (int b = tid; b < M; b += kExtractThreads) {
+    const double psr = closed_val(A.u, N, M, A.even_m, b, A.ext_col);
+    const double psi = closed_val(A.u + NM, N, M, A.even_m, b, A.ext_col);
+    if (!isfinite(psr) || !isfinite(psi)) nan_flag = 1;
+    A.ext[b] = psr;
+    A.ext[M + b] = psi;
+    const double ir = A.integ[b] + psr * A.dt;
+    const double ii = A.integ[M + b] + psi * A.dt;
+    const double dr = A.integ[2 * M + b] + ir * A.dt;
+    const double di = A.integ[3 * M + b] + ii * A.dt;
+    A.integ[b] = ir;
+    A.integ[M + b] = ii;
+    A.integ[2 * M + b] = dr;
+    A.integ[3 * M + b] = di;
+    if (out_step) {
+#pragma unroll
+      for (int l = 0; l < 7; l++) {
+        const double wl = A.wproj[l * M + b];
+        acc[2 * l] += wl * dr;
+        acc[2 * l + 1] -= wl * di;
+      }
+      acc[14] += (ir * ir + ii * ii) * A.wdedt[b];
+    }
+  }
+  if (out_step) {
+#pragma unroll
+    for (int i = 0; i < kSums; i++) {
+      double v = acc[i];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      if ((tid & 31) == 0) red[tid >> 5][i] = v;
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if (nan_flag) atomicCAS(&A.rs->err, 0, 4 /* BHR_NAN_DETECTED */);
+    if (out_step && A.rs->nrow < A.max_rows) {
+      double *row = A.rows + static_cast<size_t>(A.rs->nrow) * 16;
+      row[0] = A.rs->timer - A.Xmax;
+      for (int i = 0; i < kSums; i++) {
+        double v = 0.0;
+        for (int w = 0; w < kExtractThreads / 32; w++) v += red[w][i];
+        row[1 + i] = v;
+      }
+      A.rs->nrow += 1;
+    }
+    A.rs->timer += A.dt;
+    A.rs->k = k + 1;
+  }
+}
+
+}  // namespace
+
+// ---- host launchers -------------------------------------------------------
+size_t stage_smem_bytes() { return sizeof(StageSmem) + 128; }
+
+cudaError_t encode_state_maps(void *planes, int N, int M, CUtensorMap *tm_q, CUtensorMap *tm_p) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult qr;
+    void *fn = nullptr;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr);
+    if (e != cudaSuccess || qr != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const cuuint64_t dims[3] = {static_cast<cuuint64_t>(N), static_cast<cuuint64_t>(M), 4};
+  const cuuint64_t strides[2] = {static_cast<cuuint64_t>(N) * 8, static_cast<cuuint64_t>(N) * M * 8};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const cuuint32_t box_q[3] = {WC, QR, 2};
+  const cuuint32_t box_p[3] = {WC, TR, 2};
+  CUresult r1 = encode(tm_q, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, planes, dims, strides, box_q, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r2 = encode(tm_p, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, planes, dims, strides, box_p, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return (r1 == CUDA_SUCCESS && r2 == CUDA_SUCCESS) ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+cudaError_t launch_stage(int stage, const CUtensorMap &tm_q, const CUtensorMap &tm_p, const StageArgs &a,
+                         cudaStream_t st) {
+  const size_t smem = stage_smem_bytes();
+  const dim3 grid(a.N / TC, a.M / TR), block(32, STAGE_THREADS / 32);
+  if (stage == 1) stage_kernel<1><<<grid, block, smem, st>>>(tm_q, tm_p, a);
+  else if (stage == 2) stage_kernel<2><<<grid, block, smem, st>>>(tm_q, tm_p, a);
+  else stage_kernel<3><<<grid, block, smem, st>>>(tm_q, tm_p, a);
+  return cudaGetLastError();
+}
+
+// Once per device (the attribute is per device context).
+cudaError_t prepare_kernels() {
+  const int smem = static_cast<int>(stage_smem_bytes());
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(stage_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) ||
+      (e = cudaFuncSetAttribute(stage_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) ||
+      (e = cudaFuncSetAttribute(stage_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)))
+    return e;
+  return cudaSuccess;
+}
+
+cudaError_t launch_source(const SourceArgs &a, cudaStream_t st) {
+  source_patch_kernel<<<a.PTSY, a.PTSX, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_extract(const ExtractArgs &a, cudaStream_t st) {
+  extract_kernel<<<1, kExtractThreads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_closure(double *planes, int N, int M, int even_m, cudaStream_t st) {
+  closure_poles_kernel<<<dim3((N + 127) / 128, 4), 128, 0, st>>>(planes, N, M, even_m);
+  closure_ends_kernel<<<dim3((M + 127) / 128, 4), 128, 0, st>>>(planes, N, M);
+  return cudaGetLastError();
+}
+
+}  // namespace bhr

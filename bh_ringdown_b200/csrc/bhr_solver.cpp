@@ -1,0 +1,668 @@
+// bhr_solver.cpp -- the C ABI of include/bhr.h: one solve on one device.
+//
+// Replaces body() of HighOrder/body.cu:25-225.  Differences in structure:
+// all state is per solve (no __device__ globals), the trajectory is read
+// once into memory and turned into per-step source records before the
+// loop, the extraction integrals and the projection stay on the device, and
+// a step is five kernel launches on one stream with no host round trip.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "bhr.h"
+#include "bhr_host.h"
+#include "bhr_internal.h"
+
+namespace bhr {
+
+static thread_local std::string g_err;
+void set_error(const std::string &msg) { g_err = msg; }
+
+#define BHR_CUDA_TRY(call)                                                                \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) {                                                              \
+      set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                      \
+      return BHR_CUDA_ERROR;                                                              \
+    }                                                                                     \
+  } while (0)
+
+}  // namespace bhr
+
+using namespace bhr;
+
+struct bhr_solver {
+  bhr_params p{};
+  Grid g;
+  int nt = 0, Fr = 1, max_rows = 0, ext_col = 0;
+  bool even_m = true;
+  bool has_source = false;
+  cudaStream_t stream = nullptr;
+  // device memory
+  double *u0 = nullptr, *u1 = nullptr, *u2 = nullptr;
+  double *coltab = nullptr, *rowtab = nullptr, *rc = nullptr, *th = nullptr;
+  double *src = nullptr, *ext = nullptr, *integ = nullptr, *wproj = nullptr, *wdedt = nullptr, *rows = nullptr;
+  StepRec *recs = nullptr;
+  RunState *rs = nullptr;
+  size_t bytes = 0;
+  CUtensorMap tq[3], tp[3];
+  int steps_done = 0;
+};
+
+namespace {
+
+int validate(const bhr_params &p) {
+  if (p.N < 64 || p.N % TC != 0) {
+    set_error("N must be a positive multiple of 64");
+    return BHR_INVALID_ARG;
+  }
+  if (p.M < 16 || p.M % TR != 0) {
+    set_error("M must be a multiple of 16 and >= 16");
+    return BHR_INVALID_ARG;
+  }
+  if (!(p.Xmax > p.Xmin) || !(p.mass > 0.0) || !(std::fabs(p.a) < p.mass) || !(p.T > 0.0)) {
+    set_error("need Xmax > Xmin, mass > 0, |a| < mass, T > 0");
+    return BHR_INVALID_ARG;
+  }
+  if (p.m != std::floor(p.m)) {
+    set_error("m must be an integer");
+    return BHR_INVALID_ARG;
+  }
+  if (p.PTSX < 1 || p.PTSX > 1024 || p.PTSY < 1 || p.PTSY > 65535) {
+    set_error("PTSX in [1,1024], PTSY >= 1");
+    return BHR_INVALID_ARG;
+  }
+  if (p.precision != BHR_FP64 || p.integrator != BHR_SSPRK3) {
+    set_error("only FP64 SSP-RK3 is built in this library");
+    return BHR_INVALID_ARG;
+  }
+  return BHR_OK;
+}
+
+template <class T>
+int dalloc(bhr_solver *s, T **ptr, size_t count) {
+  const size_t nbytes = sizeof(T) * (count ? count : 1);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void **>(ptr), nbytes);
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? BHR_OUT_OF_MEMORY : BHR_CUDA_ERROR;
+  }
+  s->bytes += nbytes;
+  return BHR_OK;
+}
+
+void free_all(bhr_solver *s) {
+  void *ptrs[] = {s->u0, s->u1, s->u2, s->coltab, s->rowtab, s->rc, s->th, s->src, s->ext,
+                  s->integ, s->wproj, s->wdedt, s->rows, s->recs, s->rs};
+  for (void *q : ptrs)
+    if (q) cudaFree(q);
+  if (s->stream) cudaStreamDestroy(s->stream);
+}
+
+// Kerr tortoise coordinate as the source placement uses it
+// (HighOrder/kern.cu:1194-1199).
+double tortoise(double r, double a, double rpl, double rmn) {
+  return r + (rpl * rpl + a * a) / (rpl - rmn) * std::log(r / rpl - 1.0) -
+         (rmn * rmn + a * a) / (rpl - rmn) * std::log(r / rmn - 1.0);
+}
+
+}  // namespace
+
+extern "C" {
+
+int bhr_abi_version(void) { return BHR_ABI_VERSION; }
+const char *bhr_last_error_string(void) { return g_err.c_str(); }
+double bhr_swsh(double ell, double m, double theta) { return swsh(ell, m, theta); }
+
+int bhr_params_default(bhr_params *p) {
+  if (!p) return BHR_INVALID_ARG;
+  std::memset(p, 0, sizeof(*p));
+  p->N = 16000;
+  p->M = 256;
+  p->Xmin = -50.0;
+  p->Xmax = 50.0;
+  p->mass = 1.0;
+  p->a = 1e-8;
+  p->m = 2.0;
+  p->dt = 0.002;
+  p->courant = 0.25;
+  p->out_every = 0.0;
+  p->T = 1500.0;
+  p->Fr = 50;
+  p->out_start = p->Xmax + 200.0;
+  p->ext_col = -1;
+  p->PTSX = 128;
+  p->PTSY = 128;
+  p->wr_fac = 2.0;
+  p->wt_fac = 6.0;
+  p->integrator = BHR_SSPRK3;
+  p->precision = BHR_FP64;
+  p->init_kind = BHR_INIT_ZERO;
+  p->init_center = 20.0;
+  p->init_width = 2.0;
+  p->init_ell = 2.0;
+  p->device = 0;
+  return BHR_OK;
+}
+
+int bhr_grid(const bhr_params *p, double *x_c, double *r_c, double *theta) {
+  if (!p) return BHR_INVALID_ARG;
+  if (int st = validate(*p)) return st;
+  Grid g = make_grid(*p);
+  if (x_c) std::memcpy(x_c, g.x_c.data(), sizeof(double) * p->N);
+  if (r_c) std::memcpy(r_c, g.r_c.data(), sizeof(double) * p->N);
+  if (theta) std::memcpy(theta, g.theta.data(), sizeof(double) * p->M);
+  return BHR_OK;
+}
+
+int bhr_solver_create(const bhr_params *pin, bhr_solver **out) {
+  if (!pin || !out) {
+    set_error("null argument");
+    return BHR_INVALID_ARG;
+  }
+  *out = nullptr;
+  if (int st = validate(*pin)) return st;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+    cudaGetLastError();
+    set_error("no CUDA device");
+    return BHR_NO_DEVICE;
+  }
+  if (pin->device < 0 || pin->device >= ndev) {
+    set_error("device ordinal out of range");
+    return BHR_INVALID_ARG;
+  }
+  auto *s = new bhr_solver();
+  s->p = *pin;
+  bhr_params &p = s->p;
+  s->g = make_grid(p);
+  const Grid &g = s->g;
+  if (!(p.dt > 0.0)) {
+    double dt = p.courant * std::fmin(g.dx, g.r_c[0] * g.dtheta);
+    if (p.out_every > 0.0) {
+      const double k = std::ceil(p.out_every / dt);
+      dt = p.out_every / k;
+      if (p.Fr <= 0) p.Fr = static_cast<int>(k);
+    }
+    p.dt = dt;
+  }
+  if (p.Fr <= 0) p.Fr = (p.out_every > 0.0) ? std::max(1, static_cast<int>(std::lround(p.out_every / p.dt))) : 1;
+  s->Fr = p.Fr;
+  s->ext_col = (p.ext_col < 0 || p.ext_col >= p.N) ? p.N - 1 : p.ext_col;
+  s->even_m = (static_cast<int>(p.m) % 2) == 0;
+  // HighOrder/body.cu:56-59 for rank 0 of p = 1.
+  const double endtime = (p.T - p.Xmax - 200.0) / 1 * (0 + 1) + p.Xmax + 200.0;
+  s->nt = static_cast<int>((endtime - 0.0) / p.dt);
+  s->max_rows = s->nt / s->Fr + 2;
+
+  const size_t NM = static_cast<size_t>(p.N) * p.M;
+  int st = BHR_OK;
+  if (cudaSetDevice(p.device) != cudaSuccess || prepare_kernels() != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error("cannot set device / create stream");
+    delete s;
+    return BHR_CUDA_ERROR;
+  }
+  if ((st = dalloc(s, &s->u0, 4 * NM)) || (st = dalloc(s, &s->u1, 4 * NM)) || (st = dalloc(s, &s->u2, 4 * NM)) ||
+      (st = dalloc(s, &s->coltab, static_cast<size_t>(CF_COUNT) * p.N)) ||
+      (st = dalloc(s, &s->rowtab, static_cast<size_t>(RF_COUNT) * p.M)) || (st = dalloc(s, &s->rc, p.N)) ||
+      (st = dalloc(s, &s->th, p.M)) || (st = dalloc(s, &s->src, 2 * static_cast<size_t>(p.PTSX) * p.PTSY)) ||
+      (st = dalloc(s, &s->ext, 2 * static_cast<size_t>(p.M))) || (st = dalloc(s, &s->integ, 4 * static_cast<size_t>(p.M))) ||
+      (st = dalloc(s, &s->wproj, 7 * static_cast<size_t>(p.M))) || (st = dalloc(s, &s->wdedt, p.M)) ||
+      (st = dalloc(s, &s->rows, 16 * static_cast<size_t>(s->max_rows))) || (st = dalloc(s, &s->rs, 1))) {
+    free_all(s);
+    delete s;
+    return st;
+  }
+  std::vector<double> coltab, rowtab, w7, we, init;
+  make_tables(p, g, coltab, rowtab);
+  make_projection_weights(p, g, w7);
+  make_dedt_weights(p, g, we);
+  make_initial_data(p, g, init);
+  auto up = [&](void *dst, const void *srcp, size_t n) { return cudaMemcpyAsync(dst, srcp, n, cudaMemcpyHostToDevice, s->stream); };
+  cudaError_t e = cudaSuccess;
+  if ((e = up(s->coltab, coltab.data(), coltab.size() * 8)) || (e = up(s->rowtab, rowtab.data(), rowtab.size() * 8)) ||
+      (e = up(s->rc, g.r_c.data(), g.r_c.size() * 8)) || (e = up(s->th, g.theta.data(), g.theta.size() * 8)) ||
+      (e = up(s->wproj, w7.data(), w7.size() * 8)) || (e = up(s->wdedt, we.data(), we.size() * 8)) ||
+      (e = up(s->u0, init.data(), init.size() * 8)) ||
+      (e = cudaMemsetAsync(s->u1, 0, 4 * NM * 8, s->stream)) || (e = cudaMemsetAsync(s->u2, 0, 4 * NM * 8, s->stream)) ||
+      (e = cudaMemsetAsync(s->integ, 0, 4 * p.M * 8, s->stream)) || (e = cudaMemsetAsync(s->ext, 0, 2 * p.M * 8, s->stream)) ||
+      (e = cudaMemsetAsync(s->src, 0, 2 * static_cast<size_t>(p.PTSX) * p.PTSY * 8, s->stream)) ||
+      (e = cudaMemsetAsync(s->rs, 0, sizeof(RunState), s->stream)) || (e = cudaStreamSynchronize(s->stream))) {
+    set_error(std::string("upload: ") + cudaGetErrorString(e));
+    free_all(s);
+    delete s;
+    return BHR_CUDA_ERROR;
+  }
+  double *bufs[3] = {s->u0, s->u1, s->u2};
+  for (int i = 0; i < 3; i++) {
+    if (encode_state_maps(bufs[i], p.N, p.M, &s->tq[i], &s->tp[i]) != cudaSuccess) {
+      set_error("cuTensorMapEncodeTiled failed");
+      free_all(s);
+      delete s;
+      return BHR_CUDA_ERROR;
+    }
+  }
+  *out = s;
+  return BHR_OK;
+}
+
+void bhr_solver_destroy(bhr_solver *s) {
+  if (!s) return;
+  cudaSetDevice(s->p.device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  free_all(s);
+  delete s;
+}
+
+int bhr_solver_info(const bhr_solver *s, bhr_info *info) {
+  if (!s || !info) return BHR_INVALID_ARG;
+  info->N = s->p.N;
+  info->M = s->p.M;
+  info->dx = s->g.dx;
+  info->dtheta = s->g.dtheta;
+  info->dt = s->p.dt;
+  info->nt = s->nt;
+  info->Fr = s->Fr;
+  info->steps_done = s->steps_done;
+  RunState rs{};
+  cudaMemcpy(&rs, s->rs, sizeof(rs), cudaMemcpyDeviceToHost);
+  info->rows_done = rs.nrow;
+  info->has_source = s->has_source ? 1 : 0;
+  info->r_plus = s->g.r_plus;
+  info->device_bytes = s->bytes;
+  return BHR_OK;
+}
+
+// HighOrder/body.cu:97-124: the pre-loop reads one line and then lines
+// until ptime >= timer; each step reads two lines and uses the second; a
+// read past the end leaves the particle variables unchanged; rp gets
+// +1e-6 every step; the second time derivatives are backward differences
+// of the first over dt (zero history at step 0); third derivatives are 0.
+int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows) {
+  if (!s || !rows || nrows < 2) {
+    set_error("trajectory needs at least two rows");
+    return BHR_INVALID_ARG;
+  }
+  const bhr_params &p = s->p;
+  const double a = p.a, mass = p.mass;
+  const double rpl = mass + std::sqrt(mass * mass - a * a), rmn = mass - std::sqrt(mass * mass - a * a);
+  std::vector<StepRec> recs(s->nt);
+  double row[10] = {0};
+  int cursor = 0;
+  auto rd = [&]() {
+    if (cursor < nrows) {
+      std::memcpy(row, rows + static_cast<size_t>(10) * cursor, sizeof(row));
+      cursor++;
+    }
+  };
+  double timer = 0.0;
+  const double start = timer;
+  rd();
+  do {
+    rd();
+  } while (row[0] < timer && cursor < nrows);
+  double rp = row[1];
+  double tmp11 = 0.0, tmp22 = 0.0, tmp33 = 0.0;
+  for (int k = 0; k < s->nt; k++) {
+    const int c0 = cursor;
+    rd();
+    rd();
+    if (cursor != c0) rp = row[1];
+    rp = rp + 1e-6;
+    bhr_particle pt{};
+    pt.rp = rp;
+    pt.tp = row[2];
+    pt.phip = row[6];
+    pt.E = row[7];
+    pt.lz = row[8];
+    pt.Q = row[9];
+    pt.drdt = row[3];
+    pt.d2rdt2 = (row[3] - tmp11) / p.dt;
+    pt.dthdt = row[4];
+    pt.d2thdt2 = (row[4] - tmp22) / p.dt;
+    pt.dphidt = row[5];
+    pt.d2phidt2 = (row[5] - tmp33) / p.dt;
+    tmp11 = row[3];
+    tmp22 = row[4];
+    tmp33 = row[5];
+    double cr[6], ci[6];
+    if (int st = bhr_source_coefficients(&pt, a, mass, p.m, cr, ci)) return st;
+    const double turn = std::pow(1.0 - std::exp(-(timer - start) / 25.0), 4);
+    StepRec &R = recs[k];
+    for (int i = 0; i < 6; i++) {
+      R.c_re[i] = cr[i] * turn;
+      R.c_im[i] = ci[i] * turn;
+    }
+    R.rp = rp;
+    R.tp = pt.tp;
+    R.wr = p.wr_fac * s->g.dx * (1.0 - rpl / rp);
+    const double xp = tortoise(rp, a, rpl, rmn);
+    const double ipd = (xp - p.Xmin) / s->g.dx, itd = pt.tp / s->g.dtheta;
+    if (!std::isfinite(ipd) || !std::isfinite(itd) || std::fabs(ipd) > 1e9 || std::fabs(itd) > 1e9) {
+      set_error("trajectory point outside the grid (non-finite tortoise coordinate)");
+      return BHR_INVALID_ARG;
+    }
+    R.col0 = static_cast<int>(ipd) - p.PTSX / 2;
+    R.row0 = static_cast<int>(itd) - p.PTSY / 2;
+    timer += p.dt;
+  }
+  cudaSetDevice(p.device);
+  if (s->recs) cudaFree(s->recs), s->bytes -= sizeof(StepRec) * static_cast<size_t>(s->nt ? s->nt : 1);
+  s->recs = nullptr;
+  if (int st = dalloc(s, &s->recs, static_cast<size_t>(s->nt))) return st;
+  BHR_CUDA_TRY(cudaMemcpyAsync(s->recs, recs.data(), sizeof(StepRec) * recs.size(), cudaMemcpyHostToDevice, s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  s->has_source = true;
+  return BHR_OK;
+}
+
+int bhr_solver_load_trajectory(bhr_solver *s, const char *path) {
+  if (!s || !path) return BHR_INVALID_ARG;
+  std::ifstream f(path);
+  if (!f) {
+    set_error(std::string("cannot open ") + path);
+    return BHR_IO_ERROR;
+  }
+  std::vector<double> rows;
+  std::string line;
+  while (std::getline(f, line)) {
+    std::istringstream is(line);
+    double v[10];
+    int n = 0;
+    while (n < 10 && (is >> v[n])) n++;
+    if (n == 0) continue;
+    if (n != 10) {
+      set_error("malformed .traj row (need 10 columns)");
+      return BHR_IO_ERROR;
+    }
+    rows.insert(rows.end(), v, v + 10);
+  }
+  return bhr_solver_set_trajectory(s, rows.data(), static_cast<int>(rows.size() / 10));
+}
+
+static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
+  auto mark = [&](int i) { return ev ? cudaEventRecord(ev[i], s->stream) : cudaSuccess; };
+  const bhr_params &p = s->p;
+  const double odx = 1.0 / s->g.dx, odth = 1.0 / s->g.dtheta, odt = 1.0 / p.dt;
+  const double third = 0.33333333333333333;
+  StageArgs A{};
+  A.coltab = s->coltab;
+  A.rowtab = s->rowtab;
+  A.src = s->has_source ? s->src : nullptr;
+  A.recs = s->recs;
+  A.rs = s->rs;
+  A.err = &s->rs->err;
+  A.N = p.N;
+  A.M = p.M;
+  A.PTSX = p.PTSX;
+  A.PTSY = p.PTSY;
+  A.even_m = s->even_m ? 1 : 0;
+  A.dt = p.dt;
+  A.cx = 0.016666666666667 * odx;
+  A.cy = 0.05 * third * odth;
+  A.cyy = 0.05 * third * third * odth * odth;
+  A.cko = 0.1 * 0.0625 * odt;
+  BHR_CUDA_TRY(mark(0));
+  if (s->has_source) {
+    SourceArgs S{};
+    S.src = s->src;
+    S.recs = s->recs;
+    S.rs = s->rs;
+    S.r_c = s->rc;
+    S.theta = s->th;
+    S.N = p.N;
+    S.M = p.M;
+    S.PTSX = p.PTSX;
+    S.PTSY = p.PTSY;
+    S.a = p.a;
+    S.mass = p.mass;
+    S.m = p.m;
+    S.wt = p.wt_fac * s->g.dtheta;
+    BHR_CUDA_TRY(launch_source(S, s->stream));
+  }
+  BHR_CUDA_TRY(mark(1));
+  A.vin = s->u0; A.un = s->u0; A.out = s->u1;
+  BHR_CUDA_TRY(launch_stage(1, s->tq[0], s->tp[0], A, s->stream));
+  BHR_CUDA_TRY(mark(2));
+  A.vin = s->u1; A.un = s->u0; A.out = s->u2;
+  BHR_CUDA_TRY(launch_stage(2, s->tq[1], s->tp[1], A, s->stream));
+  BHR_CUDA_TRY(mark(3));
+  A.vin = s->u2; A.un = s->u0; A.out = s->u0;
+  BHR_CUDA_TRY(launch_stage(3, s->tq[2], s->tp[2], A, s->stream));
+  BHR_CUDA_TRY(mark(4));
+  ExtractArgs E{};
+  E.u = s->u0;
+  E.ext = s->ext;
+  E.integ = s->integ;
+  E.wproj = s->wproj;
+  E.wdedt = s->wdedt;
+  E.rows = s->rows;
+  E.rs = s->rs;
+  E.N = p.N;
+  E.M = p.M;
+  E.ext_col = s->ext_col;
+  E.Fr = s->Fr;
+  E.max_rows = s->max_rows;
+  E.even_m = s->even_m ? 1 : 0;
+  E.dt = p.dt;
+  E.out_start = p.out_start;
+  E.Xmax = p.Xmax;
+  BHR_CUDA_TRY(launch_extract(E, s->stream));
+  BHR_CUDA_TRY(mark(5));
+  return BHR_OK;
+}
+
+static int check_run_state(bhr_solver *s) {
+  RunState rs{};
+  BHR_CUDA_TRY(cudaMemcpyAsync(&rs, s->rs, sizeof(rs), cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  if (rs.err == BHR_NAN_DETECTED) {
+    set_error("non-finite value in the extracted waveform");
+    return BHR_NAN_DETECTED;
+  }
+  if (rs.err == BHR_TIMEOUT) {
+    set_error("a bounded device wait gave up");
+    return BHR_TIMEOUT;
+  }
+  return BHR_OK;
+}
+
+int bhr_solver_step(bhr_solver *s, int nsteps) {
+  if (!s || nsteps < 0) return BHR_INVALID_ARG;
+  BHR_CUDA_TRY(cudaSetDevice(s->p.device));
+  if (s->steps_done + nsteps > s->nt && s->has_source) {
+    set_error("stepping past the end of the trajectory records");
+    return BHR_INVALID_ARG;
+  }
+  for (int i = 0; i < nsteps; i++) {
+    if (int st = launch_step(s)) return st;
+    s->steps_done++;
+  }
+  return check_run_state(s);
+}
+
+int bhr_solver_waveform(bhr_solver *s, double *t, double *h, double *dedt, int max_rows, int *nrows) {
+  if (!s) return BHR_INVALID_ARG;
+  BHR_CUDA_TRY(cudaSetDevice(s->p.device));
+  RunState rs{};
+  BHR_CUDA_TRY(cudaMemcpyAsync(&rs, s->rs, sizeof(rs), cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  const int n = std::min(rs.nrow, std::max(0, max_rows));
+  std::vector<double> buf(static_cast<size_t>(n) * 16);
+  if (n > 0) {
+    BHR_CUDA_TRY(cudaMemcpyAsync(buf.data(), s->rows, buf.size() * 8, cudaMemcpyDeviceToHost, s->stream));
+    BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  }
+  for (int r = 0; r < n; r++) {
+    if (t) t[r] = buf[16 * r];
+    if (h)
+      for (int i = 0; i < 14; i++) h[14 * r + i] = buf[16 * r + 1 + i];
+    if (dedt) dedt[r] = buf[16 * r + 15];
+  }
+  if (nrows) *nrows = n;
+  return BHR_OK;
+}
+
+int bhr_solver_run(bhr_solver *s, const char *out_dir, const char *name) {
+  if (!s) return BHR_INVALID_ARG;
+  const int remaining = s->nt - s->steps_done;
+  const int chunk = 1000;
+  for (int done = 0; done < remaining; done += chunk) {
+    if (int st = bhr_solver_step(s, std::min(chunk, remaining - done))) return st;
+  }
+  if (!out_dir || !name) return BHR_OK;
+  RunState rs{};
+  BHR_CUDA_TRY(cudaMemcpy(&rs, s->rs, sizeof(rs), cudaMemcpyDeviceToHost));
+  std::vector<double> t(rs.nrow), h(static_cast<size_t>(rs.nrow) * 14), e(rs.nrow);
+  int n = 0;
+  if (int st = bhr_solver_waveform(s, t.data(), h.data(), e.data(), rs.nrow, &n)) return st;
+  // File naming as QNM_Extraction's loadwaveforms expects
+  // (QNM_Extraction/Library/ringdownlib.py:49-84): hm<m>_ for m >= 0 and
+  // hmm<|m|>_ for m < 0.
+  const int mi = static_cast<int>(s->p.m);
+  char fname[4096];
+  std::snprintf(fname, sizeof(fname), "%s/%s%d_%s.dat", out_dir, mi < 0 ? "hmm" : "hm", std::abs(mi), name);
+  FILE *f = std::fopen(fname, "w");
+  std::string full = std::string(fname) + ".full";
+  FILE *g = std::fopen(full.c_str(), "w");
+  if (!f || !g) {
+    if (f) std::fclose(f);
+    if (g) std::fclose(g);
+    set_error(std::string("cannot write ") + fname);
+    return BHR_IO_ERROR;
+  }
+  for (int r = 0; r < n; r++) {
+    // HighOrder/body.cu:208: "%lf" time then 14 "%g" values.
+    std::fprintf(f, "%lf", t[r]);
+    for (int i = 0; i < 14; i++) std::fprintf(f, " %g", h[14 * r + i]);
+    std::fprintf(f, "\n");
+    std::fprintf(g, "%.17g", t[r]);
+    for (int i = 0; i < 14; i++) std::fprintf(g, " %.17g", h[14 * r + i]);
+    std::fprintf(g, " %.17g\n", e[r]);
+  }
+  std::fclose(f);
+  std::fclose(g);
+  return BHR_OK;
+}
+
+int bhr_solver_get_state(bhr_solver *s, double *qre, double *qim, double *pre, double *pim) {
+  if (!s) return BHR_INVALID_ARG;
+  BHR_CUDA_TRY(cudaSetDevice(s->p.device));
+  const size_t NM = static_cast<size_t>(s->p.N) * s->p.M;
+  BHR_CUDA_TRY(launch_closure(s->u0, s->p.N, s->p.M, s->even_m ? 1 : 0, s->stream));
+  double *outs[4] = {qre, qim, pre, pim};
+  for (int f = 0; f < 4; f++)
+    if (outs[f]) BHR_CUDA_TRY(cudaMemcpyAsync(outs[f], s->u0 + f * NM, NM * 8, cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return BHR_OK;
+}
+
+int bhr_solver_set_state(bhr_solver *s, const double *qre, const double *qim, const double *pre, const double *pim) {
+  if (!s) return BHR_INVALID_ARG;
+  BHR_CUDA_TRY(cudaSetDevice(s->p.device));
+  const size_t NM = static_cast<size_t>(s->p.N) * s->p.M;
+  const double *ins[4] = {qre, qim, pre, pim};
+  for (int f = 0; f < 4; f++) {
+    if (ins[f]) BHR_CUDA_TRY(cudaMemcpyAsync(s->u0 + f * NM, ins[f], NM * 8, cudaMemcpyHostToDevice, s->stream));
+    else BHR_CUDA_TRY(cudaMemsetAsync(s->u0 + f * NM, 0, NM * 8, s->stream));
+  }
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return BHR_OK;
+}
+
+int bhr_solver_get_extraction(bhr_solver *s, double *psi_re, double *psi_im, double *int_re, double *int_im,
+                              double *dint_re, double *dint_im) {
+  if (!s) return BHR_INVALID_ARG;
+  BHR_CUDA_TRY(cudaSetDevice(s->p.device));
+  const int M = s->p.M;
+  std::vector<double> e(2 * M), in(4 * M);
+  BHR_CUDA_TRY(cudaMemcpyAsync(e.data(), s->ext, e.size() * 8, cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaMemcpyAsync(in.data(), s->integ, in.size() * 8, cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  double *outs[6] = {psi_re, psi_im, int_re, int_im, dint_re, dint_im};
+  const double *srcs[6] = {e.data(), e.data() + M, in.data(), in.data() + M, in.data() + 2 * M, in.data() + 3 * M};
+  for (int i = 0; i < 6; i++)
+    if (outs[i]) std::memcpy(outs[i], srcs[i], M * 8);
+  return BHR_OK;
+}
+
+int bhr_solver_get_source(bhr_solver *s, double *tre, double *tim) {
+  if (!s || !tre || !tim) return BHR_INVALID_ARG;
+  BHR_CUDA_TRY(cudaSetDevice(s->p.device));
+  const bhr_params &p = s->p;
+  const size_t NM = static_cast<size_t>(p.N) * p.M;
+  std::memset(tre, 0, NM * 8);
+  std::memset(tim, 0, NM * 8);
+  if (!s->has_source) return BHR_OK;
+  RunState rs{};
+  BHR_CUDA_TRY(cudaMemcpyAsync(&rs, s->rs, sizeof(rs), cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  if (rs.k <= 0) return BHR_OK;
+  StepRec rec{};
+  std::vector<double> patch(2 * static_cast<size_t>(p.PTSX) * p.PTSY);
+  BHR_CUDA_TRY(cudaMemcpyAsync(&rec, s->recs + (rs.k - 1), sizeof(rec), cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaMemcpyAsync(patch.data(), s->src, patch.size() * 8, cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  for (int j = 0; j < p.PTSY; j++) {
+    const int row = rec.row0 + j;
+    if (row < 0 || row >= p.M) continue;
+    for (int k = 0; k < p.PTSX; k++) {
+      const int col = rec.col0 + k;
+      if (col < 0 || col >= p.N) continue;
+      tre[static_cast<size_t>(row) * p.N + col] = patch[static_cast<size_t>(j) * p.PTSX + k];
+      tim[static_cast<size_t>(row) * p.N + col] = patch[static_cast<size_t>(p.PTSY + j) * p.PTSX + k];
+    }
+  }
+  return BHR_OK;
+}
+
+void *bhr_solver_stream(bhr_solver *s) { return s ? static_cast<void *>(s->stream) : nullptr; }
+
+int bhr_solver_profile(bhr_solver *s, int nsteps, double *avg_ms5, double *total_ms) {
+  if (!s || nsteps <= 0) return BHR_INVALID_ARG;
+  BHR_CUDA_TRY(cudaSetDevice(s->p.device));
+  if (s->has_source && s->steps_done + nsteps > s->nt) {
+    set_error("profiling past the end of the trajectory records");
+    return BHR_INVALID_ARG;
+  }
+  // Events bracket each launch of launch_step on the solver stream.
+  std::vector<cudaEvent_t> ev(6 * static_cast<size_t>(nsteps));
+  for (auto &e : ev) BHR_CUDA_TRY(cudaEventCreate(&e));
+  double sums[5] = {0, 0, 0, 0, 0};
+  cudaEvent_t t0, t1;
+  BHR_CUDA_TRY(cudaEventCreate(&t0));
+  BHR_CUDA_TRY(cudaEventCreate(&t1));
+  BHR_CUDA_TRY(cudaEventRecord(t0, s->stream));
+  for (int i = 0; i < nsteps; i++) {
+    if (int st = launch_step(s, &ev[6 * static_cast<size_t>(i)])) return st;
+    s->steps_done++;
+  }
+  BHR_CUDA_TRY(cudaEventRecord(t1, s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  for (int i = 0; i < nsteps; i++) {
+    cudaEvent_t *e = &ev[6 * static_cast<size_t>(i)];
+    for (int j = 0; j < 5; j++) {
+      float ms = 0.f;
+      BHR_CUDA_TRY(cudaEventElapsedTime(&ms, e[j], e[j + 1]));
+      sums[j] += ms;
+    }
+  }
+  float tot = 0.f;
+  BHR_CUDA_TRY(cudaEventElapsedTime(&tot, t0, t1));
+  for (auto &e : ev) cudaEventDestroy(e);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  if (avg_ms5)
+    for (int j = 0; j < 5; j++) avg_ms5[j] = sums[j] / nsteps;
+  if (total_ms) *total_ms = tot;
+  return check_run_state(s);
+}
+
+}  // extern "C"

@@ -1,0 +1,83 @@
+"""Trajectory files: the 10-column .traj format and a synthetic plunge.
+
+The reference takes its source worldline from GenOT
+(GenOT/README:113-123: columns t r theta dr/dt dtheta/dt dphi/dt phi E Lz
+Q).  GenOT's adiabatic inspiral inputs are not part of the reference tree,
+so workloads here use a stand-in: a prograde equatorial Kerr geodesic that
+starts just inside the ISCO with the ISCO energy and angular momentum and
+plunges; it is integrated in Boyer-Lindquist time with RK4 and sampled on a
+uniform time grid (body.cu consumes two rows per step, so a run with step
+dt wants rows every dt/2).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def read_traj(path: str) -> np.ndarray:
+    rows = np.loadtxt(path, dtype=np.float64, ndmin=2)
+    if rows.shape[1] != 10:
+        raise ValueError(f"{path}: expected 10 columns, found {rows.shape[1]}")
+    return rows
+
+
+def write_traj(path: str, rows: np.ndarray) -> None:
+    np.savetxt(path, rows, fmt="%.18e")
+
+
+def isco_prograde(a: float, mass: float = 1.0):
+    """ISCO radius, specific energy and angular momentum (Bardeen, Press,
+    Teukolsky 1972) for prograde equatorial orbits."""
+    a = a / mass
+    z1 = 1 + (1 - a * a) ** (1 / 3) * ((1 + a) ** (1 / 3) + (1 - a) ** (1 / 3))
+    z2 = np.sqrt(3 * a * a + z1 * z1)
+    r = 3 + z2 - np.sqrt((3 - z1) * (3 + z1 + 2 * z2))
+    v = 1 / np.sqrt(r)
+    den = np.sqrt(1 - 3 * v * v + 2 * a * v ** 3)
+    E = (1 - 2 * v * v + a * v ** 3) / den
+    L = np.sqrt(r) * (1 - 2 * a * v ** 3 + a * a * v ** 4) / den
+    return r * mass, E, L * mass
+
+
+def _rhs(y, a, E, L):
+    """d/dt of (r, phi) on an equatorial plunge (M = 1), r decreasing."""
+    r = y[0]
+    D = r * r - 2 * r + a * a
+    P = E * (r * r + a * a) - a * L
+    R = P * P - D * (r * r + (L - a * E) ** 2)
+    tdot = ((r * r + a * a) / D * P - a * (a * E - L)) / (r * r)
+    phidot = (a / D * P - (a * E - L)) / (r * r)
+    rdot = -np.sqrt(max(R, 0.0)) / (r * r)
+    return np.array([rdot / tdot, phidot / tdot])
+
+
+def synthetic_plunge(a: float, dt_row: float, duration: float, r_offset: float = 0.05,
+                     r_stop_above_horizon: float = 0.02) -> np.ndarray:
+    """Rows of a prograde equatorial plunge starting at r_isco - r_offset.
+
+    Sampled every dt_row in BL time for `duration`, or until r comes within
+    r_stop_above_horizon of r+; after that the file simply ends (a reader
+    past the end keeps the last row, as the reference's fscanf loop does).
+    """
+    r_isco, E, L = isco_prograde(a)
+    r_plus = 1 + np.sqrt(1 - a * a)
+    y = np.array([r_isco - r_offset, 0.0])
+    sub = 8
+    h = dt_row / sub
+    rows = []
+    t = 0.0
+    n = int(np.floor(duration / dt_row)) + 1
+    for i in range(n):
+        r, phi = y
+        if r < r_plus + r_stop_above_horizon:
+            break
+        rdot, phidot = _rhs(y, a, E, L)
+        rows.append((t, r, np.pi / 2, rdot, 0.0, phidot, phi, E, L, 0.0))
+        for _ in range(sub):
+            k1 = _rhs(y, a, E, L)
+            k2 = _rhs(y + 0.5 * h * k1, a, E, L)
+            k3 = _rhs(y + 0.5 * h * k2, a, E, L)
+            k4 = _rhs(y + h * k3, a, E, L)
+            y = y + h / 6 * (k1 + 2 * k2 + 2 * k3 + k4)
+        t = (i + 1) * dt_row
+    return np.array(rows, dtype=np.float64)

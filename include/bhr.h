@@ -1,0 +1,173 @@
+/*
+ * bhr.h -- C ABI of bh_ringdown_b200, a B200-native time-domain Teukolsky
+ * solver that replaces the reference TD_GPU_code/HighOrder path.
+ *
+ * The reference has no library interface.  Its boundary is the C call
+ *   void body(double *r_c, double *theta, double dtheta, double mass,
+ *             double aa, double ss, double mm, double dx, double dt,
+ *             int p, int my_rank)                  (HighOrder/body.cu:25-27)
+ * driven by main() (HighOrder/main.c:40-77) with the grid and run knobs as
+ * compile-time macros (HighOrder/parm.h:1-13), a .traj text file as source
+ * input (HighOrder/body.cu:77,97-120) and hm*.dat files as output
+ * (HighOrder/body.cu:63-78,204-212).  The entry points below cover that
+ * call and its inputs and outputs; each comment names what it replaces.
+ *
+ * Conventions: plain C types only; the library owns all device memory and
+ * streams; callers own host buffers.  Every call returns a bhr_status
+ * (0 = OK); bhr_last_error_string() describes the last failure on the
+ * calling thread.  No call exits the process or traps on the device.
+ * Field arrays are row-major M x N doubles, idx(b,a) = N*b + a as in
+ * HighOrder/parm.h:13 (theta rows b, radial columns a).
+ */
+#ifndef BHR_H
+#define BHR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BHR_ABI_VERSION 1
+
+typedef enum bhr_status {
+  BHR_OK = 0,
+  BHR_INVALID_ARG = 1,   /* bad parameter or size                          */
+  BHR_OUT_OF_MEMORY = 2, /* device allocation failed or over budget        */
+  BHR_CUDA_ERROR = 3,    /* a CUDA runtime call failed                     */
+  BHR_NAN_DETECTED = 4,  /* non-finite value in the extracted waveform     */
+  BHR_TIMEOUT = 5,       /* a bounded device wait gave up                  */
+  BHR_IO_ERROR = 6,      /* file could not be read or written              */
+  BHR_NO_DEVICE = 7      /* no CUDA device available                       */
+} bhr_status;
+
+typedef enum bhr_integrator { BHR_SSPRK3 = 0 } bhr_integrator;
+typedef enum bhr_precision { BHR_FP64 = 0, BHR_MIXED = 1 } bhr_precision;
+typedef enum bhr_init_kind { BHR_INIT_ZERO = 0, BHR_INIT_GAUSSIAN = 1 } bhr_init_kind;
+
+/* Run parameters.  Replaces HighOrder/parm.h:1-13 (N, M, Xmax, Xmin, Fr, T,
+ * PTSX, PTSY) and the constants of HighOrder/main.c:55-61 (mass, aa, ss,
+ * dt) plus the m loop of HighOrder/main.c:65.  s = -2 is fixed, as in the
+ * reference's coefficient formulas (HighOrder/kern.cu:142). */
+typedef struct bhr_params {
+  int N;              /* radial points (multiple of 64)                      */
+  int M;              /* theta points (multiple of 16, >= 16)                */
+  double Xmin, Xmax;  /* grid coordinate extent                              */
+  double mass;        /* black-hole mass                                     */
+  double a;           /* spin parameter                                      */
+  double m;           /* azimuthal number                                    */
+  double dt;          /* time step; <= 0 selects the Courant rule below      */
+  double courant;     /* dt = courant*min(dx, r_c[0]*dtheta), then shrunk so
+                         out_every/dt is an integer when out_every > 0       */
+  double out_every;   /* output spacing in time for the Courant rule (0: none) */
+  double T;           /* final time                                          */
+  int Fr;             /* waveform row every Fr steps (0: from out_every)     */
+  double out_start;   /* rows written once k*dt >= out_start (ref: Xmax+200) */
+  int ext_col;        /* extraction column, -1 = N-1 (ref)                   */
+  int PTSX, PTSY;     /* particle source patch (ref 128 x 128)               */
+  double wr_fac;      /* wr = wr_fac*dx*(1 - r+/rp), ref 2                   */
+  double wt_fac;      /* wt = wt_fac*dtheta, ref 6                           */
+  int integrator;     /* bhr_integrator                                      */
+  int precision;      /* bhr_precision                                       */
+  int init_kind;      /* bhr_init_kind                                       */
+  double init_center; /* Gaussian initial data psi = exp(-(x-c)^2/(2 w^2))   */
+  double init_width;  /*   * swsh(l, m, theta), Pi = 0                       */
+  double init_ell;
+  int device;         /* CUDA device ordinal                                 */
+} bhr_params;
+
+/* Fills the reference's defaults (HighOrder/parm.h, HighOrder/main.c):
+ * N=16000, M=256, Xmin=-50, Xmax=50, mass=1, a=1e-8, m=2, dt=0.002, T=1500,
+ * Fr=50, out_start=Xmax+200, PTSX=PTSY=128, wr_fac=2, wt_fac=6. */
+int bhr_params_default(bhr_params *p);
+
+/* One particle state as HighOrder/body.cu:112-124 passes it to sourced(). */
+typedef struct bhr_particle {
+  double rp, tp, phip, E, lz, Q;
+  double drdt, d2rdt2, d3rdt3;
+  double dthdt, d2thdt2, d3thdt3;
+  double dphidt, d2phidt2;
+} bhr_particle;
+
+typedef struct bhr_info {
+  int N, M;
+  double dx, dtheta, dt;
+  int nt;             /* steps of a full run                                 */
+  int Fr;
+  int steps_done;
+  int rows_done;      /* waveform rows produced so far                       */
+  int has_source;
+  double r_plus;
+  size_t device_bytes;
+} bhr_info;
+
+typedef struct bhr_solver bhr_solver;
+
+/* Grid of HighOrder/main.c:79-198 (x_c[N], r_c[N], theta[M]); host only. */
+int bhr_grid(const bhr_params *p, double *x_c, double *r_c, double *theta);
+
+/* Creates a solve: grid, coefficient tables, fields, initial data on the
+ * device.  Replaces the set-up half of body() (HighOrder/body.cu:30-60)
+ * and kernel_init (HighOrder/kern.cu:84-169). */
+int bhr_solver_create(const bhr_params *p, bhr_solver **out);
+void bhr_solver_destroy(bhr_solver *s);
+int bhr_solver_info(const bhr_solver *s, bhr_info *info);
+
+/* Trajectory input: rows of the 10 .traj columns t r theta dr/dt dtheta/dt
+ * dphi/dt phi E Lz Q (row-major, nrows x 10).  The data are copied in.
+ * Replaces the fopen/fscanf consumption of HighOrder/body.cu:77,97-120. */
+int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows);
+int bhr_solver_load_trajectory(bhr_solver *s, const char *path);
+
+/* Advances nsteps full time steps (source, three SSP-RK3 stages with
+ * closures, extraction, time integration, waveform rows on output steps).
+ * Replaces one pass of the loop at HighOrder/body.cu:105-215. */
+int bhr_solver_step(bhr_solver *s, int nsteps);
+/* Runs to the final time and, when path_prefix is not NULL, writes
+ * <dir>/hm0<m>_<name>.dat or hmm<|m|>_<name>.dat in the reference format
+ * (HighOrder/body.cu:63-70,208) plus a %.17g companion <file>.full.
+ * Replaces the whole of body(). */
+int bhr_solver_run(bhr_solver *s, const char *out_dir, const char *name);
+
+/* Waveform rows produced so far: t[r] (= timer - Xmax), h[r*14 + 2l] = h+
+ * and h[r*14+2l+1] = hx for l = |m|+0..6, dedt[r] (HighOrder/body.cu:
+ * 174-212).  Any output pointer may be NULL. */
+int bhr_solver_waveform(bhr_solver *s, double *t, double *h, double *dedt, int max_rows, int *nrows);
+
+/* Field access for checks: full M x N planes with the boundary closure
+ * applied (what the reference holds after kernel_boundary2b). */
+int bhr_solver_get_state(bhr_solver *s, double *qre, double *qim, double *pre, double *pim);
+int bhr_solver_set_state(bhr_solver *s, const double *qre, const double *qim, const double *pre,
+                         const double *pim);
+/* psi at the extraction column after the last step (d_qre_buff/d_qim_buff
+ * of HighOrder/kern.cu:750-751) and the running integrals int/dint of
+ * HighOrder/body.cu:178-186. */
+int bhr_solver_get_extraction(bhr_solver *s, double *psi_re, double *psi_im, double *int_re, double *int_im,
+                              double *dint_re, double *dint_im);
+/* Source planes (tred/timd of HighOrder/kern.cu:15-16) for the current step
+ * as the device built them (zero off the patch). */
+int bhr_solver_get_source(bhr_solver *s, double *tre, double *tim);
+
+/* Device stream the solver launches on (a cudaStream_t). */
+void *bhr_solver_stream(bhr_solver *s);
+/* Times nsteps steps on the solver stream with CUDA events; per-kernel
+ * average durations in ms for: source, stage1, stage2, stage3, extract. */
+int bhr_solver_profile(bhr_solver *s, int nsteps, double *avg_ms5, double *total_ms);
+
+/* The particle-only bilinear coefficients of the point-particle source:
+ * C[k] multiplies DelR^(i) DelTH^(j) for (i,j) = (0,0) (0,1) (0,2) (1,0)
+ * (1,1) (2,0).  Replaces the Maple block of HighOrder/kern.cu:1229-2664. */
+int bhr_source_coefficients(const bhr_particle *pt, double a, double mass, double m, double *c_re6,
+                            double *c_im6);
+
+/* Spin-weighted spherical harmonic of HighOrder/proj.c:16-35 (s = -2). */
+double bhr_swsh(double ell, double m, double theta);
+
+const char *bhr_last_error_string(void);
+int bhr_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

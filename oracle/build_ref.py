@@ -1,0 +1,99 @@
+"""Build recipe for oracle/_ref: the reference's own HighOrder code on CPU.
+
+TEST INFRASTRUCTURE ONLY.  For each grid tag this script makes a folder
+oracle/_ref/<tag>/ holding symlinks to the reference sources where they lie
+(TD_GPU_code/HighOrder/{kern.cu,mycmplx.h,main.c,proj.c}) and a grid header
+parm.h with the tag's N, M, Xmin, Xmax (the reference fixes these at compile
+time in HighOrder/parm.h:1-13; the "ho" tag links the reference's own
+parm.h unchanged).  It then compiles them with oracle/ref_emu/ into
+oracle/_ref/libref_<tag>.so.  Nothing is copied out of the reference tree
+and nothing is written outside oracle/_ref/.
+
+Usage: python oracle/build_ref.py [--ref /root/reference] [tag ...]
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+EMU = os.path.join(HERE, "ref_emu")
+
+# Grid tags: (N, M, Xmin, Xmax) or None for the reference's own parm.h.
+TAGS = {
+    "ho": None,                           # 16000 x 256 on [-50, 50]
+    "pin": (256, 32, -50.0, 50.0),        # small reference-domain pin grid
+    "c1s": (512, 64, -100.0, 300.0),      # config-1 domain, reduced grid
+    "cfg2": (8192, 128, -200.0, 600.0),   # plunge-ringdown workload grid
+}
+DEFAULT_TAGS = ("pin", "c1s", "cfg2")
+
+# main.c defines globals with the same names as kern.cu's device scalars;
+# they are renamed at compile time so both link into one library.
+MAIN_RENAMES = ["mass", "aa", "ss", "mm", "dx", "dtheta", "timer", "dt", "delta"]
+
+
+def grid_header(n: int, m: int, xmin: float, xmax: float) -> str:
+    return (
+        f"#define N {n}\n#define M {m}\n#define Xmax {xmax!r}\n#define Xmin {xmin!r}\n"
+        "#define Text 90.0\n#define Nd 100\n#define Fr 50\n#define T  1500.0\n"
+        "#define PTSX 128\n#define PTSY 128\n#define Pi 3.14159265358979\n"
+        "#define idx(b,a) (N*(b)+(a))\n"
+    )
+
+
+def run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+
+
+def build_tag(ref_root: str, tag: str) -> str:
+    ho = os.path.join(ref_root, "TD_GPU_code", "HighOrder")
+    d = os.path.join(OUT, tag)
+    os.makedirs(d, exist_ok=True)
+    names = ["kern.cu", "mycmplx.h", "main.c", "proj.c"] + (["parm.h"] if TAGS[tag] is None else [])
+    for name in names:
+        link = os.path.join(d, name)
+        if os.path.lexists(link):
+            os.remove(link)
+        os.symlink(os.path.join(ho, name), link)
+    if TAGS[tag] is not None:
+        with open(os.path.join(d, "parm.h"), "w") as f:
+            f.write(grid_header(*TAGS[tag]))
+    lib = os.path.join(OUT, f"libref_{tag}.so")
+    drv_o, main_o, proj_o = (os.path.join(d, x) for x in ("driver.o", "main.o", "proj.o"))
+    run(["g++", "-O2", "-fopenmp", "-fPIC", "-w", "-std=c++17", "-include", os.path.join(EMU, "prelude.h"),
+         "-I", d, "-c", os.path.join(EMU, "ref_driver.cpp"), "-o", drv_o])
+    defs = [f"-D{v}=hmc_{v}" for v in MAIN_RENAMES] + ["-Dmain=hmc_main", "-Dbody=hmc_body"]
+    run(["gcc", "-O2", "-fPIC", "-w", *defs, "-c", os.path.join(d, "main.c"), "-o", main_o])
+    run(["gcc", "-O2", "-fPIC", "-w", "-c", os.path.join(d, "proj.c"), "-o", proj_o])
+    run(["g++", "-shared", "-fopenmp", "-o", lib, drv_o, main_o, proj_o, "-lm"])
+    return lib
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default=os.environ.get("BHR_REFERENCE_ROOT", "/root/reference"))
+    ap.add_argument("tags", nargs="*", default=list(DEFAULT_TAGS))
+    args = ap.parse_args(argv)
+    if not os.path.isdir(os.path.join(args.ref, "TD_GPU_code", "HighOrder")):
+        print(f"build_ref: reference not found at {args.ref}; skipping", file=sys.stderr)
+        return 0
+    bad = [t for t in args.tags if t not in TAGS]
+    if bad:
+        print(f"unknown tags {bad}; known {sorted(TAGS)}", file=sys.stderr)
+        return 2
+    os.makedirs(OUT, exist_ok=True)
+    with ThreadPoolExecutor(max_workers=len(args.tags)) as ex:
+        for lib in ex.map(lambda t: build_tag(args.ref, t), args.tags):
+            print("built", os.path.relpath(lib, os.path.dirname(HERE)))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
