@@ -66,19 +66,85 @@ def test_waveform_rows_match_oracle(m):
     assert np.linalg.norm(es - dedt) <= WAVE_TOL * np.linalg.norm(dedt)
 
 
-def test_config1_domain_reduced_length_waveform():
-    """Config-1 grid (1024 x 64 on [-100, 300], a=0.5, m=2, dt from the
-    Courant rule rounded to 0.5M outputs) with extraction at the column
-    nearest x=250, for the first 20M."""
+def test_config1_full_length_waveform():
+    """Config 1 at full size and length: 1024 x 64 on [-100, 300], a=0.5,
+    m=2, dt from the Courant rule rounded so 0.5M outputs are whole steps,
+    psi0 = exp(-(x-20)^2/8) swsh(2,2), extraction at the column nearest
+    x=250, T=300."""
     N, M, Xmin, Xmax = 1024, 64, -100.0, 300.0
     x = Xmin + np.arange(N) * (Xmax - Xmin) / N
     col = int(np.argmin(np.abs(x - 250.0)))
     s, o, info = pair(N, M, Xmin, Xmax, 0.5, 2.0, center=20.0, width=2.0, ell=2.0, T=300.0, ext_col=col,
                       courant=0.25, out_every=0.5)
-    nsteps = int(round(20.0 / info["dt"]))
+    nsteps = info["nt"]
     s.step(nsteps)
     t, h, dedt, steps, _, _ = o.run(nsteps=nsteps)
     ts, hs, es = s.waveform()
     assert np.array_equal(ts, t)
     assert np.linalg.norm(hs - h) <= WAVE_TOL * np.linalg.norm(h)
     assert rel_field_err(s.get_state(), o.get_state()) <= FIELD_TOL * 10
+
+
+def traj_pair(N, M, Xmin, Xmax, a, m, Fr=5, T=100.0, PTSX=128, PTSY=128):
+    from bh_ringdown_b200.trajectory import synthetic_plunge
+    from tests.test_source import product_coef_fn
+    dt = 0.25 * (Xmax - Xmin) / N
+    prm = bhr.Params(N=N, M=M, Xmin=Xmin, Xmax=Xmax, a=a, m=m, dt=dt, Fr=Fr, T=T, out_start=0.0,
+                     PTSX=PTSX, PTSY=PTSY)
+    rows = synthetic_plunge(a, dt / 2.0, duration=T)
+    s = bhr.Solver(prm)
+    s.set_trajectory(rows)
+    o = pyoracle.Oracle(N, M, Xmin, Xmax, a, m, dt, T=T, Fr=Fr, out_start=0.0, PTSX=PTSX, PTSY=PTSY)
+    return s, o, rows, product_coef_fn()
+
+
+@pytest.mark.parametrize("a,m", [(0.6, 2.0), (0.9, -3.0)])
+def test_plunge_sourced_run_matches_oracle(a, m):
+    """Source from a plunge worldline: trajectory cursor (two rows per step,
+    rp + 1e-6, backward-difference accelerations), patch placement, Gaussian
+    approximants, tilde-phi phase, turn-on, and the evolution it drives."""
+    s, o, rows, coef = traj_pair(256, 32, -50.0, 50.0, a, m)
+    n = 300
+    s.step(1)
+    o.run(traj=rows, coef_fn=coef, nsteps=1, max_rows=10)
+    gt, gi = s.get_source()
+    ot, oi = o.get_source()
+    scale = np.max(np.abs(ot + 1j * oi))
+    assert scale > 0
+    assert np.max(np.abs((gt + 1j * gi) - (ot + 1j * oi))) <= 1e-12 * scale
+    # continue: the oracle restarts its cursor, so run both from scratch
+    s2, o2, rows, coef = traj_pair(256, 32, -50.0, 50.0, a, m)
+    s2.step(n)
+    t, h, dedt, steps, _, _ = o2.run(traj=rows, coef_fn=coef, nsteps=n)
+    ts, hs, es = s2.waveform()
+    assert np.array_equal(ts, t)
+    assert rel_field_err(s2.get_state(), o2.get_state()) <= FIELD_TOL
+    assert np.linalg.norm(hs - h) <= WAVE_TOL * np.linalg.norm(h)
+
+
+def test_source_patch_clipped_at_the_grid_edge():
+    """Patch columns at or past N are dropped (the reference writes past the
+    row end there); the grid is narrow enough that the 128-wide patch of a
+    particle near r=3.5 reaches past column N-1."""
+    s, o, rows, coef = traj_pair(128, 16, -50.0, 50.0, 0.6, 2.0)
+    s.step(5)
+    o.run(traj=rows, coef_fn=coef, nsteps=5, max_rows=10)
+    assert rel_field_err(s.get_state(), o.get_state()) <= FIELD_TOL
+
+
+def test_headline_workload_grid_matches_oracle():
+    """The benchmark workload at full size: 8192 x 128 on [-200, 600],
+    a=0.9, m=2, plunge source; 40 steps on both paths."""
+    from bh_ringdown_b200.trajectory import synthetic_plunge
+    from tests.test_source import product_coef_fn
+    N, M, Xmin, Xmax, a, m = 8192, 128, -200.0, 600.0, 0.9, 2.0
+    x, r, th = bhr.grid(bhr.Params(N=N, M=M, Xmin=Xmin, Xmax=Xmax, a=a))
+    dt = 0.25 * min((Xmax - Xmin) / N, r[0] * np.pi / M)
+    prm = bhr.Params(N=N, M=M, Xmin=Xmin, Xmax=Xmax, a=a, m=m, dt=dt, Fr=10, T=1000.0, out_start=0.0)
+    rows = synthetic_plunge(a, dt / 2.0, duration=5.0)
+    s = bhr.Solver(prm)
+    s.set_trajectory(rows)
+    o = pyoracle.Oracle(N, M, Xmin, Xmax, a, m, dt, T=1000.0, Fr=10, out_start=0.0)
+    s.step(40)
+    o.run(traj=rows, coef_fn=product_coef_fn(), nsteps=40, max_rows=10)
+    assert rel_field_err(s.get_state(), o.get_state()) <= FIELD_TOL
