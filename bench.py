@@ -183,24 +183,30 @@ def run_ours(args, rank, local_rank, world):
         solver.set_trajectory(rows)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    def one_step():
+    def flush_l2():
         flush.zero_()
         torch.cuda.synchronize()
-        avg, tot = solver.profile(1)
-        return avg, tot
 
+    # warm-up, then the timed steps: each step is one captured-graph launch
+    # bracketed by CUDA events on the solver stream, with L2 flushed before it
     for _ in range(args.warmup):
-        one_step()
+        flush_l2()
+        solver.time_steps(1)
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
-    per_kernel = np.zeros(5)
     total_ms = 0.0
     with ClockSampler(local_rank) as clk:
         for _ in range(args.steps):
-            avg, tot = one_step()
-            per_kernel += avg
-            total_ms += tot
+            flush_l2()
+            total_ms += solver.time_steps(1)
+    torch.cuda.synchronize()
+    # per-kernel breakdown (eager launches, events around each kernel)
+    per_kernel = np.zeros(5)
+    for _ in range(args.steps):
+        flush_l2()
+        avg, _tot = solver.profile(1)
+        per_kernel += avg
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()

@@ -130,6 +130,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "bhr_solver_get_source": (I, [vp, dp, dp]),
         "bhr_solver_stream": (vp, [vp]),
         "bhr_solver_profile": (I, [vp, I, dp, dp]),
+        "bhr_solver_time_steps": (I, [vp, I, dp]),
         "bhr_source_coefficients": (I, [P(Particle), D, D, D, dp, dp]),
         "bhr_swsh": (D, [D, D, D]),
     }
@@ -254,6 +255,12 @@ class Solver:
 
     def stream(self) -> int:
         return int(self.lib.bhr_solver_stream(self._h) or 0)
+
+    def time_steps(self, nsteps: int) -> float:
+        """Advance nsteps (captured CUDA graphs) and return their device time in ms."""
+        ms = np.zeros(1)
+        _check(self.lib.bhr_solver_time_steps(self._h, int(nsteps), _ptr(ms)))
+        return float(ms[0])
 
     def profile(self, nsteps: int):
         avg, tot = np.zeros(5), np.zeros(1)

@@ -53,7 +53,11 @@ struct bhr_solver {
   size_t bytes = 0;
   CUtensorMap tq[3], tp[3];
   int steps_done = 0;
+  // Captured step graphs: one step, and kGraphBatch steps in one launch.
+  cudaGraphExec_t g1 = nullptr, gb = nullptr;
 };
+
+static constexpr int kGraphBatch = 16;
 
 namespace {
 
@@ -102,6 +106,9 @@ void free_all(bhr_solver *s) {
                   s->integ, s->wproj, s->wdedt, s->rows, s->recs, s->rs};
   for (void *q : ptrs)
     if (q) cudaFree(q);
+  if (s->g1) cudaGraphExecDestroy(s->g1);
+  if (s->gb) cudaGraphExecDestroy(s->gb);
+  s->g1 = s->gb = nullptr;
   if (s->stream) cudaStreamDestroy(s->stream);
 }
 
@@ -474,6 +481,48 @@ static int check_run_state(bhr_solver *s) {
   return BHR_OK;
 }
 
+// Captures `count` steps of launch_step into an executable graph.  Every
+// launch argument is fixed per solve; what changes from step to step (the
+// step index, the timer, the source record) is read on the device from
+// RunState, so one captured graph replays any step.
+static int capture_steps(bhr_solver *s, int count, cudaGraphExec_t *out) {
+  cudaGraph_t g = nullptr;
+  BHR_CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  int st = BHR_OK;
+  for (int i = 0; i < count && st == BHR_OK; i++) st = launch_step(s);
+  cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+  if (st != BHR_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+    return BHR_CUDA_ERROR;
+  }
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    return BHR_CUDA_ERROR;
+  }
+  return BHR_OK;
+}
+
+static int enqueue_steps(bhr_solver *s, int nsteps) {
+  if (!s->g1)
+    if (int st = capture_steps(s, 1, &s->g1)) return st;
+  if (nsteps >= kGraphBatch && !s->gb)
+    if (int st = capture_steps(s, kGraphBatch, &s->gb)) return st;
+  int left = nsteps;
+  while (left >= kGraphBatch) {
+    BHR_CUDA_TRY(cudaGraphLaunch(s->gb, s->stream));
+    left -= kGraphBatch;
+  }
+  while (left-- > 0) BHR_CUDA_TRY(cudaGraphLaunch(s->g1, s->stream));
+  s->steps_done += nsteps;
+  return BHR_OK;
+}
+
 int bhr_solver_step(bhr_solver *s, int nsteps) {
   if (!s || nsteps < 0) return BHR_INVALID_ARG;
   BHR_CUDA_TRY(cudaSetDevice(s->p.device));
@@ -481,10 +530,34 @@ int bhr_solver_step(bhr_solver *s, int nsteps) {
     set_error("stepping past the end of the trajectory records");
     return BHR_INVALID_ARG;
   }
-  for (int i = 0; i < nsteps; i++) {
-    if (int st = launch_step(s)) return st;
-    s->steps_done++;
+  if (int st = enqueue_steps(s, nsteps)) return st;
+  return check_run_state(s);
+}
+
+int bhr_solver_time_steps(bhr_solver *s, int nsteps, double *ms) {
+  if (!s || nsteps < 0 || !ms) return BHR_INVALID_ARG;
+  BHR_CUDA_TRY(cudaSetDevice(s->p.device));
+  if (s->steps_done + nsteps > s->nt && s->has_source) {
+    set_error("stepping past the end of the trajectory records");
+    return BHR_INVALID_ARG;
   }
+  if (!s->g1)
+    if (int st = capture_steps(s, 1, &s->g1)) return st;
+  if (nsteps >= kGraphBatch && !s->gb)
+    if (int st = capture_steps(s, kGraphBatch, &s->gb)) return st;
+  cudaEvent_t e0, e1;
+  BHR_CUDA_TRY(cudaEventCreate(&e0));
+  BHR_CUDA_TRY(cudaEventCreate(&e1));
+  BHR_CUDA_TRY(cudaEventRecord(e0, s->stream));
+  const int st = enqueue_steps(s, nsteps);
+  BHR_CUDA_TRY(cudaEventRecord(e1, s->stream));
+  BHR_CUDA_TRY(cudaEventSynchronize(e1));
+  float f = 0.f;
+  BHR_CUDA_TRY(cudaEventElapsedTime(&f, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = f;
+  if (st) return st;
   return check_run_state(s);
 }
 

@@ -149,6 +149,10 @@ int bhr_solver_get_extraction(bhr_solver *s, double *psi_re, double *psi_im, dou
  * as the device built them (zero off the patch). */
 int bhr_solver_get_source(bhr_solver *s, double *tre, double *tim);
 
+/* Advances nsteps steps like bhr_solver_step and reports the device time
+ * between CUDA events recorded on the solver stream around them. */
+int bhr_solver_time_steps(bhr_solver *s, int nsteps, double *ms);
+
 /* Device stream the solver launches on (a cudaStream_t). */
 void *bhr_solver_stream(bhr_solver *s);
 /* Times nsteps steps on the solver stream with CUDA events; per-kernel
