@@ -133,6 +133,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "bhr_solver_time_steps": (I, [vp, I, dp]),
         "bhr_source_coefficients": (I, [P(Particle), D, D, D, dp, dp]),
         "bhr_swsh": (D, [D, D, D]),
+        "bhr_write_waveform": (I, [C.c_char_p, C.c_char_p, D, dp, dp, dp, I]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -174,6 +175,14 @@ def source_coefficients(pt: Particle, a: float, mass: float, m: float):
     cr, ci = np.zeros(6), np.zeros(6)
     _check(lib.bhr_source_coefficients(C.byref(pt), a, mass, m, _ptr(cr), _ptr(ci)))
     return cr + 1j * ci
+
+
+def write_waveform(out_dir: str, name: str, m: float, t: np.ndarray, h: np.ndarray, dedt=None):
+    """hm<m>_<name>.dat in the reference format (plus a full-precision .full)."""
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    h = np.ascontiguousarray(h, dtype=np.float64).reshape(len(t), 14)
+    e = None if dedt is None else np.ascontiguousarray(dedt, dtype=np.float64)
+    _check(load_library().bhr_write_waveform(out_dir.encode(), name.encode(), m, _ptr(t), _ptr(h), _ptr(e), len(t)))
 
 
 class Solver:

@@ -596,10 +596,19 @@ int bhr_solver_run(bhr_solver *s, const char *out_dir, const char *name) {
   std::vector<double> t(rs.nrow), h(static_cast<size_t>(rs.nrow) * 14), e(rs.nrow);
   int n = 0;
   if (int st = bhr_solver_waveform(s, t.data(), h.data(), e.data(), rs.nrow, &n)) return st;
+  return bhr_write_waveform(out_dir, name, s->p.m, t.data(), h.data(), e.data(), n);
+}
+
+int bhr_write_waveform(const char *out_dir, const char *name, double m, const double *t, const double *h,
+                       const double *dedt, int nrows) {
+  if (!out_dir || !name || nrows < 0 || (nrows > 0 && (!t || !h))) {
+    set_error("bad waveform arguments");
+    return BHR_INVALID_ARG;
+  }
   // File naming as QNM_Extraction's loadwaveforms expects
   // (QNM_Extraction/Library/ringdownlib.py:49-84): hm<m>_ for m >= 0 and
   // hmm<|m|>_ for m < 0.
-  const int mi = static_cast<int>(s->p.m);
+  const int mi = static_cast<int>(m);
   char fname[4096];
   std::snprintf(fname, sizeof(fname), "%s/%s%d_%s.dat", out_dir, mi < 0 ? "hmm" : "hm", std::abs(mi), name);
   FILE *f = std::fopen(fname, "w");
@@ -611,14 +620,14 @@ int bhr_solver_run(bhr_solver *s, const char *out_dir, const char *name) {
     set_error(std::string("cannot write ") + fname);
     return BHR_IO_ERROR;
   }
-  for (int r = 0; r < n; r++) {
+  for (int r = 0; r < nrows; r++) {
     // HighOrder/body.cu:208: "%lf" time then 14 "%g" values.
     std::fprintf(f, "%lf", t[r]);
     for (int i = 0; i < 14; i++) std::fprintf(f, " %g", h[14 * r + i]);
     std::fprintf(f, "\n");
     std::fprintf(g, "%.17g", t[r]);
     for (int i = 0; i < 14; i++) std::fprintf(g, " %.17g", h[14 * r + i]);
-    std::fprintf(g, " %.17g\n", e[r]);
+    std::fprintf(g, " %.17g\n", dedt ? dedt[r] : 0.0);
   }
   std::fclose(f);
   std::fclose(g);

@@ -130,6 +130,13 @@ int bhr_solver_step(bhr_solver *s, int nsteps);
  * Replaces the whole of body(). */
 int bhr_solver_run(bhr_solver *s, const char *out_dir, const char *name);
 
+/* Writes waveform rows (as bhr_solver_waveform returns them) to
+ * <dir>/hm<m>_<name>.dat (hmm<|m|>_ for m < 0) in the reference's row format
+ * "%lf %g x14" (HighOrder/body.cu:208) and a "%.17g" companion <file>.full
+ * with dE/dt appended.  Host only. */
+int bhr_write_waveform(const char *out_dir, const char *name, double m, const double *t, const double *h,
+                       const double *dedt, int nrows);
+
 /* Waveform rows produced so far: t[r] (= timer - Xmax), h[r*14 + 2l] = h+
  * and h[r*14+2l+1] = hx for l = |m|+0..6, dedt[r] (HighOrder/body.cu:
  * 174-212).  Any output pointer may be NULL. */

@@ -24,6 +24,7 @@ sys.path.insert(0, ROOT)
 from oracle import pyoracle  # noqa: E402
 
 D = C.c_double
+REF = os.environ.get("BHR_REFERENCE_ROOT", "/root/reference")
 
 
 def ref_lib(tag):
@@ -163,6 +164,15 @@ def main():
     L2.ref_grid(D(1.0), D(0.5), p(x), p(r), p(t))
     np.savez_compressed(os.path.join(HERE, "grid_c1s_a05.npz"), x_c=x, r_c=r, theta=t, N=N2, M=M2,
                         Xmin=L2.ref_Xmin(), Xmax=L2.ref_Xmax(), a=0.5)
+    # The head of two of the reference's example waveform files
+    # (QNM_Extraction/Examples, written by HighOrder/body.cu:208) for the
+    # byte-level writer test.
+    ex = os.path.join(REF, "QNM_Extraction", "Examples")
+    for fn in ("hm2_a0.7_thi000_thf090.0_n.dat", "hmm1_a0.7_thi000_thf090.0_n.dat"):
+        with open(os.path.join(ex, fn)) as f:
+            head = [next(f) for _ in range(40)]
+        with open(os.path.join(HERE, "example_head_" + fn.replace(".dat", ".txt")), "w") as f:
+            f.writelines(head)
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))
