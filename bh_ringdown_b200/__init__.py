@@ -134,6 +134,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "bhr_source_coefficients": (I, [P(Particle), D, D, D, dp, dp]),
         "bhr_swsh": (D, [D, D, D]),
         "bhr_write_waveform": (I, [C.c_char_p, C.c_char_p, D, dp, dp, dp, I]),
+        "bhr_step_noalloc": (I, [P(_Params), vp, I, vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -183,6 +184,14 @@ def write_waveform(out_dir: str, name: str, m: float, t: np.ndarray, h: np.ndarr
     h = np.ascontiguousarray(h, dtype=np.float64).reshape(len(t), 14)
     e = None if dedt is None else np.ascontiguousarray(dedt, dtype=np.float64)
     _check(load_library().bhr_write_waveform(out_dir.encode(), name.encode(), m, _ptr(t), _ptr(h), _ptr(e), len(t)))
+
+
+def step_noalloc(params: Params, state_ptr: int, nsteps: int, stream: int = 0):
+    """bhr_step_noalloc on device memory the caller owns (state_ptr: address
+    of four contiguous closed M x N FP64 planes)."""
+    p = params.to_c()
+    _check(load_library().bhr_step_noalloc(C.byref(p), C.c_void_p(state_ptr), int(nsteps),
+                                           C.c_void_p(stream) if stream else None))
 
 
 class Solver:

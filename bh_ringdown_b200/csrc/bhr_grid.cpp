@@ -19,33 +19,27 @@ constexpr double kThirdH = 0.33333333333333333;  // HighOrder/kern.cu:46
 // r - r+ falls below FP64 resolution the reference iteration returns NaN;
 // from the first point whose step lands at or inside r+ onwards, r is set
 // to the next double above r+.
-Grid make_grid(const bhr_params &p) {
-  Grid g;
-  g.N = p.N;
-  g.M = p.M;
-  g.dx = (p.Xmax - p.Xmin) / p.N;
-  g.dtheta = kPiParm / p.M;
-  g.x_c.resize(p.N);
-  g.r_c.resize(p.N);
-  g.theta.resize(p.M);
+void fill_grid(const bhr_params &p, double *x_c, double *r_c, double *theta, double *tx, double *r_plus,
+               double *r_minus) {
+  const double dx = (p.Xmax - p.Xmin) / p.N;
+  const double dtheta = kPiParm / p.M;
   const double mass = p.mass, aa = p.a;
-  for (int l = 0; l < p.N; l++) g.x_c[l] = p.Xmin + static_cast<double>(l) * g.dx;
-  for (int b = 0; b < p.M; b++) g.theta[b] = static_cast<double>(b) * g.dtheta;
+  for (int l = 0; l < p.N; l++) x_c[l] = p.Xmin + static_cast<double>(l) * dx;
+  for (int b = 0; b < p.M; b++) theta[b] = static_cast<double>(b) * dtheta;
   const double rin = p.Xmin + (p.Xmax - p.Xmin) * 0.64;
   const double Rrpt = p.Xmax + 1e-6;
-  std::vector<double> tx(p.N);
   for (int l = 0; l < p.N; l++) {
-    const double x = g.x_c[l];
+    const double x = x_c[l];
     const double om = (x < rin) ? 1.0 : 1.0 - std::pow((x - rin) / (Rrpt - rin), 4);
     tx[l] = x / om;
   }
   const double rp = mass + std::sqrt(mass * mass - aa * aa);
   const double rm = mass - std::sqrt(mass * mass - aa * aa);
-  g.r_plus = rp;
-  g.r_minus = rm;
+  *r_plus = rp;
+  *r_minus = rm;
   if (mass == 0.0) {
-    for (int l = 0; l < p.N; l++) g.r_c[l] = tx[l];
-    return g;
+    for (int l = 0; l < p.N; l++) r_c[l] = tx[l];
+    return;
   }
   const double tol = 1e-12;
   const double r_floor = std::nextafter(rp, INFINITY);
@@ -53,7 +47,7 @@ Grid make_grid(const bhr_params &p) {
   double r_old = tx[p.N - 1], r_new = r_old;
   for (int l = p.N - 1; l >= 0; l--) {
     if (floored) {
-      g.r_c[l] = r_floor;
+      r_c[l] = r_floor;
       continue;
     }
     double diff;
@@ -76,9 +70,22 @@ Grid make_grid(const bhr_params &p) {
       diff = std::fabs(r_new - r_old) / r_old;
       r_old = r_new;
     } while (diff > tol);
-    g.r_c[l] = r_new;
+    r_c[l] = r_new;
     r_old = r_new;
   }
+}
+
+Grid make_grid(const bhr_params &p) {
+  Grid g;
+  g.N = p.N;
+  g.M = p.M;
+  g.dx = (p.Xmax - p.Xmin) / p.N;
+  g.dtheta = kPiParm / p.M;
+  g.x_c.resize(p.N);
+  g.r_c.resize(p.N);
+  g.theta.resize(p.M);
+  std::vector<double> tx(p.N);
+  fill_grid(p, g.x_c.data(), g.r_c.data(), g.theta.data(), tx.data(), &g.r_plus, &g.r_minus);
   return g;
 }
 
@@ -87,15 +94,21 @@ Grid make_grid(const bhr_params &p) {
 // per-row factor) / bir with bir = B0 + B1 sin^2(theta); the tables hold
 // those numerators and the row factors.
 void make_tables(const bhr_params &p, const Grid &g, std::vector<double> &coltab, std::vector<double> &rowtab) {
+  coltab.assign(static_cast<size_t>(CF_COUNT) * p.N, 0.0);
+  rowtab.assign(static_cast<size_t>(RF_COUNT) * p.M, 0.0);
+  fill_tables(p, g.dx, g.r_c.data(), g.theta.data(), coltab.data(), rowtab.data());
+}
+
+void fill_tables(const bhr_params &p, double dx, const double *r_c, const double *theta, double *coltab,
+                 double *rowtab) {
   const int N = p.N, M = p.M;
-  coltab.assign(static_cast<size_t>(CF_COUNT) * N, 0.0);
-  rowtab.assign(static_cast<size_t>(RF_COUNT) * M, 0.0);
+  for (size_t i = 0; i < static_cast<size_t>(RF_COUNT) * M; i++) rowtab[i] = 0.0;
   const double mass = p.mass, spin = p.a, em = p.m;
   const double rin = p.Xmin + (p.Xmax - p.Xmin) * 0.64;
   const double Rrpt = p.Xmax + 1e-6;
   const double a2 = spin * spin, a4 = a2 * a2;
   for (int j = 0; j < N; j++) {
-    const double x = p.Xmin + static_cast<double>(j) * g.dx;
+    const double x = p.Xmin + static_cast<double>(j) * dx;
     double Om = 1.0, O1 = 0.0, O2 = 0.0;
     if (x >= rin) {
       const double L = Rrpt - rin, L4 = std::pow(L, 4);
@@ -104,7 +117,7 @@ void make_tables(const bhr_params &p, const Grid &g, std::vector<double> &coltab
       O2 = -12.0 * std::pow(x - rin, 2) / L4;
     }
     const double cL = Om - x * O1;
-    const double eR = Om * g.r_c[j];
+    const double eR = Om * r_c[j];
     const double eR2 = eR * eR, eR3 = eR2 * eR, eR5 = eR3 * eR2;
     const double Om2 = Om * Om, Om3 = Om2 * Om, Om4 = Om2 * Om2, Om5 = Om4 * Om;
     const double cL2 = cL * cL, cL3 = cL2 * cL;
@@ -123,7 +136,7 @@ void make_tables(const bhr_params &p, const Grid &g, std::vector<double> &coltab
               Om4 * (6.0 * Om2 + 2.0 * O1 * O1 * x * (-eR + 3.0 * x) + Om * (2.0 * eR * O1 - 12.0 * O1 * x + eR * O2 * x)) *
                   a4 +
               2.0 * cL2 * eR * (2.0 * eR3 - 6.0 * eR2 * mass * Om + 5.0 * eR * Om2 * a2 - 4.0 * mass * Om3 * a2));
-    double *c = coltab.data();
+    double *c = coltab;
     c[CF_B0 * N + j] = -((2.0 * cL - Om2) * Sg * Sg) / cL2;
     c[CF_B1 * N + j] = a2 * Dt;
     c[CF_ATN * N + j] = (2.0 * (cL - Om2) * Sg * Sg) / cL2;
@@ -139,7 +152,7 @@ void make_tables(const bhr_params &p, const Grid &g, std::vector<double> &coltab
     c[CF_CIN * N + j] = (2.0 * em * Om * spin * (eR2 + 2.0 * eR * mass * Om - 3.0 * Om2 * a2)) / eR;
   }
   for (int b = 3; b < M - 3; b++) {
-    const double y = g.theta[b];
+    const double y = theta[b];
     const double sn = std::sin(y);
     const double cot = 1.0 / std::tan(y), csc = 1.0 / std::sin(y);
     rowtab[RF_S2 * M + b] = sn * sn;

@@ -20,8 +20,14 @@ struct Grid {
 // Grid of HighOrder/main.c:79-198, with a horizon floor where the Newton
 // iteration would step to r <= r+ (see grid.cpp).
 Grid make_grid(const bhr_params &p);
+// The same, into caller arrays (x_c, r_c, tx of N; theta of M); no allocation.
+void fill_grid(const bhr_params &p, double *x_c, double *r_c, double *theta, double *tx, double *r_plus,
+               double *r_minus);
 // Per-column and per-row coefficient factors (layouts of bhr_internal.h).
 void make_tables(const bhr_params &p, const Grid &g, std::vector<double> &coltab, std::vector<double> &rowtab);
+// The same, into caller arrays (CF_COUNT*N and RF_COUNT*M); no allocation.
+void fill_tables(const bhr_params &p, double dx, const double *r_c, const double *theta, double *coltab,
+                 double *rowtab);
 // Spin-weighted harmonic s=-2 (HighOrder/proj.c:16-35).
 double swsh(double ell, double ml, double the);
 // Boole-rule projection weights: h_l = sum_b W[l*M + b] * q[b] for

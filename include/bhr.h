@@ -175,6 +175,25 @@ int bhr_source_coefficients(const bhr_particle *pt, double a, double mass, doubl
 /* Spin-weighted spherical harmonic of HighOrder/proj.c:16-35 (s = -2). */
 double bhr_swsh(double ell, double m, double theta);
 
+/* Source-free SSP-RK3 steps on a state the caller owns, allocating nothing.
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * a framework that reserves the device memory up front and hands out
+ * pieces of it, or a latency-critical loop that may not take cudaMalloc's
+ * implicit device synchronisation.  `state` is device memory holding the
+ * four closed M x N FP64 planes q_re, q_im, p_re, p_im back to back
+ * (16-byte aligned); it is advanced nsteps steps in place on `stream` (a
+ * cudaStream_t, NULL for the default stream) and closed again on return.
+ * p->dt must be > 0.  The two intermediate stages and the coefficient
+ * tables live in one fixed file-scope device array of about 10 MB, so
+ * grids are limited to N*M <= 131072, N <= 16384, M <= 1024; larger ones
+ * are rejected with BHR_INVALID_ARG.  Every GPU that loads the library
+ * holds that array until the process exits.  The first call on a device
+ * looks up the array's device address and sets the stage kernels'
+ * shared-memory size; make that first call before any stream capture.  All
+ * calls share the array and it keeps the last call's contents: calls that
+ * overlap on the GPU (other streams, other host threads' streams) race. */
+int bhr_step_noalloc(const bhr_params *p, double *state, int nsteps, void *stream);
+
 const char *bhr_last_error_string(void);
 int bhr_abi_version(void);
 
