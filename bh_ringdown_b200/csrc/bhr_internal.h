@@ -94,9 +94,12 @@ struct ExtractArgs {
 };
 
 // Launchers (bhr_kernels.cu).
-cudaError_t encode_state_maps(void *planes, int N, int M, CUtensorMap *tm_q, CUtensorMap *tm_p);
-cudaError_t launch_stage(int stage, const CUtensorMap &tm_q, const CUtensorMap &tm_p, const StageArgs &a,
-                         cudaStream_t st);
+// Tensor maps of one state (four M x N planes): q planes with the +-3 row
+// and +-4 column halo, p planes with the column halo, and (tm_u, may be
+// null) the bare tile of all four planes for reading u^n.
+cudaError_t encode_state_maps(void *planes, int N, int M, CUtensorMap *tm_q, CUtensorMap *tm_p, CUtensorMap *tm_u);
+cudaError_t launch_stage(int stage, const CUtensorMap &tm_q, const CUtensorMap &tm_p, const CUtensorMap &tm_u,
+                         const StageArgs &a, cudaStream_t st);
 cudaError_t launch_source(const SourceArgs &a, cudaStream_t st);
 cudaError_t launch_extract(const ExtractArgs &a, cudaStream_t st);
 cudaError_t launch_closure(double *planes, int N, int M, int even_m, cudaStream_t st);

@@ -23,6 +23,8 @@
 
 #include <cudaTypedefs.h>
 
+#include <algorithm>
+
 namespace bhr {
 
 namespace {
@@ -80,19 +82,50 @@ __device__ __forceinline__ double ko8c(const double *v, int c) {
          56.0 * (v[c + 1] + v[c - 1]) + 70.0 * v[c];
 }
 
+// Reciprocal by Newton-Raphson iteration y <- y (2 - x y) from the hardware
+// approximation (two steps take its ~2^-22 relative error below 1 ulp).
+__device__ __forceinline__ double rcp_nr(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
+// Square root of x >= 0: Newton-Raphson for 1/sqrt(x), y <- y (3/2 - x y^2 / 2),
+// from the hardware approximation, then one correction of s = x y by the
+// residual x - s^2.
+__device__ __forceinline__ double sqrt_nr(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  y = y * fma(-0.5 * x * y, y, 1.5);
+  y = y * fma(-0.5 * x * y, y, 1.5);
+  double s = x * y;
+  s = fma(fma(-s, s, x), 0.5 * y, s);
+  return x > 0.0 ? s : 0.0;
+}
+
+// Column factors the main pass reads per point, in this order.
+constexpr int kColFields = 9;
+__device__ __constant__ int kColFieldIds[kColFields] = {CF_CCN, CF_XR, CF_YR, CF_BI0, CF_BI1,
+                                                        CF_BRI, CF_CR0, CF_CR1, CF_CIN};
+
 struct __align__(128) StageSmem {
-  double q[2][QR][WC];  // TMA box {WC, QR, 2} of planes q_re, q_im
-  double p[2][TR][WC];  // TMA box {WC, TR, 2} of planes p_re, p_im
-  double bb[TR][WC];    // bb on the window columns (for d bb/dx)
-  double ib[TR][WC];    // 1/bir
-  double ee[TR][WC];    // ee = Ataurho + bb
+  double q[2][QR][WC];          // TMA box {WC, QR, 2} of planes q_re, q_im
+  double p[2][TR][WC];          // TMA box {WC, TR, 2} of planes p_re, p_im
+  double bb[TR][WC];            // bb on the window columns (for d bb/dx)
+  double ib[TR][TC];            // 1/bir on the tile columns
+  double ee[TR][TC];            // ee = Ataurho + bb on the tile columns
+  double cf[kColFields][TC];    // column factors of the tile columns
+  double un[4][TR][TC];         // TMA box {TC, TR, 4} of u^n (stages 2 and 3)
   uint64_t bar;
 };
 
 template <int STAGE>
 __global__ void __launch_bounds__(STAGE_THREADS, 2)
     stage_kernel(const __grid_constant__ CUtensorMap tm_q, const __grid_constant__ CUtensorMap tm_p,
-                 const StageArgs A) {
+                 const __grid_constant__ CUtensorMap tm_u, const StageArgs A) {
   extern __shared__ unsigned char smem_raw[];
   StageSmem &S = *reinterpret_cast<StageSmem *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
@@ -107,27 +140,43 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
   }
   __syncthreads();
   if (tid == 0) {
-    mbar_expect_tx(&S.bar, static_cast<uint32_t>(sizeof(S.q) + sizeof(S.p)));
+    const uint32_t bytes = static_cast<uint32_t>(sizeof(S.q) + sizeof(S.p) + (STAGE == 1 ? 0 : sizeof(S.un)));
+    mbar_expect_tx(&S.bar, bytes);
     tma_load_3d(&S.q[0][0][0], &tm_q, c0 - 4, b0 - 3, 0, &S.bar);
     tma_load_3d(&S.p[0][0][0], &tm_p, c0 - 4, b0, 2, &S.bar);
+    if (STAGE != 1) tma_load_3d(&S.un[0][0][0], &tm_u, c0, b0, 0, &S.bar);
   }
 
-  // Coefficient pass while the tile is in flight: bb, 1/bir and ee on the
-  // window columns of the tile rows (HighOrder/kern.cu:132-149).
+  // While the tile is in flight: column factors of the tile columns, and
+  // bb on the window columns with 1/bir and ee on the tile columns
+  // (HighOrder/kern.cu:132-158).  Columns are lanes, rows are warps.
   const double *ct = A.coltab;
   const double *rt = A.rowtab;
-  for (int i = tid; i < TR * WC; i += STAGE_THREADS) {
-    const int r = i / WC, w = i - r * WC;
-    const int b = b0 + r, a = c0 - 4 + w;
-    if (w >= 1 && w < WC - 1 && b >= 3 && b < M - 3 && a >= 0 && a < N) {
-      const double bir = __ldg(ct + CF_B0 * N + a) + __ldg(ct + CF_B1 * N + a) * __ldg(rt + RF_S2 * M + b);
-      const double ib = 1.0 / bir;
-      const double At = __ldg(ct + CF_ATN * N + a) * ib;
-      const double Ar = __ldg(ct + CF_ARN * N + a) * ib;
-      const double bb = -(At + sqrt(At * At + 4.0 * Ar)) * 0.5;
+  for (int i = tid; i < kColFields * TC; i += STAGE_THREADS) {
+    const int f = i / TC, col = i % TC;
+    const int a = c0 + col;
+    S.cf[f][col] = (a < N) ? __ldg(ct + kColFieldIds[f] * N + a) : 0.0;
+  }
+#pragma unroll
+  for (int wi = 0; wi < 3; wi++) {
+    const int w = tx + 1 + 32 * wi;
+    const int a = c0 - 4 + w;
+    if (w >= WC - 1 || a < 0 || a >= N) continue;
+    const double B0 = __ldg(ct + CF_B0 * N + a), B1 = __ldg(ct + CF_B1 * N + a);
+    const double ATN = __ldg(ct + CF_ATN * N + a), ARN = __ldg(ct + CF_ARN * N + a);
+#pragma unroll
+    for (int rj = 0; rj < TR / 8; rj++) {
+      const int r = ty + 8 * rj;
+      const int b = b0 + r;
+      if (b < 3 || b >= M - 3) continue;
+      const double ib = rcp_nr(fma(B1, __ldg(rt + RF_S2 * M + b), B0));
+      const double At = ATN * ib, Ar = ARN * ib;
+      const double bb = -(At + sqrt_nr(fma(At, At, 4.0 * Ar))) * 0.5;
       S.bb[r][w] = bb;
-      S.ib[r][w] = ib;
-      S.ee[r][w] = At + bb;
+      if (w >= 4 && w < TC + 4) {
+        S.ib[r][w - 4] = ib;
+        S.ee[r][w - 4] = At + bb;
+      }
     }
   }
 
@@ -201,6 +250,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
     src_r0 = rec.row0;
     tile_src = (src_c0 < c0 + TC) && (src_c0 + A.PTSX > c0) && (src_r0 < b0 + TR) && (src_r0 + A.PTSY > b0);
   }
+  // Tiles away from both radial ends need no per-column end checks.
+  const bool inner = !lo_cols && !hi_cols;
 
   const int a0 = c0 + 2 * tx;  // this thread's columns a0, a0+1
   const int w0 = 2 * tx + 4;   // their window column
@@ -210,30 +261,10 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
     const int r = 2 * ty + rr;
     const int b = b0 + r;
     if (b < 3 || b >= M - 3) continue;
-    if (a0 + 1 < 3 || a0 >= N - 3) continue;
+    if (!inner && (a0 + 1 < 3 || a0 >= N - 3)) continue;
 
-    // Radial first derivative and dissipation of the four planes.
-    double fx[4][2], fk[4][2], fc[4][2];
-#pragma unroll
-    for (int pl = 0; pl < 4; pl++) {
-      const double *row = pl < 2 ? &S.q[pl][r + 3][0] : &S.p[pl - 2][r][0];
-      double v[10];
-#pragma unroll
-      for (int j = 0; j < 5; j++) {
-        const double2 t = *reinterpret_cast<const double2 *>(row + w0 - 4 + 2 * j);
-        v[2 * j] = t.x;
-        v[2 * j + 1] = t.y;
-      }
-#pragma unroll
-      for (int c = 0; c < 2; c++) {
-        const int a = a0 + c;
-        fc[pl][c] = v[4 + c];
-        fx[pl][c] = d1c(v, 4 + c) * A.cx;
-        fk[pl][c] = (a >= 4 && a < N - 4) ? ko8c(v, 4 + c) * A.cko : 0.0;
-      }
-    }
     // Theta derivatives of q (HighOrder/kern.cu:206-226).
-    const double ctan = __ldg(rt + RF_CTAN * M + b);
+    const double ctan_cy = __ldg(rt + RF_CTAN * M + b) * A.cy;
     double ll[2][2];
 #pragma unroll
     for (int pl = 0; pl < 2; pl++) {
@@ -249,30 +280,46 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
         const double y1 = (f[6][c] - f[0][c]) - 9.0 * (f[5][c] - f[1][c]) + 45.0 * (f[4][c] - f[2][c]);
         const double y2 = 2.0 * (f[6][c] + f[0][c]) - 27.0 * (f[5][c] + f[1][c]) +
                           270.0 * (f[4][c] + f[2][c]) - 490.0 * f[3][c];
-        ll[pl][c] = y2 * A.cyy + ctan * (y1 * A.cy);
+        ll[pl][c] = y2 * A.cyy + ctan_cy * y1;
       }
     }
 
+    // Coefficients at the two points (HighOrder/kern.cu:132-158, 192-197).
     const double cs = __ldg(rt + RF_COS * M + b);
     const double gth = __ldg(rt + RF_G * M + b);
+    double kbb[2], kee[2], kdre[2], kdim[2], kare[2], kaim[2], kvre[2], kvim[2];
     double res[4][2];
+    // bb on columns a0-4 .. a0+5, and the per-column arrays, as 16-byte pairs
+    double bw[10];
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      const double2 t = *reinterpret_cast<const double2 *>(&S.bb[r][w0 - 4 + 2 * j]);
+      bw[2 * j] = t.x;
+      bw[2 * j + 1] = t.y;
+    }
+    auto pair = [&](const double *base) { return *reinterpret_cast<const double2 *>(base + 2 * tx); };
+    const double2 ib2 = pair(S.ib[r]), ee2 = pair(S.ee[r]);
+    const double2 f0 = pair(S.cf[0]), f1 = pair(S.cf[1]), f2 = pair(S.cf[2]), f3 = pair(S.cf[3]),
+                  f4 = pair(S.cf[4]), f5 = pair(S.cf[5]), f6 = pair(S.cf[6]), f7 = pair(S.cf[7]),
+                  f8 = pair(S.cf[8]);
 #pragma unroll
     for (int c = 0; c < 2; c++) {
       const int a = a0 + c;
-      const int w = w0 + c;
-      const int ac = (a < N) ? a : N - 1;  // table reads stay in range
-      const double bb = S.bb[r][w], ib = S.ib[r][w], ee = S.ee[r][w];
-      const double dbdx = (45.0 * (S.bb[r][w + 1] - S.bb[r][w - 1]) - 9.0 * (S.bb[r][w + 2] - S.bb[r][w - 2]) +
-                           (S.bb[r][w + 3] - S.bb[r][w - 3])) * A.cx;
-      const double cc = __ldg(ct + CF_CCN * N + ac) * ib;
-      const double btr = __ldg(ct + CF_XR * N + ac) * ib;
-      const double brr = __ldg(ct + CF_YR * N + ac) * ib;
-      const double bti = (__ldg(ct + CF_BI0 * N + ac) + __ldg(ct + CF_BI1 * N + ac) * cs) * ib;
-      const double dim = __ldg(ct + CF_BRI * N + ac) * ib - bb * bti;
-      const double vre = -(__ldg(ct + CF_CR0 * N + ac) + __ldg(ct + CF_CR1 * N + ac) * gth) * ib;
-      const double vim = -__ldg(ct + CF_CIN * N + ac) * ib;
-      const double are = -btr, aim = -bti;
-      const double dre = (brr - bb * btr) - dbdx * ee;
+      auto pk = [&](double2 v) { return c ? v.y : v.x; };
+      const double bb = bw[4 + c], ib = pk(ib2), ee = pk(ee2);
+      const double dbdx = d1c(bw, 4 + c) * A.cx;
+      const double cc = pk(f0) * ib;
+      const double btr = pk(f1) * ib;
+      const double brr = pk(f2) * ib;
+      const double bti = (pk(f3) + pk(f4) * cs) * ib;
+      kbb[c] = bb;
+      kee[c] = ee;
+      kdim[c] = pk(f5) * ib - bb * bti;
+      kvre[c] = -(pk(f6) + pk(f7) * gth) * ib;
+      kvim[c] = -pk(f8) * ib;
+      kare[c] = -btr;
+      kaim[c] = -bti;
+      kdre[c] = (brr - bb * btr) - dbdx * ee;
       double sre = 0.0, sim = 0.0;
       if (tile_src) {
         const int sc = a - src_c0, sr = b - src_r0;
@@ -281,19 +328,56 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
           sim = A.src[static_cast<size_t>(A.PTSY + sr) * A.PTSX + sc];
         }
       }
-      const double qr = fc[0][c], qi = fc[1][c], pr = fc[2][c], pi = fc[3][c];
-      const double qxr = fx[0][c], qxi = fx[1][c], pxr = fx[2][c], pxi = fx[3][c];
-      res[0][c] = -bb * qxr + pr - fk[0][c];
-      res[1][c] = -bb * qxi + pi - fk[1][c];
-      res[2][c] = sre + ee * pxr - fk[2][c] + cc * ll[0][c] + dre * qxr - dim * qxi - are * pr + aim * pi -
-                  vre * qr + vim * qi;
-      res[3][c] = sim + ee * pxi - fk[3][c] + cc * ll[1][c] + dre * qxi + dim * qxr - are * pi - aim * pr -
-                  vre * qi - vim * qr;
+      res[0][c] = 0.0;
+      res[1][c] = 0.0;
+      res[2][c] = sre + cc * ll[0][c];
+      res[3][c] = sim + cc * ll[1][c];
+    }
+
+    // Radial first derivative and dissipation plane by plane, each folded
+    // into the right-hand side as soon as it is formed
+    // (HighOrder/kern.cu:233-261, 281-296).
+    double fc[4][2];
+#pragma unroll
+    for (int pl = 0; pl < 4; pl++) {
+      const double *row = pl < 2 ? &S.q[pl][r + 3][0] : &S.p[pl - 2][r][0];
+      double v[10];
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+        const double2 t = *reinterpret_cast<const double2 *>(row + w0 - 4 + 2 * j);
+        v[2 * j] = t.x;
+        v[2 * j + 1] = t.y;
+      }
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const int a = a0 + c;
+        const double f0 = v[4 + c];
+        const double fx = d1c(v, 4 + c) * A.cx;
+        const double fk = (inner || (a >= 4 && a < N - 4)) ? ko8c(v, 4 + c) * A.cko : 0.0;
+        fc[pl][c] = f0;
+        if (pl == 0) {         // q_re
+          res[0][c] += -kbb[c] * fx - fk;
+          res[2][c] += kdre[c] * fx - kvre[c] * f0;
+          res[3][c] += kdim[c] * fx - kvim[c] * f0;
+        } else if (pl == 1) {  // q_im
+          res[1][c] += -kbb[c] * fx - fk;
+          res[2][c] += -kdim[c] * fx + kvim[c] * f0;
+          res[3][c] += kdre[c] * fx - kvre[c] * f0;
+        } else if (pl == 2) {  // p_re
+          res[0][c] += f0;
+          res[2][c] += kee[c] * fx - fk - kare[c] * f0;
+          res[3][c] += -kaim[c] * f0;
+        } else {               // p_im
+          res[1][c] += f0;
+          res[2][c] += kaim[c] * f0;
+          res[3][c] += kee[c] * fx - fk - kare[c] * f0;
+        }
+      }
     }
 
     // Shu-Osher stage combination (HighOrder/kern.cu:301-318, 582-620).
     const size_t base = static_cast<size_t>(b) * N + a0;
-    const bool both = (a0 >= 3) && (a0 + 1 < N - 3);
+    const bool both = inner || ((a0 >= 3) && (a0 + 1 < N - 3));
 #pragma unroll
     for (int pl = 0; pl < 4; pl++) {
       double o[2];
@@ -301,7 +385,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
         o[0] = fc[pl][0] + dt * res[pl][0];
         o[1] = fc[pl][1] + dt * res[pl][1];
       } else {
-        const double2 u = *reinterpret_cast<const double2 *>(A.un + pl * NM + base);
+        const double2 u = *reinterpret_cast<const double2 *>(&S.un[pl][r][2 * tx]);
         if (STAGE == 2) {
           o[0] = 0.25 * (3.0 * u.x + fc[pl][0] + dt * res[pl][0]);
           o[1] = 0.25 * (3.0 * u.y + fc[pl][1] + dt * res[pl][1]);
@@ -509,7 +593,7 @@ __global__ void __launch_bounds__(kExtractThreads) extract_kernel(const ExtractA
 // ---- host launchers -------------------------------------------------------
 size_t stage_smem_bytes() { return sizeof(StageSmem) + 128; }
 
-cudaError_t encode_state_maps(void *planes, int N, int M, CUtensorMap *tm_q, CUtensorMap *tm_p) {
+cudaError_t encode_state_maps(void *planes, int N, int M, CUtensorMap *tm_q, CUtensorMap *tm_p, CUtensorMap *tm_u) {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     cudaDriverEntryPointQueryResult qr;
@@ -529,16 +613,23 @@ cudaError_t encode_state_maps(void *planes, int N, int M, CUtensorMap *tm_q, CUt
   CUresult r2 = encode(tm_p, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, planes, dims, strides, box_p, estr,
                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  return (r1 == CUDA_SUCCESS && r2 == CUDA_SUCCESS) ? cudaSuccess : cudaErrorInvalidValue;
+  CUresult r3 = CUDA_SUCCESS;
+  if (tm_u) {
+    const cuuint32_t box_u[3] = {TC, TR, 4};
+    r3 = encode(tm_u, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, planes, dims, strides, box_u, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  }
+  return (r1 == CUDA_SUCCESS && r2 == CUDA_SUCCESS && r3 == CUDA_SUCCESS) ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-cudaError_t launch_stage(int stage, const CUtensorMap &tm_q, const CUtensorMap &tm_p, const StageArgs &a,
-                         cudaStream_t st) {
+cudaError_t launch_stage(int stage, const CUtensorMap &tm_q, const CUtensorMap &tm_p, const CUtensorMap &tm_u,
+                         const StageArgs &a, cudaStream_t st) {
   const size_t smem = stage_smem_bytes();
   const dim3 grid(a.N / TC, a.M / TR), block(32, STAGE_THREADS / 32);
-  if (stage == 1) stage_kernel<1><<<grid, block, smem, st>>>(tm_q, tm_p, a);
-  else if (stage == 2) stage_kernel<2><<<grid, block, smem, st>>>(tm_q, tm_p, a);
-  else stage_kernel<3><<<grid, block, smem, st>>>(tm_q, tm_p, a);
+  if (stage == 1) stage_kernel<1><<<grid, block, smem, st>>>(tm_q, tm_p, tm_u, a);
+  else if (stage == 2) stage_kernel<2><<<grid, block, smem, st>>>(tm_q, tm_p, tm_u, a);
+  else stage_kernel<3><<<grid, block, smem, st>>>(tm_q, tm_p, tm_u, a);
   return cudaGetLastError();
 }
 

@@ -87,10 +87,10 @@ extern "C" int bhr_step_noalloc(const bhr_params *p, double *state, int nsteps, 
   const double dx = (p->Xmax - p->Xmin) / N, dth = kPiParm / M;
   fill_tables(*p, dx, h_r, h_th, h_col, h_row);
 
-  CUtensorMap tq[3], tp[3];
+  CUtensorMap tq[3], tp[3], tu;
   double *bufs[3] = {state, u1, u2};
   for (int i = 0; i < 3; i++)
-    if (encode_state_maps(bufs[i], N, M, &tq[i], &tp[i]) != cudaSuccess)
+    if (encode_state_maps(bufs[i], N, M, &tq[i], &tp[i], i == 0 ? &tu : nullptr) != cudaSuccess)
       return fail(BHR_CUDA_ERROR, "bhr_step_noalloc: cuTensorMapEncodeTiled failed (state must be 16-byte aligned)");
   // The tables must be current for this call; the flag must start at zero.
   if (cudaMemcpyAsync(coltab, h_col, sizeof(double) * CF_COUNT * N, cudaMemcpyHostToDevice, st) != cudaSuccess ||
@@ -118,11 +118,11 @@ extern "C" int bhr_step_noalloc(const bhr_params *p, double *state, int nsteps, 
   A.cko = 0.1 * 0.0625 * (1.0 / p->dt);
   for (int k = 0; k < nsteps; k++) {
     A.vin = state; A.un = state; A.out = u1;
-    if (launch_stage(1, tq[0], tp[0], A, st) != cudaSuccess) return fail(BHR_CUDA_ERROR, "stage 1 launch failed");
+    if (launch_stage(1, tq[0], tp[0], tu, A, st) != cudaSuccess) return fail(BHR_CUDA_ERROR, "stage 1 launch failed");
     A.vin = u1; A.un = state; A.out = u2;
-    if (launch_stage(2, tq[1], tp[1], A, st) != cudaSuccess) return fail(BHR_CUDA_ERROR, "stage 2 launch failed");
+    if (launch_stage(2, tq[1], tp[1], tu, A, st) != cudaSuccess) return fail(BHR_CUDA_ERROR, "stage 2 launch failed");
     A.vin = u2; A.un = state; A.out = state;
-    if (launch_stage(3, tq[2], tp[2], A, st) != cudaSuccess) return fail(BHR_CUDA_ERROR, "stage 3 launch failed");
+    if (launch_stage(3, tq[2], tp[2], tu, A, st) != cudaSuccess) return fail(BHR_CUDA_ERROR, "stage 3 launch failed");
   }
   if (launch_closure(state, N, M, A.even_m, st) != cudaSuccess) return fail(BHR_CUDA_ERROR, "closure launch failed");
   int h_flag = 0;

@@ -51,7 +51,7 @@ struct bhr_solver {
   StepRec *recs = nullptr;
   RunState *rs = nullptr;
   size_t bytes = 0;
-  CUtensorMap tq[3], tp[3];
+  CUtensorMap tq[3], tp[3], tu;
   int steps_done = 0;
   // Captured step graphs: one step, and kGraphBatch steps in one launch.
   cudaGraphExec_t g1 = nullptr, gb = nullptr;
@@ -249,7 +249,7 @@ int bhr_solver_create(const bhr_params *pin, bhr_solver **out) {
   }
   double *bufs[3] = {s->u0, s->u1, s->u2};
   for (int i = 0; i < 3; i++) {
-    if (encode_state_maps(bufs[i], p.N, p.M, &s->tq[i], &s->tp[i]) != cudaSuccess) {
+    if (encode_state_maps(bufs[i], p.N, p.M, &s->tq[i], &s->tp[i], i == 0 ? &s->tu : nullptr) != cudaSuccess) {
       set_error("cuTensorMapEncodeTiled failed");
       free_all(s);
       delete s;
@@ -436,13 +436,13 @@ static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
   }
   BHR_CUDA_TRY(mark(1));
   A.vin = s->u0; A.un = s->u0; A.out = s->u1;
-  BHR_CUDA_TRY(launch_stage(1, s->tq[0], s->tp[0], A, s->stream));
+  BHR_CUDA_TRY(launch_stage(1, s->tq[0], s->tp[0], s->tu, A, s->stream));
   BHR_CUDA_TRY(mark(2));
   A.vin = s->u1; A.un = s->u0; A.out = s->u2;
-  BHR_CUDA_TRY(launch_stage(2, s->tq[1], s->tp[1], A, s->stream));
+  BHR_CUDA_TRY(launch_stage(2, s->tq[1], s->tp[1], s->tu, A, s->stream));
   BHR_CUDA_TRY(mark(3));
   A.vin = s->u2; A.un = s->u0; A.out = s->u0;
-  BHR_CUDA_TRY(launch_stage(3, s->tq[2], s->tp[2], A, s->stream));
+  BHR_CUDA_TRY(launch_stage(3, s->tq[2], s->tp[2], s->tu, A, s->stream));
   BHR_CUDA_TRY(mark(4));
   ExtractArgs E{};
   E.u = s->u0;
