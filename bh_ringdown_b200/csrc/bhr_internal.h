@@ -94,12 +94,24 @@ struct ExtractArgs {
 };
 
 // Launchers (bhr_kernels.cu).
+// Tensor maps a stage kernel reads through: the input state (q with halo,
+// p with column halo), u^n (bare tile, stages 2 and 3), the per-point
+// coefficient planes (bb with column halo; 1/bir and ee) and the column
+// factor table.
+struct StageMaps {
+  CUtensorMap q, p, u, coef_bb, coef_ie, colf;
+};
+
 // Tensor maps of one state (four M x N planes): q planes with the +-3 row
 // and +-4 column halo, p planes with the column halo, and (tm_u, may be
 // null) the bare tile of all four planes for reading u^n.
 cudaError_t encode_state_maps(void *planes, int N, int M, CUtensorMap *tm_q, CUtensorMap *tm_p, CUtensorMap *tm_u);
-cudaError_t launch_stage(int stage, const CUtensorMap &tm_q, const CUtensorMap &tm_p, const CUtensorMap &tm_u,
-                         const StageArgs &a, cudaStream_t st);
+cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st);
+// Per-point coefficient planes [bb | 1/bir | ee] (3 x M x N) from the tables,
+// and the tensor maps over them and over the column table.
+cudaError_t launch_coef_tables(const double *coltab, const double *rowtab, double *ctab, int N, int M,
+                               cudaStream_t st);
+cudaError_t encode_coef_maps(double *ctab, const double *coltab, int N, int M, StageMaps *maps);
 cudaError_t launch_source(const SourceArgs &a, cudaStream_t st);
 cudaError_t launch_extract(const ExtractArgs &a, cudaStream_t st);
 cudaError_t launch_closure(double *planes, int N, int M, int even_m, cudaStream_t st);

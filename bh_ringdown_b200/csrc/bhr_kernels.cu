@@ -24,6 +24,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <type_traits>
 
 namespace bhr {
 
@@ -73,6 +74,14 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // ---- stencils (HighOrder/kern.cu:192-261) ---------------------------------
 __device__ __forceinline__ double d1c(const double *v, int c) {
   return 45.0 * (v[c + 1] - v[c - 1]) - 9.0 * (v[c + 2] - v[c - 2]) + (v[c + 3] - v[c - 3]);
@@ -106,26 +115,43 @@ __device__ __forceinline__ double sqrt_nr(double x) {
   return x > 0.0 ? s : 0.0;
 }
 
-// Column factors the main pass reads per point, in this order.
-constexpr int kColFields = 9;
-__device__ __constant__ int kColFieldIds[kColFields] = {CF_CCN, CF_XR, CF_YR, CF_BI0, CF_BI1,
-                                                        CF_BRI, CF_CR0, CF_CR1, CF_CIN};
+// Column factors the main pass reads per point: rows CF_CCN..CF_CIN of the
+// column table, in enum order.
+constexpr int kColFields = CF_COUNT - CF_CCN;
+enum { K_CCN = 0, K_XR, K_YR, K_CR0, K_CR1, K_BI0, K_BI1, K_BRI, K_CIN };
 
 struct __align__(128) StageSmem {
-  double q[2][QR][WC];          // TMA box {WC, QR, 2} of planes q_re, q_im
-  double p[2][TR][WC];          // TMA box {WC, TR, 2} of planes p_re, p_im
-  double bb[TR][WC];            // bb on the window columns (for d bb/dx)
-  double ib[TR][TC];            // 1/bir on the tile columns
-  double ee[TR][TC];            // ee = Ataurho + bb on the tile columns
-  double cf[kColFields][TC];    // column factors of the tile columns
-  double un[4][TR][TC];         // TMA box {TC, TR, 4} of u^n (stages 2 and 3)
+  double q[2][QR][WC];          // TMA box {WC, QR, 2}: planes q_re, q_im with halo
+  double p[2][TR][WC];          // TMA box {WC, TR, 2}: planes p_re, p_im with column halo
+  double bb[TR][WC];            // TMA box {WC, TR, 1}: bb on the window columns
+  double ie[2][TR][TC];         // TMA box {TC, TR, 2}: 1/bir and ee on the tile columns
+  double cf[kColFields][TC];    // TMA box {TC, 9}: column factors of the tile columns
+  double un[4][TR][TC];         // TMA box {TC, TR, 4}: u^n (stages 2 and 3)
   uint64_t bar;
 };
 
+// Time-independent per-point coefficients bb, 1/bir and ee
+// (HighOrder/kern.cu:132-149) for the interior rows, once per solve.
+__global__ void coef_table_kernel(const double *coltab, const double *rowtab, double *ctab, int N, int M) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
+  if (a >= N) return;
+  const size_t NM = static_cast<size_t>(N) * M, id = static_cast<size_t>(b) * N + a;
+  double bb = 0.0, ib = 0.0, ee = 0.0;
+  if (b >= 3 && b < M - 3) {
+    ib = rcp_nr(fma(coltab[CF_B1 * N + a], rowtab[RF_S2 * M + b], coltab[CF_B0 * N + a]));
+    const double At = coltab[CF_ATN * N + a] * ib, Ar = coltab[CF_ARN * N + a] * ib;
+    bb = -(At + sqrt_nr(fma(At, At, 4.0 * Ar))) * 0.5;
+    ee = At + bb;
+  }
+  ctab[id] = bb;
+  ctab[NM + id] = ib;
+  ctab[2 * NM + id] = ee;
+}
+
 template <int STAGE>
 __global__ void __launch_bounds__(STAGE_THREADS, 2)
-    stage_kernel(const __grid_constant__ CUtensorMap tm_q, const __grid_constant__ CUtensorMap tm_p,
-                 const __grid_constant__ CUtensorMap tm_u, const StageArgs A) {
+    stage_kernel(const __grid_constant__ StageMaps T, const StageArgs A) {
   extern __shared__ unsigned char smem_raw[];
   StageSmem &S = *reinterpret_cast<StageSmem *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
@@ -140,45 +166,18 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
   }
   __syncthreads();
   if (tid == 0) {
-    const uint32_t bytes = static_cast<uint32_t>(sizeof(S.q) + sizeof(S.p) + (STAGE == 1 ? 0 : sizeof(S.un)));
+    const uint32_t bytes = static_cast<uint32_t>(sizeof(S.q) + sizeof(S.p) + sizeof(S.bb) + sizeof(S.ie) +
+                                                 sizeof(S.cf) + (STAGE == 1 ? 0 : sizeof(S.un)));
     mbar_expect_tx(&S.bar, bytes);
-    tma_load_3d(&S.q[0][0][0], &tm_q, c0 - 4, b0 - 3, 0, &S.bar);
-    tma_load_3d(&S.p[0][0][0], &tm_p, c0 - 4, b0, 2, &S.bar);
-    if (STAGE != 1) tma_load_3d(&S.un[0][0][0], &tm_u, c0, b0, 0, &S.bar);
+    tma_load_3d(&S.q[0][0][0], &T.q, c0 - 4, b0 - 3, 0, &S.bar);
+    tma_load_3d(&S.p[0][0][0], &T.p, c0 - 4, b0, 2, &S.bar);
+    tma_load_3d(&S.bb[0][0], &T.coef_bb, c0 - 4, b0, 0, &S.bar);
+    tma_load_3d(&S.ie[0][0][0], &T.coef_ie, c0, b0, 1, &S.bar);
+    tma_load_2d(&S.cf[0][0], &T.colf, c0, CF_CCN, &S.bar);
+    if (STAGE != 1) tma_load_3d(&S.un[0][0][0], &T.u, c0, b0, 0, &S.bar);
   }
 
-  // While the tile is in flight: column factors of the tile columns, and
-  // bb on the window columns with 1/bir and ee on the tile columns
-  // (HighOrder/kern.cu:132-158).  Columns are lanes, rows are warps.
-  const double *ct = A.coltab;
   const double *rt = A.rowtab;
-  for (int i = tid; i < kColFields * TC; i += STAGE_THREADS) {
-    const int f = i / TC, col = i % TC;
-    const int a = c0 + col;
-    S.cf[f][col] = (a < N) ? __ldg(ct + kColFieldIds[f] * N + a) : 0.0;
-  }
-#pragma unroll
-  for (int wi = 0; wi < 3; wi++) {
-    const int w = tx + 1 + 32 * wi;
-    const int a = c0 - 4 + w;
-    if (w >= WC - 1 || a < 0 || a >= N) continue;
-    const double B0 = __ldg(ct + CF_B0 * N + a), B1 = __ldg(ct + CF_B1 * N + a);
-    const double ATN = __ldg(ct + CF_ATN * N + a), ARN = __ldg(ct + CF_ARN * N + a);
-#pragma unroll
-    for (int rj = 0; rj < TR / 8; rj++) {
-      const int r = ty + 8 * rj;
-      const int b = b0 + r;
-      if (b < 3 || b >= M - 3) continue;
-      const double ib = rcp_nr(fma(B1, __ldg(rt + RF_S2 * M + b), B0));
-      const double At = ATN * ib, Ar = ARN * ib;
-      const double bb = -(At + sqrt_nr(fma(At, At, 4.0 * Ar))) * 0.5;
-      S.bb[r][w] = bb;
-      if (w >= 4 && w < TC + 4) {
-        S.ib[r][w - 4] = ib;
-        S.ee[r][w - 4] = At + bb;
-      }
-    }
-  }
 
   const bool ok = mbar_wait_bounded(&S.bar, 0);
   if (!__syncthreads_and(ok)) {
@@ -250,12 +249,14 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
     src_r0 = rec.row0;
     tile_src = (src_c0 < c0 + TC) && (src_c0 + A.PTSX > c0) && (src_r0 < b0 + TR) && (src_r0 + A.PTSY > b0);
   }
-  // Tiles away from both radial ends need no per-column end checks.
-  const bool inner = !lo_cols && !hi_cols;
 
   const int a0 = c0 + 2 * tx;  // this thread's columns a0, a0+1
   const int w0 = 2 * tx + 4;   // their window column
   const double dt = A.dt;
+  // The row work, instantiated once for interior tiles (no per-column end
+  // checks) and once for tiles at a radial end.
+  auto rows = [&](auto inner_tag) {
+  constexpr bool inner = decltype(inner_tag)::value;
 #pragma unroll 1
   for (int rr = 0; rr < 2; rr++) {
     const int r = 2 * ty + rr;
@@ -298,10 +299,10 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
       bw[2 * j + 1] = t.y;
     }
     auto pair = [&](const double *base) { return *reinterpret_cast<const double2 *>(base + 2 * tx); };
-    const double2 ib2 = pair(S.ib[r]), ee2 = pair(S.ee[r]);
-    const double2 f0 = pair(S.cf[0]), f1 = pair(S.cf[1]), f2 = pair(S.cf[2]), f3 = pair(S.cf[3]),
-                  f4 = pair(S.cf[4]), f5 = pair(S.cf[5]), f6 = pair(S.cf[6]), f7 = pair(S.cf[7]),
-                  f8 = pair(S.cf[8]);
+    const double2 ib2 = pair(S.ie[0][r]), ee2 = pair(S.ie[1][r]);
+    const double2 f0 = pair(S.cf[K_CCN]), f1 = pair(S.cf[K_XR]), f2 = pair(S.cf[K_YR]), f3 = pair(S.cf[K_BI0]),
+                  f4 = pair(S.cf[K_BI1]), f5 = pair(S.cf[K_BRI]), f6 = pair(S.cf[K_CR0]), f7 = pair(S.cf[K_CR1]),
+                  f8 = pair(S.cf[K_CIN]);
 #pragma unroll
     for (int c = 0; c < 2; c++) {
       const int a = a0 + c;
@@ -330,8 +331,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
       }
       res[0][c] = 0.0;
       res[1][c] = 0.0;
-      res[2][c] = sre + cc * ll[0][c];
-      res[3][c] = sim + cc * ll[1][c];
+      res[2][c] = fma(cc, ll[0][c], sre);
+      res[3][c] = fma(cc, ll[1][c], sim);
     }
 
     // Radial first derivative and dissipation plane by plane, each folded
@@ -355,22 +356,23 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
         const double fx = d1c(v, 4 + c) * A.cx;
         const double fk = (inner || (a >= 4 && a < N - 4)) ? ko8c(v, 4 + c) * A.cko : 0.0;
         fc[pl][c] = f0;
+        // each plane's contribution is formed on its own, then added once
         if (pl == 0) {         // q_re
-          res[0][c] += -kbb[c] * fx - fk;
-          res[2][c] += kdre[c] * fx - kvre[c] * f0;
-          res[3][c] += kdim[c] * fx - kvim[c] * f0;
+          res[0][c] += fma(-kbb[c], fx, -fk);
+          res[2][c] += fma(kdre[c], fx, -kvre[c] * f0);
+          res[3][c] += fma(kdim[c], fx, -kvim[c] * f0);
         } else if (pl == 1) {  // q_im
-          res[1][c] += -kbb[c] * fx - fk;
-          res[2][c] += -kdim[c] * fx + kvim[c] * f0;
-          res[3][c] += kdre[c] * fx - kvre[c] * f0;
+          res[1][c] += fma(-kbb[c], fx, -fk);
+          res[2][c] += fma(-kdim[c], fx, kvim[c] * f0);
+          res[3][c] += fma(kdre[c], fx, -kvre[c] * f0);
         } else if (pl == 2) {  // p_re
           res[0][c] += f0;
-          res[2][c] += kee[c] * fx - fk - kare[c] * f0;
+          res[2][c] += fma(kee[c], fx, fma(-kare[c], f0, -fk));
           res[3][c] += -kaim[c] * f0;
         } else {               // p_im
           res[1][c] += f0;
           res[2][c] += kaim[c] * f0;
-          res[3][c] += kee[c] * fx - fk - kare[c] * f0;
+          res[3][c] += fma(kee[c], fx, fma(-kare[c], f0, -fk));
         }
       }
     }
@@ -403,6 +405,10 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
       }
     }
   }
+  };
+  if (!lo_cols && !hi_cols) rows(std::true_type{});
+  else rows(std::false_type{});
+
 }
 
 // ---- closure of stored planes (HighOrder/kern.cu:622-753) ------------------
@@ -593,15 +599,50 @@ __global__ void __launch_bounds__(kExtractThreads) extract_kernel(const ExtractA
 // ---- host launchers -------------------------------------------------------
 size_t stage_smem_bytes() { return sizeof(StageSmem) + 128; }
 
-cudaError_t encode_state_maps(void *planes, int N, int M, CUtensorMap *tm_q, CUtensorMap *tm_p, CUtensorMap *tm_u) {
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     cudaDriverEntryPointQueryResult qr;
     void *fn = nullptr;
     cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr);
-    if (e != cudaSuccess || qr != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
+    if (e != cudaSuccess || qr != cudaDriverEntryPointSuccess || !fn) return nullptr;
     encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   }
+  return encode;
+}
+
+cudaError_t encode_coef_maps(double *ctab, const double *coltab, int N, int M, StageMaps *maps) {
+  auto encode = tensor_map_encoder();
+  if (!encode) return cudaErrorNotSupported;
+  const cuuint64_t dims[3] = {static_cast<cuuint64_t>(N), static_cast<cuuint64_t>(M), 3};
+  const cuuint64_t strides[2] = {static_cast<cuuint64_t>(N) * 8, static_cast<cuuint64_t>(N) * M * 8};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const cuuint32_t box_bb[3] = {WC, TR, 1};
+  const cuuint32_t box_ie[3] = {TC, TR, 2};
+  const cuuint64_t cdims[2] = {static_cast<cuuint64_t>(N), CF_COUNT};
+  const cuuint64_t cstrides[1] = {static_cast<cuuint64_t>(N) * 8};
+  const cuuint32_t box_cf[2] = {TC, kColFields};
+  CUresult r1 = encode(&maps->coef_bb, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, ctab, dims, strides, box_bb, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r2 = encode(&maps->coef_ie, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, ctab, dims, strides, box_ie, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r3 = encode(&maps->colf, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(coltab), cdims, cstrides,
+                       box_cf, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                       CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return (r1 == CUDA_SUCCESS && r2 == CUDA_SUCCESS && r3 == CUDA_SUCCESS) ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+cudaError_t launch_coef_tables(const double *coltab, const double *rowtab, double *ctab, int N, int M,
+                               cudaStream_t st) {
+  coef_table_kernel<<<dim3((N + 255) / 256, M), 256, 0, st>>>(coltab, rowtab, ctab, N, M);
+  return cudaGetLastError();
+}
+
+cudaError_t encode_state_maps(void *planes, int N, int M, CUtensorMap *tm_q, CUtensorMap *tm_p, CUtensorMap *tm_u) {
+  auto encode = tensor_map_encoder();
+  if (!encode) return cudaErrorNotSupported;
   const cuuint64_t dims[3] = {static_cast<cuuint64_t>(N), static_cast<cuuint64_t>(M), 4};
   const cuuint64_t strides[2] = {static_cast<cuuint64_t>(N) * 8, static_cast<cuuint64_t>(N) * M * 8};
   const cuuint32_t estr[3] = {1, 1, 1};
@@ -623,13 +664,12 @@ cudaError_t encode_state_maps(void *planes, int N, int M, CUtensorMap *tm_q, CUt
   return (r1 == CUDA_SUCCESS && r2 == CUDA_SUCCESS && r3 == CUDA_SUCCESS) ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-cudaError_t launch_stage(int stage, const CUtensorMap &tm_q, const CUtensorMap &tm_p, const CUtensorMap &tm_u,
-                         const StageArgs &a, cudaStream_t st) {
+cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st) {
   const size_t smem = stage_smem_bytes();
   const dim3 grid(a.N / TC, a.M / TR), block(32, STAGE_THREADS / 32);
-  if (stage == 1) stage_kernel<1><<<grid, block, smem, st>>>(tm_q, tm_p, tm_u, a);
-  else if (stage == 2) stage_kernel<2><<<grid, block, smem, st>>>(tm_q, tm_p, tm_u, a);
-  else stage_kernel<3><<<grid, block, smem, st>>>(tm_q, tm_p, tm_u, a);
+  if (stage == 1) stage_kernel<1><<<grid, block, smem, st>>>(maps, a);
+  else if (stage == 2) stage_kernel<2><<<grid, block, smem, st>>>(maps, a);
+  else stage_kernel<3><<<grid, block, smem, st>>>(maps, a);
   return cudaGetLastError();
 }
 

@@ -25,12 +25,13 @@ constexpr int kNoAllocMaxPoints = 131072;  // N*M
 constexpr int kNoAllocMaxN = 16384;
 constexpr int kNoAllocMaxM = 1024;
 constexpr size_t kStageDoubles = 4 * static_cast<size_t>(kNoAllocMaxPoints);
-constexpr size_t kColOff = 2 * kStageDoubles;
+constexpr size_t kCoefOff = 2 * kStageDoubles;  // per-point coefficient planes
+constexpr size_t kColOff = kCoefOff + 3 * static_cast<size_t>(kNoAllocMaxPoints);
 constexpr size_t kRowOff = kColOff + static_cast<size_t>(CF_COUNT) * kNoAllocMaxN;
 constexpr size_t kFlagOff = kRowOff + static_cast<size_t>(RF_COUNT) * kNoAllocMaxM;
-constexpr size_t kScratchDoubles = kFlagOff + 32;  // about 10.1 MB in all
+constexpr size_t kScratchDoubles = kFlagOff + 32;  // about 13.3 MB in all
 
-// Scratch: [u1 | u2 | column tables | row tables | error flag].  In host code
+// Scratch: [u1 | u2 | coefficient planes | column tables | row tables | error flag].  In host code
 // this name is only a stand-in for the device symbol; the device address
 // comes from cudaGetSymbolAddress below.
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
@@ -77,7 +78,7 @@ extern "C" int bhr_step_noalloc(const bhr_params *p, double *state, int nsteps, 
   }
   double *scr = g_scratch[p->device];
   double *u1 = scr, *u2 = scr + kStageDoubles;
-  double *coltab = scr + kColOff, *rowtab = scr + kRowOff;
+  double *coltab = scr + kColOff, *rowtab = scr + kRowOff, *ctab = scr + kCoefOff;
   int *flag = reinterpret_cast<int *>(scr + kFlagOff);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
 
@@ -87,15 +88,20 @@ extern "C" int bhr_step_noalloc(const bhr_params *p, double *state, int nsteps, 
   const double dx = (p->Xmax - p->Xmin) / N, dth = kPiParm / M;
   fill_tables(*p, dx, h_r, h_th, h_col, h_row);
 
-  CUtensorMap tq[3], tp[3], tu;
+  StageMaps maps[3];
   double *bufs[3] = {state, u1, u2};
-  for (int i = 0; i < 3; i++)
-    if (encode_state_maps(bufs[i], N, M, &tq[i], &tp[i], i == 0 ? &tu : nullptr) != cudaSuccess)
+  for (int i = 0; i < 3; i++) {
+    CUtensorMap unused_q, unused_p;
+    if (encode_state_maps(state, N, M, &unused_q, &unused_p, &maps[i].u) != cudaSuccess ||
+        encode_state_maps(bufs[i], N, M, &maps[i].q, &maps[i].p, nullptr) != cudaSuccess ||
+        encode_coef_maps(ctab, coltab, N, M, &maps[i]) != cudaSuccess)
       return fail(BHR_CUDA_ERROR, "bhr_step_noalloc: cuTensorMapEncodeTiled failed (state must be 16-byte aligned)");
+  }
   // The tables must be current for this call; the flag must start at zero.
   if (cudaMemcpyAsync(coltab, h_col, sizeof(double) * CF_COUNT * N, cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(rowtab, h_row, sizeof(double) * RF_COUNT * M, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-      cudaMemsetAsync(flag, 0, sizeof(int), st) != cudaSuccess)
+      cudaMemsetAsync(flag, 0, sizeof(int), st) != cudaSuccess ||
+      launch_coef_tables(coltab, rowtab, ctab, N, M, st) != cudaSuccess)
     return fail(BHR_CUDA_ERROR, "bhr_step_noalloc: table upload failed");
 
   const double third = 0.33333333333333333;
@@ -118,11 +124,11 @@ extern "C" int bhr_step_noalloc(const bhr_params *p, double *state, int nsteps, 
   A.cko = 0.1 * 0.0625 * (1.0 / p->dt);
   for (int k = 0; k < nsteps; k++) {
     A.vin = state; A.un = state; A.out = u1;
-    if (launch_stage(1, tq[0], tp[0], tu, A, st) != cudaSuccess) return fail(BHR_CUDA_ERROR, "stage 1 launch failed");
+    if (launch_stage(1, maps[0], A, st) != cudaSuccess) return fail(BHR_CUDA_ERROR, "stage 1 launch failed");
     A.vin = u1; A.un = state; A.out = u2;
-    if (launch_stage(2, tq[1], tp[1], tu, A, st) != cudaSuccess) return fail(BHR_CUDA_ERROR, "stage 2 launch failed");
+    if (launch_stage(2, maps[1], A, st) != cudaSuccess) return fail(BHR_CUDA_ERROR, "stage 2 launch failed");
     A.vin = u2; A.un = state; A.out = state;
-    if (launch_stage(3, tq[2], tp[2], tu, A, st) != cudaSuccess) return fail(BHR_CUDA_ERROR, "stage 3 launch failed");
+    if (launch_stage(3, maps[2], A, st) != cudaSuccess) return fail(BHR_CUDA_ERROR, "stage 3 launch failed");
   }
   if (launch_closure(state, N, M, A.even_m, st) != cudaSuccess) return fail(BHR_CUDA_ERROR, "closure launch failed");
   int h_flag = 0;

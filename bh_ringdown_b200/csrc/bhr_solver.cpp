@@ -46,12 +46,12 @@ struct bhr_solver {
   cudaStream_t stream = nullptr;
   // device memory
   double *u0 = nullptr, *u1 = nullptr, *u2 = nullptr;
-  double *coltab = nullptr, *rowtab = nullptr, *rc = nullptr, *th = nullptr;
+  double *coltab = nullptr, *rowtab = nullptr, *ctab = nullptr, *rc = nullptr, *th = nullptr;
   double *src = nullptr, *ext = nullptr, *integ = nullptr, *wproj = nullptr, *wdedt = nullptr, *rows = nullptr;
   StepRec *recs = nullptr;
   RunState *rs = nullptr;
   size_t bytes = 0;
-  CUtensorMap tq[3], tp[3], tu;
+  StageMaps maps[3];  // per stage input state (u^n, u1, u2)
   int steps_done = 0;
   // Captured step graphs: one step, and kGraphBatch steps in one launch.
   cudaGraphExec_t g1 = nullptr, gb = nullptr;
@@ -102,7 +102,7 @@ int dalloc(bhr_solver *s, T **ptr, size_t count) {
 }
 
 void free_all(bhr_solver *s) {
-  void *ptrs[] = {s->u0, s->u1, s->u2, s->coltab, s->rowtab, s->rc, s->th, s->src, s->ext,
+  void *ptrs[] = {s->u0, s->u1, s->u2, s->coltab, s->rowtab, s->ctab, s->rc, s->th, s->src, s->ext,
                   s->integ, s->wproj, s->wdedt, s->rows, s->recs, s->rs};
   for (void *q : ptrs)
     if (q) cudaFree(q);
@@ -218,7 +218,8 @@ int bhr_solver_create(const bhr_params *pin, bhr_solver **out) {
   }
   if ((st = dalloc(s, &s->u0, 4 * NM)) || (st = dalloc(s, &s->u1, 4 * NM)) || (st = dalloc(s, &s->u2, 4 * NM)) ||
       (st = dalloc(s, &s->coltab, static_cast<size_t>(CF_COUNT) * p.N)) ||
-      (st = dalloc(s, &s->rowtab, static_cast<size_t>(RF_COUNT) * p.M)) || (st = dalloc(s, &s->rc, p.N)) ||
+      (st = dalloc(s, &s->rowtab, static_cast<size_t>(RF_COUNT) * p.M)) || (st = dalloc(s, &s->ctab, 3 * NM)) ||
+      (st = dalloc(s, &s->rc, p.N)) ||
       (st = dalloc(s, &s->th, p.M)) || (st = dalloc(s, &s->src, 2 * static_cast<size_t>(p.PTSX) * p.PTSY)) ||
       (st = dalloc(s, &s->ext, 2 * static_cast<size_t>(p.M))) || (st = dalloc(s, &s->integ, 4 * static_cast<size_t>(p.M))) ||
       (st = dalloc(s, &s->wproj, 7 * static_cast<size_t>(p.M))) || (st = dalloc(s, &s->wdedt, p.M)) ||
@@ -238,6 +239,7 @@ int bhr_solver_create(const bhr_params *pin, bhr_solver **out) {
       (e = up(s->rc, g.r_c.data(), g.r_c.size() * 8)) || (e = up(s->th, g.theta.data(), g.theta.size() * 8)) ||
       (e = up(s->wproj, w7.data(), w7.size() * 8)) || (e = up(s->wdedt, we.data(), we.size() * 8)) ||
       (e = up(s->u0, init.data(), init.size() * 8)) ||
+      (e = launch_coef_tables(s->coltab, s->rowtab, s->ctab, p.N, p.M, s->stream)) ||
       (e = cudaMemsetAsync(s->u1, 0, 4 * NM * 8, s->stream)) || (e = cudaMemsetAsync(s->u2, 0, 4 * NM * 8, s->stream)) ||
       (e = cudaMemsetAsync(s->integ, 0, 4 * p.M * 8, s->stream)) || (e = cudaMemsetAsync(s->ext, 0, 2 * p.M * 8, s->stream)) ||
       (e = cudaMemsetAsync(s->src, 0, 2 * static_cast<size_t>(p.PTSX) * p.PTSY * 8, s->stream)) ||
@@ -249,7 +251,11 @@ int bhr_solver_create(const bhr_params *pin, bhr_solver **out) {
   }
   double *bufs[3] = {s->u0, s->u1, s->u2};
   for (int i = 0; i < 3; i++) {
-    if (encode_state_maps(bufs[i], p.N, p.M, &s->tq[i], &s->tp[i], i == 0 ? &s->tu : nullptr) != cudaSuccess) {
+    StageMaps &m = s->maps[i];
+    CUtensorMap unused_q, unused_p;
+    if (encode_state_maps(s->u0, p.N, p.M, &unused_q, &unused_p, &m.u) != cudaSuccess ||
+        encode_state_maps(bufs[i], p.N, p.M, &m.q, &m.p, nullptr) != cudaSuccess ||
+        encode_coef_maps(s->ctab, s->coltab, p.N, p.M, &m) != cudaSuccess) {
       set_error("cuTensorMapEncodeTiled failed");
       free_all(s);
       delete s;
@@ -436,13 +442,13 @@ static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
   }
   BHR_CUDA_TRY(mark(1));
   A.vin = s->u0; A.un = s->u0; A.out = s->u1;
-  BHR_CUDA_TRY(launch_stage(1, s->tq[0], s->tp[0], s->tu, A, s->stream));
+  BHR_CUDA_TRY(launch_stage(1, s->maps[0], A, s->stream));
   BHR_CUDA_TRY(mark(2));
   A.vin = s->u1; A.un = s->u0; A.out = s->u2;
-  BHR_CUDA_TRY(launch_stage(2, s->tq[1], s->tp[1], s->tu, A, s->stream));
+  BHR_CUDA_TRY(launch_stage(2, s->maps[1], A, s->stream));
   BHR_CUDA_TRY(mark(3));
   A.vin = s->u2; A.un = s->u0; A.out = s->u0;
-  BHR_CUDA_TRY(launch_stage(3, s->tq[2], s->tp[2], s->tu, A, s->stream));
+  BHR_CUDA_TRY(launch_stage(3, s->maps[2], A, s->stream));
   BHR_CUDA_TRY(mark(4));
   ExtractArgs E{};
   E.u = s->u0;
