@@ -13,9 +13,8 @@ namespace bhr {
 // HighOrder/kern.cu:247-256) and 3 rows each side for q (the 6th-order
 // theta stencils reach +-3, HighOrder/kern.cu:206-222).
 constexpr int TC = 64;
-constexpr int TR = 16;
+constexpr int TR = 16;       // largest tile height; tiles are 8 or 16 rows
 constexpr int WC = TC + 8;   // window columns
-constexpr int QR = TR + 6;   // q window rows
 constexpr int STAGE_THREADS = 256;
 
 // Per-column coefficient factors (host-built, FP64).  With bir = B0 +
@@ -68,6 +67,7 @@ struct StageArgs {
   int *err;
   int N, M, PTSX, PTSY;
   int even_m;
+  int rows;             // tile height: 8 or 16 theta rows
   double dt, cx, cy, cyy, cko;
 };
 
@@ -105,13 +105,14 @@ struct StageMaps {
 // Tensor maps of one state (four M x N planes): q planes with the +-3 row
 // and +-4 column halo, p planes with the column halo, and (tm_u, may be
 // null) the bare tile of all four planes for reading u^n.
-cudaError_t encode_state_maps(void *planes, int N, int M, CUtensorMap *tm_q, CUtensorMap *tm_p, CUtensorMap *tm_u);
+cudaError_t encode_state_maps(void *planes, int N, int M, int rows, CUtensorMap *tm_q, CUtensorMap *tm_p,
+                              CUtensorMap *tm_u);
 cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st);
 // Per-point coefficient planes [bb | 1/bir | ee] (3 x M x N) from the tables,
 // and the tensor maps over them and over the column table.
 cudaError_t launch_coef_tables(const double *coltab, const double *rowtab, double *ctab, int N, int M,
                                cudaStream_t st);
-cudaError_t encode_coef_maps(double *ctab, const double *coltab, int N, int M, StageMaps *maps);
+cudaError_t encode_coef_maps(double *ctab, const double *coltab, int N, int M, int rows, StageMaps *maps);
 cudaError_t launch_source(const SourceArgs &a, cudaStream_t st);
 cudaError_t launch_extract(const ExtractArgs &a, cudaStream_t st);
 cudaError_t launch_closure(double *planes, int N, int M, int even_m, cudaStream_t st);

@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <type_traits>
+#include <utility>
 
 namespace bhr {
 
@@ -65,6 +66,11 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase)
     if (mbar_try_wait(bar, phase)) return true;
   return false;
 }
+// Programmatic dependent launch: wait for the kernels this one depends on
+// (their writes become visible), and let the next kernel start launching.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // 3D tiled TMA load, no multicast.
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
   asm volatile(
@@ -120,13 +126,15 @@ __device__ __forceinline__ double sqrt_nr(double x) {
 constexpr int kColFields = CF_COUNT - CF_CCN;
 enum { K_CCN = 0, K_XR, K_YR, K_CR0, K_CR1, K_BI0, K_BI1, K_BRI, K_CIN };
 
+// Shared memory of one tile of ROWS theta rows (8 or 16).
+template <int ROWS>
 struct __align__(128) StageSmem {
-  double q[2][QR][WC];          // TMA box {WC, QR, 2}: planes q_re, q_im with halo
-  double p[2][TR][WC];          // TMA box {WC, TR, 2}: planes p_re, p_im with column halo
-  double bb[TR][WC];            // TMA box {WC, TR, 1}: bb on the window columns
-  double ie[2][TR][TC];         // TMA box {TC, TR, 2}: 1/bir and ee on the tile columns
+  double q[2][ROWS + 6][WC];    // TMA box {WC, ROWS+6, 2}: planes q_re, q_im with halo
+  double p[2][ROWS][WC];        // TMA box {WC, ROWS, 2}: planes p_re, p_im with column halo
+  double bb[ROWS][WC];          // TMA box {WC, ROWS, 1}: bb on the window columns
+  double ie[2][ROWS][TC];       // TMA box {TC, ROWS, 2}: 1/bir and ee on the tile columns
   double cf[kColFields][TC];    // TMA box {TC, 9}: column factors of the tile columns
-  double un[4][TR][TC];         // TMA box {TC, TR, 4}: u^n (stages 2 and 3)
+  double un[4][ROWS][TC];       // TMA box {TC, ROWS, 4}: u^n (stages 2 and 3)
   uint64_t bar;
 };
 
@@ -149,11 +157,13 @@ __global__ void coef_table_kernel(const double *coltab, const double *rowtab, do
   ctab[2 * NM + id] = ee;
 }
 
-template <int STAGE>
+template <int STAGE, int ROWS>
 __global__ void __launch_bounds__(STAGE_THREADS, 2)
     stage_kernel(const __grid_constant__ StageMaps T, const StageArgs A) {
+  constexpr int TR = ROWS;           // tile rows
+  constexpr int RPT = ROWS / 8;      // rows per thread
   extern __shared__ unsigned char smem_raw[];
-  StageSmem &S = *reinterpret_cast<StageSmem *>(
+  StageSmem<ROWS> &S = *reinterpret_cast<StageSmem<ROWS> *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
   const int c0 = blockIdx.x * TC, b0 = blockIdx.y * TR;
@@ -169,11 +179,18 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
     const uint32_t bytes = static_cast<uint32_t>(sizeof(S.q) + sizeof(S.p) + sizeof(S.bb) + sizeof(S.ie) +
                                                  sizeof(S.cf) + (STAGE == 1 ? 0 : sizeof(S.un)));
     mbar_expect_tx(&S.bar, bytes);
-    tma_load_3d(&S.q[0][0][0], &T.q, c0 - 4, b0 - 3, 0, &S.bar);
-    tma_load_3d(&S.p[0][0][0], &T.p, c0 - 4, b0, 2, &S.bar);
+    // Coefficient planes and column factors are written once, at set-up:
+    // they can be requested before the previous kernel has finished.
     tma_load_3d(&S.bb[0][0], &T.coef_bb, c0 - 4, b0, 0, &S.bar);
     tma_load_3d(&S.ie[0][0][0], &T.coef_ie, c0, b0, 1, &S.bar);
     tma_load_2d(&S.cf[0][0], &T.colf, c0, CF_CCN, &S.bar);
+  }
+  // Everything below reads what the earlier kernels of the step wrote.
+  grid_dependency_wait();
+  launch_dependents();
+  if (tid == 0) {
+    tma_load_3d(&S.q[0][0][0], &T.q, c0 - 4, b0 - 3, 0, &S.bar);
+    tma_load_3d(&S.p[0][0][0], &T.p, c0 - 4, b0, 2, &S.bar);
     if (STAGE != 1) tma_load_3d(&S.un[0][0][0], &T.u, c0, b0, 0, &S.bar);
   }
 
@@ -258,8 +275,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
   auto rows = [&](auto inner_tag) {
   constexpr bool inner = decltype(inner_tag)::value;
 #pragma unroll 1
-  for (int rr = 0; rr < 2; rr++) {
-    const int r = 2 * ty + rr;
+  for (int rr = 0; rr < RPT; rr++) {
+    const int r = RPT * ty + rr;
     const int b = b0 + r;
     if (b < 3 || b >= M - 3) continue;
     if (!inner && (a0 + 1 < 3 || a0 >= N - 3)) continue;
@@ -481,6 +498,8 @@ __global__ void closure_ends_kernel(double *P, int N, int M) {
 
 // ---- particle source patch (HighOrder/kern.cu:1185-1227, 2666-2683) ---------
 __global__ void source_patch_kernel(const SourceArgs A) {
+  grid_dependency_wait();
+  launch_dependents();
   const int j = blockIdx.x, k = threadIdx.x;
   if (k >= A.PTSX) return;
   const StepRec &rec = A.recs[A.rs->k];
@@ -533,6 +552,8 @@ constexpr int kSums = 15;
 __global__ void __launch_bounds__(kExtractThreads) extract_kernel(const ExtractArgs A) {
   __shared__ double red[kExtractThreads / 32][kSums];
   __shared__ int nan_flag;
+  grid_dependency_wait();
+  launch_dependents();
   const int tid = threadIdx.x;
   const int N = A.N, M = A.M;
   const size_t NM = static_cast<size_t>(N) * M;
@@ -597,7 +618,7 @@ __global__ void __launch_bounds__(kExtractThreads) extract_kernel(const ExtractA
 }  // namespace
 
 // ---- host launchers -------------------------------------------------------
-size_t stage_smem_bytes() { return sizeof(StageSmem) + 128; }
+size_t stage_smem_bytes() { return sizeof(StageSmem<16>) + 128; }
 
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
@@ -611,14 +632,15 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return encode;
 }
 
-cudaError_t encode_coef_maps(double *ctab, const double *coltab, int N, int M, StageMaps *maps) {
+cudaError_t encode_coef_maps(double *ctab, const double *coltab, int N, int M, int rows, StageMaps *maps) {
+  const cuuint32_t TRb = static_cast<cuuint32_t>(rows);
   auto encode = tensor_map_encoder();
   if (!encode) return cudaErrorNotSupported;
   const cuuint64_t dims[3] = {static_cast<cuuint64_t>(N), static_cast<cuuint64_t>(M), 3};
   const cuuint64_t strides[2] = {static_cast<cuuint64_t>(N) * 8, static_cast<cuuint64_t>(N) * M * 8};
   const cuuint32_t estr[3] = {1, 1, 1};
-  const cuuint32_t box_bb[3] = {WC, TR, 1};
-  const cuuint32_t box_ie[3] = {TC, TR, 2};
+  const cuuint32_t box_bb[3] = {WC, TRb, 1};
+  const cuuint32_t box_ie[3] = {TC, TRb, 2};
   const cuuint64_t cdims[2] = {static_cast<cuuint64_t>(N), CF_COUNT};
   const cuuint64_t cstrides[1] = {static_cast<cuuint64_t>(N) * 8};
   const cuuint32_t box_cf[2] = {TC, kColFields};
@@ -640,14 +662,16 @@ cudaError_t launch_coef_tables(const double *coltab, const double *rowtab, doubl
   return cudaGetLastError();
 }
 
-cudaError_t encode_state_maps(void *planes, int N, int M, CUtensorMap *tm_q, CUtensorMap *tm_p, CUtensorMap *tm_u) {
+cudaError_t encode_state_maps(void *planes, int N, int M, int rows, CUtensorMap *tm_q, CUtensorMap *tm_p,
+                              CUtensorMap *tm_u) {
+  const cuuint32_t TRb = static_cast<cuuint32_t>(rows);
   auto encode = tensor_map_encoder();
   if (!encode) return cudaErrorNotSupported;
   const cuuint64_t dims[3] = {static_cast<cuuint64_t>(N), static_cast<cuuint64_t>(M), 4};
   const cuuint64_t strides[2] = {static_cast<cuuint64_t>(N) * 8, static_cast<cuuint64_t>(N) * M * 8};
   const cuuint32_t estr[3] = {1, 1, 1};
-  const cuuint32_t box_q[3] = {WC, QR, 2};
-  const cuuint32_t box_p[3] = {WC, TR, 2};
+  const cuuint32_t box_q[3] = {WC, TRb + 6, 2};
+  const cuuint32_t box_p[3] = {WC, TRb, 2};
   CUresult r1 = encode(tm_q, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, planes, dims, strides, box_q, estr,
                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -656,7 +680,7 @@ cudaError_t encode_state_maps(void *planes, int N, int M, CUtensorMap *tm_q, CUt
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   CUresult r3 = CUDA_SUCCESS;
   if (tm_u) {
-    const cuuint32_t box_u[3] = {TC, TR, 4};
+    const cuuint32_t box_u[3] = {TC, TRb, 4};
     r3 = encode(tm_u, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, planes, dims, strides, box_u, estr,
                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -664,34 +688,58 @@ cudaError_t encode_state_maps(void *planes, int N, int M, CUtensorMap *tm_q, CUt
   return (r1 == CUDA_SUCCESS && r2 == CUDA_SUCCESS && r3 == CUDA_SUCCESS) ? cudaSuccess : cudaErrorInvalidValue;
 }
 
+// Launch with programmatic stream serialisation allowed: the kernel may
+// begin while its predecessor on the stream drains, and holds every read
+// of the predecessor's results behind grid_dependency_wait().
+template <class... KArgs, class... Args>
+static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+template <int ROWS>
+static cudaError_t launch_rows(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st) {
+  const size_t smem = sizeof(StageSmem<ROWS>) + 128;
+  const dim3 grid(a.N / TC, a.M / ROWS), block(32, STAGE_THREADS / 32);
+  if (stage == 1) return launch_pdl(stage_kernel<1, ROWS>, grid, block, smem, st, maps, a);
+  if (stage == 2) return launch_pdl(stage_kernel<2, ROWS>, grid, block, smem, st, maps, a);
+  return launch_pdl(stage_kernel<3, ROWS>, grid, block, smem, st, maps, a);
+}
+
 cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st) {
-  const size_t smem = stage_smem_bytes();
-  const dim3 grid(a.N / TC, a.M / TR), block(32, STAGE_THREADS / 32);
-  if (stage == 1) stage_kernel<1><<<grid, block, smem, st>>>(maps, a);
-  else if (stage == 2) stage_kernel<2><<<grid, block, smem, st>>>(maps, a);
-  else stage_kernel<3><<<grid, block, smem, st>>>(maps, a);
-  return cudaGetLastError();
+  return a.rows == 8 ? launch_rows<8>(stage, maps, a, st) : launch_rows<16>(stage, maps, a, st);
 }
 
 // Once per device (the attribute is per device context).
 cudaError_t prepare_kernels() {
-  const int smem = static_cast<int>(stage_smem_bytes());
+  const int s8 = static_cast<int>(sizeof(StageSmem<8>) + 128), s16 = static_cast<int>(sizeof(StageSmem<16>) + 128);
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(stage_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) ||
-      (e = cudaFuncSetAttribute(stage_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) ||
-      (e = cudaFuncSetAttribute(stage_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)))
+  if ((e = cudaFuncSetAttribute(stage_kernel<1, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
+      (e = cudaFuncSetAttribute(stage_kernel<2, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
+      (e = cudaFuncSetAttribute(stage_kernel<3, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
+      (e = cudaFuncSetAttribute(stage_kernel<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)) ||
+      (e = cudaFuncSetAttribute(stage_kernel<2, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)) ||
+      (e = cudaFuncSetAttribute(stage_kernel<3, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)))
     return e;
   return cudaSuccess;
 }
 
 cudaError_t launch_source(const SourceArgs &a, cudaStream_t st) {
-  source_patch_kernel<<<a.PTSY, a.PTSX, 0, st>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(source_patch_kernel, dim3(a.PTSY), dim3(a.PTSX), 0, st, a);
 }
 
 cudaError_t launch_extract(const ExtractArgs &a, cudaStream_t st) {
-  extract_kernel<<<1, kExtractThreads, 0, st>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(extract_kernel, dim3(1), dim3(kExtractThreads), 0, st, a);
 }
 
 cudaError_t launch_closure(double *planes, int N, int M, int even_m, cudaStream_t st) {

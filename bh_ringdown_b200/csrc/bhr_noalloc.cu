@@ -92,9 +92,9 @@ extern "C" int bhr_step_noalloc(const bhr_params *p, double *state, int nsteps, 
   double *bufs[3] = {state, u1, u2};
   for (int i = 0; i < 3; i++) {
     CUtensorMap unused_q, unused_p;
-    if (encode_state_maps(state, N, M, &unused_q, &unused_p, &maps[i].u) != cudaSuccess ||
-        encode_state_maps(bufs[i], N, M, &maps[i].q, &maps[i].p, nullptr) != cudaSuccess ||
-        encode_coef_maps(ctab, coltab, N, M, &maps[i]) != cudaSuccess)
+    if (encode_state_maps(state, N, M, TR, &unused_q, &unused_p, &maps[i].u) != cudaSuccess ||
+        encode_state_maps(bufs[i], N, M, TR, &maps[i].q, &maps[i].p, nullptr) != cudaSuccess ||
+        encode_coef_maps(ctab, coltab, N, M, TR, &maps[i]) != cudaSuccess)
       return fail(BHR_CUDA_ERROR, "bhr_step_noalloc: cuTensorMapEncodeTiled failed (state must be 16-byte aligned)");
   }
   // The tables must be current for this call; the flag must start at zero.
@@ -117,6 +117,7 @@ extern "C" int bhr_step_noalloc(const bhr_params *p, double *state, int nsteps, 
   A.PTSX = p->PTSX;
   A.PTSY = p->PTSY;
   A.even_m = (static_cast<int>(p->m) % 2) == 0 ? 1 : 0;
+  A.rows = TR;
   A.dt = p->dt;
   A.cx = 0.016666666666667 * (1.0 / dx);
   A.cy = 0.05 * third * (1.0 / dth);

@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <array>
 #include <mutex>
 #include <sstream>
 #include <string>
@@ -52,6 +53,7 @@ struct bhr_solver {
   RunState *rs = nullptr;
   size_t bytes = 0;
   StageMaps maps[3];  // per stage input state (u^n, u1, u2)
+  int tile_rows = 16; // stage tile height chosen for this grid
   int steps_done = 0;
   // Captured step graphs: one step, and kGraphBatch steps in one launch.
   cudaGraphExec_t g1 = nullptr, gb = nullptr;
@@ -122,6 +124,8 @@ double tortoise(double r, double a, double rpl, double rmn) {
 }  // namespace
 
 extern "C" {
+
+static int autotune_rows(bhr_solver *s);
 
 int bhr_abi_version(void) { return BHR_ABI_VERSION; }
 const char *bhr_last_error_string(void) { return g_err.c_str(); }
@@ -249,18 +253,10 @@ int bhr_solver_create(const bhr_params *pin, bhr_solver **out) {
     delete s;
     return BHR_CUDA_ERROR;
   }
-  double *bufs[3] = {s->u0, s->u1, s->u2};
-  for (int i = 0; i < 3; i++) {
-    StageMaps &m = s->maps[i];
-    CUtensorMap unused_q, unused_p;
-    if (encode_state_maps(s->u0, p.N, p.M, &unused_q, &unused_p, &m.u) != cudaSuccess ||
-        encode_state_maps(bufs[i], p.N, p.M, &m.q, &m.p, nullptr) != cudaSuccess ||
-        encode_coef_maps(s->ctab, s->coltab, p.N, p.M, &m) != cudaSuccess) {
-      set_error("cuTensorMapEncodeTiled failed");
-      free_all(s);
-      delete s;
-      return BHR_CUDA_ERROR;
-    }
+  if (int st = autotune_rows(s)) {
+    free_all(s);
+    delete s;
+    return st;
   }
   *out = s;
   return BHR_OK;
@@ -290,6 +286,7 @@ int bhr_solver_info(const bhr_solver *s, bhr_info *info) {
   info->has_source = s->has_source ? 1 : 0;
   info->r_plus = s->g.r_plus;
   info->device_bytes = s->bytes;
+  info->tile_rows = s->tile_rows;
   return BHR_OK;
 }
 
@@ -400,8 +397,73 @@ int bhr_solver_load_trajectory(bhr_solver *s, const char *path) {
   return bhr_solver_set_trajectory(s, rows.data(), static_cast<int>(rows.size() / 10));
 }
 
-static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
-  auto mark = [&](int i) { return ev ? cudaEventRecord(ev[i], s->stream) : cudaSuccess; };
+static int encode_maps(bhr_solver *s, int rows) {
+  const bhr_params &p = s->p;
+  double *bufs[3] = {s->u0, s->u1, s->u2};
+  for (int i = 0; i < 3; i++) {
+    StageMaps &m = s->maps[i];
+    CUtensorMap unused_q, unused_p;
+    if (encode_state_maps(s->u0, p.N, p.M, rows, &unused_q, &unused_p, &m.u) != cudaSuccess ||
+        encode_state_maps(bufs[i], p.N, p.M, rows, &m.q, &m.p, nullptr) != cudaSuccess ||
+        encode_coef_maps(s->ctab, s->coltab, p.N, p.M, rows, &m) != cudaSuccess) {
+      set_error("cuTensorMapEncodeTiled failed");
+      return BHR_CUDA_ERROR;
+    }
+  }
+  s->tile_rows = rows;
+  return BHR_OK;
+}
+
+static StageArgs stage_args(bhr_solver *s);
+
+// Tile-height autotuner: per (device, N, M) the stage kernels are timed with
+// 8- and 16-row tiles on stages 1 and 2, which write only the solve's
+// scratch stages (u1, u2), and the faster height is kept for the process.
+static int autotune_rows(bhr_solver *s) {
+  static std::mutex mu;
+  static std::vector<std::array<int, 4>> cache;  // device, N, M, rows
+  const bhr_params &p = s->p;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto &c : cache)
+      if (c[0] == p.device && c[1] == p.N && c[2] == p.M) return encode_maps(s, c[3]);
+  }
+  static const int cands[2] = {8, 16};
+  double best_ms = 1e30;
+  int best = 16;
+  cudaEvent_t e0, e1;
+  BHR_CUDA_TRY(cudaEventCreate(&e0));
+  BHR_CUDA_TRY(cudaEventCreate(&e1));
+  for (int rows : cands) {
+    if (int st = encode_maps(s, rows)) return st;
+    StageArgs A = stage_args(s);
+    A.src = nullptr;
+    for (int rep = 0; rep < 6; rep++) {
+      if (rep == 2) BHR_CUDA_TRY(cudaEventRecord(e0, s->stream));
+      A.vin = s->u0; A.un = s->u0; A.out = s->u1;
+      BHR_CUDA_TRY(launch_stage(1, s->maps[0], A, s->stream));
+      A.vin = s->u1; A.un = s->u0; A.out = s->u2;
+      BHR_CUDA_TRY(launch_stage(2, s->maps[1], A, s->stream));
+    }
+    BHR_CUDA_TRY(cudaEventRecord(e1, s->stream));
+    BHR_CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    BHR_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = rows;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    cache.push_back({p.device, p.N, p.M, best});
+  }
+  return encode_maps(s, best);
+}
+
+static StageArgs stage_args(bhr_solver *s) {
   const bhr_params &p = s->p;
   const double odx = 1.0 / s->g.dx, odth = 1.0 / s->g.dtheta, odt = 1.0 / p.dt;
   const double third = 0.33333333333333333;
@@ -417,11 +479,19 @@ static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
   A.PTSX = p.PTSX;
   A.PTSY = p.PTSY;
   A.even_m = s->even_m ? 1 : 0;
+  A.rows = s->tile_rows;
   A.dt = p.dt;
   A.cx = 0.016666666666667 * odx;
   A.cy = 0.05 * third * odth;
   A.cyy = 0.05 * third * third * odth * odth;
   A.cko = 0.1 * 0.0625 * odt;
+  return A;
+}
+
+static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
+  auto mark = [&](int i) { return ev ? cudaEventRecord(ev[i], s->stream) : cudaSuccess; };
+  const bhr_params &p = s->p;
+  StageArgs A = stage_args(s);
   BHR_CUDA_TRY(mark(0));
   if (s->has_source) {
     SourceArgs S{};

@@ -100,6 +100,7 @@ typedef struct bhr_info {
   int has_source;
   double r_plus;
   size_t device_bytes;
+  int tile_rows;      /* stage tile height the autotuner chose (8 or 16)   */
 } bhr_info;
 
 typedef struct bhr_solver bhr_solver;
