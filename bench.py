@@ -24,7 +24,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import subprocess
 import sys
 import time
 
@@ -75,59 +74,64 @@ def profile_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and throttle reasons sampled through NVML every few ms while
+    the timed region runs (read-only queries)."""
 
-    def __init__(self, device_index):
-        self.dev = device_index
-        self.proc = None
-        self.path = os.path.join("/tmp", f"bhr_clocks_{os.getpid()}.csv")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
+
+    def __init__(self, cuda_device):
+        self.dev = cuda_device
+        self.samples = []
+        self.stop = None
+        self.thread = None
+        self.max_mhz = None
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.dev)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.dev)
 
     def __enter__(self):
+        import threading
         try:
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=clocks.sm,clocks.max.sm,"
-                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+            import pynvml
+            h = self._handle()
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            self.stop = threading.Event()
+
+            def run():
+                while not self.stop.is_set():
+                    try:
+                        mhz = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                        rs = pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                        self.samples.append((mhz, rs))
+                    except Exception:
+                        pass
+                    time.sleep(0.002)
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
         except Exception:
-            self.proc = None
+            self.thread = None
         return self
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
-            self.f.close()
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=2)
 
     def summary(self):
-        if self.proc is None:
+        if not self.samples:
             return None
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        try:
-            for line in open(self.path):
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) < 6:
-                    continue
-                try:
-                    sm.append(float(parts[0]))
-                    mx.append(float(parts[1]))
-                except ValueError:
-                    continue
-                for n, v in zip(names, parts[2:6]):
-                    if v.lower().startswith("active"):
-                        reasons.add(n)
-            os.remove(self.path)
-        except Exception:
-            return None
-        if not sm:
-            return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        mhz = [m for m, _ in self.samples]
+        reasons = sorted({n for _, r in self.samples for n, bit in self.REASONS.items() if r & bit})
+        return {"sm_mhz": float(np.median(mhz)), "sm_max_mhz": float(self.max_mhz or max(mhz)),
+                "reasons": reasons, "samples": len(mhz), "source": "NVML during the timed region"}
 
 
 def source_available():
@@ -200,6 +204,7 @@ def run_ours(args, rank, local_rank, world):
         for _ in range(args.steps):
             flush_l2()
             total_ms += solver.time_steps(1)
+        torch.cuda.synchronize()
     torch.cuda.synchronize()
     # per-kernel breakdown (eager launches, events around each kernel)
     per_kernel = np.zeros(5)
@@ -376,7 +381,7 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=2000)

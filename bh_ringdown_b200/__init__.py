@@ -59,6 +59,16 @@ class _Info(C.Structure):
                 ("tile_rows", I)]
 
 
+class _RequestInfo(C.Structure):
+    _fields_ = [("state", I), ("status", I), ("steps_total", I), ("steps_done", I), ("nrows", I),
+                ("submit_s", D), ("start_s", D), ("finish_s", D)]
+
+
+class _EngineStats(C.Structure):
+    _fields_ = [("queued", I), ("running", I), ("finished", I), ("tiles", I), ("batch_steps", C.c_longlong),
+                ("point_updates", D), ("bytes_in_use", C.c_size_t), ("budget", C.c_size_t)]
+
+
 @dataclass
 class Params:
     """Run parameters; defaults are the reference's (HighOrder/parm.h, main.c)."""
@@ -136,6 +146,13 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "bhr_swsh": (D, [D, D, D]),
         "bhr_write_waveform": (I, [C.c_char_p, C.c_char_p, D, dp, dp, dp, I]),
         "bhr_step_noalloc": (I, [P(_Params), vp, I, vp]),
+        "bhr_engine_create": (I, [I, C.c_size_t, P(vp)]),
+        "bhr_engine_destroy": (None, [vp]),
+        "bhr_engine_submit": (I, [vp, P(_Params), dp, I, P(C.c_int64)]),
+        "bhr_engine_step": (I, [vp, I, P(I)]),
+        "bhr_engine_poll": (I, [vp, C.c_int64, P(_RequestInfo)]),
+        "bhr_engine_result": (I, [vp, C.c_int64, dp, dp, dp, I, P(I)]),
+        "bhr_engine_stats": (I, [vp, P(_EngineStats)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -287,5 +304,78 @@ class Solver:
         return avg, float(tot[0])
 
 
-__all__ = ["Params", "Particle", "Solver", "BhrError", "grid", "swsh", "source_coefficients", "load_library",
+class Engine:
+    """Many solves on one device advanced together (bhr_engine_*): submit
+    requests at any time, call step() to advance everything running, and
+    collect each finished request's waveform with result()."""
+
+    QUEUED, RUNNING, DONE, FAILED = 1, 2, 3, 4
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 64 << 30):
+        self.lib = load_library()
+        h = C.c_void_p()
+        _check(self.lib.bhr_engine_create(int(device), int(hbm_budget_bytes), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.bhr_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, params: Params, traj: Optional[np.ndarray] = None) -> int:
+        p = params.to_c()
+        rid = C.c_int64(0)
+        if traj is None:
+            _check(self.lib.bhr_engine_submit(self._h, C.byref(p), None, 0, C.byref(rid)))
+        else:
+            rows = np.ascontiguousarray(traj, dtype=np.float64)
+            assert rows.ndim == 2 and rows.shape[1] == 10
+            _check(self.lib.bhr_engine_submit(self._h, C.byref(p), _ptr(rows), rows.shape[0], C.byref(rid)))
+        return rid.value
+
+    def step(self, max_steps: int) -> int:
+        running = I(0)
+        _check(self.lib.bhr_engine_step(self._h, int(max_steps), C.byref(running)))
+        return running.value
+
+    def poll(self, rid: int) -> dict:
+        inf = _RequestInfo()
+        _check(self.lib.bhr_engine_poll(self._h, int(rid), C.byref(inf)))
+        return {f[0]: getattr(inf, f[0]) for f in _RequestInfo._fields_}
+
+    def result(self, rid: int):
+        n_max = self.poll(rid)["nrows"]
+        t, h, e = np.zeros(n_max), np.zeros(n_max * 14), np.zeros(n_max)
+        n = I(0)
+        _check(self.lib.bhr_engine_result(self._h, int(rid), _ptr(t), _ptr(h), _ptr(e), n_max, C.byref(n)))
+        n = n.value
+        return t[:n], h[: n * 14].reshape(n, 14), e[:n]
+
+    def stats(self) -> dict:
+        st = _EngineStats()
+        _check(self.lib.bhr_engine_stats(self._h, C.byref(st)))
+        return {f[0]: getattr(st, f[0]) for f in _EngineStats._fields_}
+
+    def run_all(self, chunk: int = 1 << 30) -> None:
+        """Steps until nothing is queued or running."""
+        while True:
+            running = self.step(chunk)
+            st = self.stats()
+            if running == 0 and st["queued"] == 0:
+                return
+
+
+__all__ = ["Params", "Particle", "Solver", "Engine", "BhrError", "grid", "swsh", "source_coefficients", "load_library",
            "BHR_INIT_ZERO", "BHR_INIT_GAUSSIAN", "BHR_FP64", "BHR_MIXED", "BHR_SSPRK3"]

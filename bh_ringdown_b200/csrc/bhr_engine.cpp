@@ -1,0 +1,451 @@
+// bhr_engine.cpp -- many solves on one device, advanced together.
+//
+// The reference runs one solve per process (HighOrder/main.c:65-70 loops the
+// m modes; TD_GPU_code/run.sh submits one job per trajectory).  The engine
+// keeps every admitted solve's fields and tables resident, admits queued
+// requests while the HBM budget allows, and advances all running solves with
+// one launch per RK stage over a work-list of (solve, tile) pairs, captured
+// as a CUDA graph.  Requests arriving while others run join at the next
+// step boundary (continuous batching); finished solves leave with their
+// waveform.  Each tile is computed by the same code as a lone solve, so a
+// request's result does not depend on what it shares the GPU with.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "bhr.h"
+#include "bhr_host.h"
+#include "bhr_internal.h"
+#include "bhr_solver_impl.h"
+
+using namespace bhr;
+
+namespace {
+
+struct Request {
+  int64_t id;
+  bhr_params p;
+  std::vector<double> traj;
+  double t_submit;
+};
+
+struct Running {
+  int64_t id;
+  bhr_solver *s;
+  double t_submit, t_start;
+  int remaining;
+};
+
+struct Finished {
+  int state = 3;  // 3 done, 4 failed
+  int status = BHR_OK;
+  std::string error;
+  double t_submit = 0, t_start = 0, t_finish = 0;
+  int steps = 0;
+  std::vector<double> t, h, dedt;
+};
+
+double now_s() {
+  using clk = std::chrono::steady_clock;
+  static const clk::time_point t0 = clk::now();
+  return std::chrono::duration<double>(clk::now() - t0).count();
+}
+
+// Device bytes a solve will hold (states, coefficient planes, tables, rows,
+// source records), estimated before creating it.
+size_t solve_bytes(const bhr_params &p, int traj_rows) {
+  const size_t NM = static_cast<size_t>(p.N) * p.M;
+  size_t b = NM * 8 * (12 + 3);                                  // u0, u1, u2 (4 planes each), coefficient planes
+  b += static_cast<size_t>(CF_COUNT + 2) * p.N * 8 + static_cast<size_t>(RF_COUNT + 12) * p.M * 8;
+  b += static_cast<size_t>(2) * p.PTSX * p.PTSY * 8;
+  if (traj_rows > 0 && p.dt > 0) b += static_cast<size_t>(p.T / p.dt + 2) * sizeof(StepRec);
+  if (p.dt > 0 && p.Fr > 0) b += static_cast<size_t>(p.T / p.dt / p.Fr + 2) * 16 * 8;
+  return b + (1 << 20);
+}
+
+}  // namespace
+
+struct bhr_engine {
+  int device = 0;
+  size_t budget = 0, used = 0;
+  int rows = 16;
+  cudaStream_t stream = nullptr;
+  std::mutex qmu;  // the submission queue
+  std::deque<Request> queue;
+  int64_t next_id = 1;
+  std::mutex mu;   // everything else
+  std::vector<Running> active;
+  std::unordered_map<int64_t, Finished> done;
+  // device work tables
+  BatchSolve *d_solves = nullptr;
+  BatchTile *d_tiles = nullptr;
+  ExtractArgs *d_ext = nullptr;
+  SourceArgs *d_src = nullptr;
+  int cap_solves = 0, cap_tiles = 0, ntiles = 0, nsrc = 0, max_ptsx = 1, max_ptsy = 1;
+  cudaGraphExec_t graph = nullptr;
+  bool dirty = true;
+  // totals
+  long long batch_steps = 0;
+  double point_updates = 0.0;
+  int finished = 0;
+};
+
+namespace {
+
+int set_fail(int status, const std::string &msg) {
+  set_error(msg);
+  return status;
+}
+
+void release_tables(bhr_engine *e) {
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  e->graph = nullptr;
+  if (e->d_solves) cudaFree(e->d_solves);
+  if (e->d_tiles) cudaFree(e->d_tiles);
+  if (e->d_ext) cudaFree(e->d_ext);
+  if (e->d_src) cudaFree(e->d_src);
+  e->d_solves = nullptr;
+  e->d_tiles = nullptr;
+  e->d_ext = nullptr;
+  e->d_src = nullptr;
+  e->cap_solves = e->cap_tiles = 0;
+}
+
+// One batch step: sources of the sourced solves, three stages over the
+// work-list, extraction of every solve.
+int enqueue_batch_step(bhr_engine *e) {
+  const int n = static_cast<int>(e->active.size());
+  if (e->nsrc > 0) {
+    cudaError_t err = launch_source_batch(e->d_src, e->nsrc, e->max_ptsy, e->max_ptsx, e->stream);
+    if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("source batch: ") + cudaGetErrorString(err));
+  }
+  for (int stage = 1; stage <= 3; stage++) {
+    cudaError_t err = launch_stage_batch(stage, e->rows, e->d_solves, e->d_tiles, e->ntiles, e->stream);
+    if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("stage batch: ") + cudaGetErrorString(err));
+  }
+  cudaError_t err = launch_extract_batch(e->d_ext, n, e->stream);
+  if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("extract batch: ") + cudaGetErrorString(err));
+  return BHR_OK;
+}
+
+// Rebuilds the solve table, the work-list and the step graph after the set
+// of running solves changed.
+int rebuild(bhr_engine *e) {
+  const int n = static_cast<int>(e->active.size());
+  if (e->graph) {
+    cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+  }
+  e->dirty = false;
+  if (n == 0) {
+    e->ntiles = 0;
+    return BHR_OK;
+  }
+  std::vector<BatchSolve> solves(n);
+  std::vector<BatchTile> tiles;
+  std::vector<ExtractArgs> ext(n);
+  std::vector<SourceArgs> src;
+  e->max_ptsx = 1;
+  e->max_ptsy = 1;
+  for (int i = 0; i < n; i++) {
+    bhr_solver *s = e->active[i].s;
+    BatchSolve &B = solves[i];
+    double *vin[3] = {s->u0, s->u1, s->u2}, *out[3] = {s->u1, s->u2, s->u0};
+    for (int k = 0; k < 3; k++) {
+      B.maps[k] = s->maps[k];
+      B.args[k] = solver_stage_args(s);
+      B.args[k].vin = vin[k];
+      B.args[k].un = s->u0;
+      B.args[k].out = out[k];
+    }
+    for (int b0 = 0; b0 < s->p.M; b0 += e->rows)
+      for (int c0 = 0; c0 < s->p.N; c0 += TC) tiles.push_back({i, c0, b0, 0});
+    ext[i] = solver_extract_args(s);
+    if (s->has_source) {
+      src.push_back(solver_source_args(s));
+      e->max_ptsx = std::max(e->max_ptsx, s->p.PTSX);
+      e->max_ptsy = std::max(e->max_ptsy, s->p.PTSY);
+    }
+  }
+  // Blocks are ordered solve by solve, row block by row block.
+  e->ntiles = static_cast<int>(tiles.size());
+  e->nsrc = static_cast<int>(src.size());
+  auto grow = [&](auto **ptr, int need, int &cap) -> cudaError_t {
+    if (need <= cap) return cudaSuccess;
+    if (*ptr) cudaFree(*ptr);
+    *ptr = nullptr;
+    const int c = std::max(need, cap * 2);
+    cudaError_t err = cudaMalloc(reinterpret_cast<void **>(ptr), sizeof(**ptr) * static_cast<size_t>(c));
+    cap = err == cudaSuccess ? c : 0;
+    return err;
+  };
+  int cap_e = e->cap_solves, cap_s = e->cap_solves;
+  cudaError_t err = cudaSuccess;
+  if (n > e->cap_solves) {
+    if (e->d_ext) cudaFree(e->d_ext);
+    if (e->d_src) cudaFree(e->d_src);
+    e->d_ext = nullptr;
+    e->d_src = nullptr;
+    cap_e = cap_s = 0;
+    if ((err = grow(&e->d_ext, n, cap_e)) || (err = grow(&e->d_src, n, cap_s)) ||
+        (err = grow(&e->d_solves, n, e->cap_solves)))
+      return set_fail(BHR_OUT_OF_MEMORY, std::string("engine tables: ") + cudaGetErrorString(err));
+  }
+  if ((err = grow(&e->d_tiles, e->ntiles, e->cap_tiles)))
+    return set_fail(BHR_OUT_OF_MEMORY, std::string("engine work-list: ") + cudaGetErrorString(err));
+  if ((err = cudaMemcpyAsync(e->d_solves, solves.data(), sizeof(BatchSolve) * n, cudaMemcpyHostToDevice, e->stream)) ||
+      (err = cudaMemcpyAsync(e->d_tiles, tiles.data(), sizeof(BatchTile) * tiles.size(), cudaMemcpyHostToDevice,
+                             e->stream)) ||
+      (err = cudaMemcpyAsync(e->d_ext, ext.data(), sizeof(ExtractArgs) * n, cudaMemcpyHostToDevice, e->stream)) ||
+      (e->nsrc > 0 && (err = cudaMemcpyAsync(e->d_src, src.data(), sizeof(SourceArgs) * e->nsrc,
+                                             cudaMemcpyHostToDevice, e->stream))) ||
+      (err = cudaStreamSynchronize(e->stream)))
+    return set_fail(BHR_CUDA_ERROR, std::string("engine upload: ") + cudaGetErrorString(err));
+  // Capture one batch step.
+  cudaGraph_t g = nullptr;
+  if ((err = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal)))
+    return set_fail(BHR_CUDA_ERROR, std::string("capture: ") + cudaGetErrorString(err));
+  const int st = enqueue_batch_step(e);
+  err = cudaStreamEndCapture(e->stream, &g);
+  if (st != BHR_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("capture: ") + cudaGetErrorString(err));
+  err = cudaGraphInstantiate(&e->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("instantiate: ") + cudaGetErrorString(err));
+  return BHR_OK;
+}
+
+void fail_request(bhr_engine *e, const Request &r, int status, const std::string &msg) {
+  Finished f;
+  f.state = 4;
+  f.status = status;
+  f.error = msg;
+  f.t_submit = r.t_submit;
+  f.t_start = f.t_finish = now_s();
+  e->done[r.id] = std::move(f);
+}
+
+// Admits queued requests in arrival order while they fit the budget.
+int admit(bhr_engine *e) {
+  for (;;) {
+    Request r;
+    {
+      std::lock_guard<std::mutex> lock(e->qmu);
+      if (e->queue.empty()) return BHR_OK;
+      const size_t need = solve_bytes(e->queue.front().p, static_cast<int>(e->queue.front().traj.size() / 10));
+      if (e->used + need > e->budget && !e->active.empty()) return BHR_OK;  // wait for memory
+      r = std::move(e->queue.front());
+      e->queue.pop_front();
+    }
+    r.p.device = e->device;
+    bhr_solver *s = nullptr;
+    int st = solver_create(&r.p, e->rows, &s);
+    if (st == BHR_OK && !r.traj.empty())
+      st = bhr_solver_set_trajectory(s, r.traj.data(), static_cast<int>(r.traj.size() / 10));
+    if (st != BHR_OK) {
+      const std::string msg = bhr_last_error_string();
+      if (s) bhr_solver_destroy(s);
+      fail_request(e, r, st, msg);
+      continue;
+    }
+    e->used += s->bytes;
+    e->active.push_back({r.id, s, r.t_submit, now_s(), s->nt - s->steps_done});
+    e->dirty = true;
+  }
+}
+
+// Retires solves whose last step has run.
+int retire(bhr_engine *e) {
+  for (size_t i = 0; i < e->active.size();) {
+    Running &R = e->active[i];
+    if (R.remaining > 0) {
+      i++;
+      continue;
+    }
+    Finished f;
+    f.t_submit = R.t_submit;
+    f.t_start = R.t_start;
+    f.steps = R.s->nt;
+    bhr_info inf{};
+    bhr_solver_info(R.s, &inf);
+    f.t.resize(inf.rows_done);
+    f.h.resize(static_cast<size_t>(inf.rows_done) * 14);
+    f.dedt.resize(inf.rows_done);
+    int nrows = 0;
+    f.status = bhr_solver_waveform(R.s, f.t.data(), f.h.data(), f.dedt.data(), inf.rows_done, &nrows);
+    if (f.status == BHR_OK) {
+      RunState rs{};
+      cudaMemcpy(&rs, R.s->rs, sizeof(rs), cudaMemcpyDeviceToHost);
+      if (rs.err) f.status = rs.err;
+    }
+    f.state = f.status == BHR_OK ? 3 : 4;
+    if (f.status != BHR_OK) f.error = bhr_last_error_string();
+    f.t_finish = now_s();
+    e->used -= std::min(e->used, R.s->bytes);
+    bhr_solver_destroy(R.s);
+    e->done[R.id] = std::move(f);
+    e->finished++;
+    e->active.erase(e->active.begin() + static_cast<long>(i));
+    e->dirty = true;
+  }
+  return BHR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bhr_engine_create(int device, size_t hbm_budget_bytes, bhr_engine **out) {
+  if (!out) return set_fail(BHR_INVALID_ARG, "null argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+    cudaGetLastError();
+    return set_fail(BHR_NO_DEVICE, "no CUDA device");
+  }
+  if (device < 0 || device >= ndev) return set_fail(BHR_INVALID_ARG, "device ordinal out of range");
+  auto *e = new bhr_engine();
+  e->device = device;
+  e->budget = hbm_budget_bytes;
+  if (cudaSetDevice(device) != cudaSuccess || prepare_kernels() != cudaSuccess ||
+      cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete e;
+    return set_fail(BHR_CUDA_ERROR, "engine set-up failed");
+  }
+  *out = e;
+  return BHR_OK;
+}
+
+void bhr_engine_destroy(bhr_engine *e) {
+  if (!e) return;
+  std::lock_guard<std::mutex> lock(e->mu);
+  cudaSetDevice(e->device);
+  cudaStreamSynchronize(e->stream);
+  for (auto &R : e->active) bhr_solver_destroy(R.s);
+  e->active.clear();
+  release_tables(e);
+  cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+int bhr_engine_submit(bhr_engine *e, const bhr_params *p, const double *traj_rows, int nrows, int64_t *id) {
+  if (!e || !p || !id || (traj_rows && nrows < 2)) return set_fail(BHR_INVALID_ARG, "bad submit arguments");
+  Request r;
+  r.p = *p;
+  if (traj_rows) r.traj.assign(traj_rows, traj_rows + static_cast<size_t>(nrows) * 10);
+  r.t_submit = now_s();
+  std::lock_guard<std::mutex> lock(e->qmu);
+  r.id = e->next_id++;
+  *id = r.id;
+  e->queue.push_back(std::move(r));
+  return BHR_OK;
+}
+
+int bhr_engine_step(bhr_engine *e, int max_steps, int *running) {
+  if (!e || max_steps < 0) return set_fail(BHR_INVALID_ARG, "bad step arguments");
+  std::lock_guard<std::mutex> lock(e->mu);
+  if (cudaSetDevice(e->device) != cudaSuccess) return set_fail(BHR_CUDA_ERROR, "cudaSetDevice failed");
+  if (int st = admit(e)) return st;
+  if (e->dirty)
+    if (int st = rebuild(e)) return st;
+  int n = max_steps;
+  for (auto &R : e->active) n = std::min(n, R.remaining);
+  if (!e->active.empty() && n > 0) {
+    for (int i = 0; i < n; i++) {
+      cudaError_t err = cudaGraphLaunch(e->graph, e->stream);
+      if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("graph launch: ") + cudaGetErrorString(err));
+    }
+    cudaError_t err = cudaStreamSynchronize(e->stream);
+    if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("engine step: ") + cudaGetErrorString(err));
+    double pts = 0.0;
+    for (auto &R : e->active) {
+      R.remaining -= n;
+      R.s->steps_done += n;
+      pts += static_cast<double>(R.s->p.N) * R.s->p.M;
+    }
+    e->batch_steps += n;
+    e->point_updates += pts * n;
+  }
+  if (int st = retire(e)) return st;
+  if (running) *running = static_cast<int>(e->active.size());
+  return BHR_OK;
+}
+
+int bhr_engine_poll(bhr_engine *e, int64_t id, bhr_request_info *info) {
+  if (!e || !info) return set_fail(BHR_INVALID_ARG, "bad poll arguments");
+  std::memset(info, 0, sizeof(*info));
+  {
+    std::lock_guard<std::mutex> lock(e->qmu);
+    for (auto &r : e->queue)
+      if (r.id == id) {
+        info->state = 1;
+        info->submit_s = r.t_submit;
+        return BHR_OK;
+      }
+  }
+  std::lock_guard<std::mutex> lock(e->mu);
+  for (auto &R : e->active)
+    if (R.id == id) {
+      info->state = 2;
+      info->steps_total = R.s->nt;
+      info->steps_done = R.s->steps_done;
+      info->submit_s = R.t_submit;
+      info->start_s = R.t_start;
+      return BHR_OK;
+    }
+  auto it = e->done.find(id);
+  if (it == e->done.end()) return BHR_OK;  // unknown: state 0
+  const Finished &f = it->second;
+  info->state = f.state;
+  info->status = f.status;
+  info->nrows = static_cast<int>(f.t.size());
+  info->steps_total = info->steps_done = f.steps;
+  info->submit_s = f.t_submit;
+  info->start_s = f.t_start;
+  info->finish_s = f.t_finish;
+  return BHR_OK;
+}
+
+int bhr_engine_result(bhr_engine *e, int64_t id, double *t, double *h, double *dedt, int max_rows, int *nrows) {
+  if (!e) return set_fail(BHR_INVALID_ARG, "null engine");
+  std::lock_guard<std::mutex> lock(e->mu);
+  auto it = e->done.find(id);
+  if (it == e->done.end()) return set_fail(BHR_INVALID_ARG, "request not finished");
+  const Finished &f = it->second;
+  if (f.state != 3) return set_fail(f.status ? f.status : BHR_INVALID_ARG, "request failed: " + f.error);
+  const int n = std::min(static_cast<int>(f.t.size()), std::max(0, max_rows));
+  if (t) std::memcpy(t, f.t.data(), sizeof(double) * n);
+  if (h) std::memcpy(h, f.h.data(), sizeof(double) * 14 * n);
+  if (dedt) std::memcpy(dedt, f.dedt.data(), sizeof(double) * n);
+  if (nrows) *nrows = n;
+  return BHR_OK;
+}
+
+int bhr_engine_stats(bhr_engine *e, bhr_engine_counters *st) {
+  if (!e || !st) return set_fail(BHR_INVALID_ARG, "bad stats arguments");
+  std::memset(st, 0, sizeof(*st));
+  {
+    std::lock_guard<std::mutex> lock(e->qmu);
+    st->queued = static_cast<int>(e->queue.size());
+  }
+  std::lock_guard<std::mutex> lock(e->mu);
+  st->running = static_cast<int>(e->active.size());
+  st->finished = e->finished;
+  st->batch_steps = e->batch_steps;
+  st->point_updates = e->point_updates;
+  st->bytes_in_use = e->used;
+  st->budget = e->budget;
+  st->tiles = e->ntiles;
+  return BHR_OK;
+}
+
+}  // extern "C"

@@ -102,6 +102,16 @@ struct StageMaps {
   CUtensorMap q, p, u, coef_bb, coef_ie, colf;
 };
 
+// A batch of solves advanced together: per solve, the tensor maps and
+// arguments of its three stages; per block, one (solve, tile) work item.
+struct BatchSolve {
+  StageMaps maps[3];
+  StageArgs args[3];
+};
+struct BatchTile {
+  int solve, c0, b0, pad;
+};
+
 // Tensor maps of one state (four M x N planes): q planes with the +-3 row
 // and +-4 column halo, p planes with the column halo, and (tm_u, may be
 // null) the bare tile of all four planes for reading u^n.
@@ -114,6 +124,10 @@ cudaError_t launch_coef_tables(const double *coltab, const double *rowtab, doubl
                                cudaStream_t st);
 cudaError_t encode_coef_maps(double *ctab, const double *coltab, int N, int M, int rows, StageMaps *maps);
 cudaError_t launch_source(const SourceArgs &a, cudaStream_t st);
+cudaError_t launch_stage_batch(int stage, int rows, const BatchSolve *solves, const BatchTile *tiles, int ntiles,
+                               cudaStream_t st);
+cudaError_t launch_source_batch(const SourceArgs *args, int nsolves, int max_ptsy, int max_ptsx, cudaStream_t st);
+cudaError_t launch_extract_batch(const ExtractArgs *args, int nsolves, cudaStream_t st);
 cudaError_t launch_extract(const ExtractArgs &a, cudaStream_t st);
 cudaError_t launch_closure(double *planes, int N, int M, int even_m, cudaStream_t st);
 size_t stage_smem_bytes();

@@ -157,16 +157,15 @@ __global__ void coef_table_kernel(const double *coltab, const double *rowtab, do
   ctab[2 * NM + id] = ee;
 }
 
+// One tile (columns c0..c0+63, rows b0..b0+ROWS-1) of one SSP-RK3 stage.
 template <int STAGE, int ROWS>
-__global__ void __launch_bounds__(STAGE_THREADS, 2)
-    stage_kernel(const __grid_constant__ StageMaps T, const StageArgs A) {
+__device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &A, const int c0, const int b0) {
   constexpr int TR = ROWS;           // tile rows
   constexpr int RPT = ROWS / 8;      // rows per thread
   extern __shared__ unsigned char smem_raw[];
   StageSmem<ROWS> &S = *reinterpret_cast<StageSmem<ROWS> *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
-  const int c0 = blockIdx.x * TC, b0 = blockIdx.y * TR;
   const int N = A.N, M = A.M;
   const size_t NM = static_cast<size_t>(N) * M;
 
@@ -428,6 +427,24 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
 
 }
 
+// One solve: the grid is the solve's tiles.
+template <int STAGE, int ROWS>
+__global__ void __launch_bounds__(STAGE_THREADS, 2)
+    stage_kernel(const __grid_constant__ StageMaps T, const StageArgs A) {
+  stage_tile<STAGE, ROWS>(T, A, blockIdx.x * TC, blockIdx.y * ROWS);
+}
+
+// Many solves advanced together: block i takes entry i of the work-list of
+// (solve, tile) pairs; tensor maps and arguments come from the solve table
+// in device memory.
+template <int STAGE, int ROWS>
+__global__ void __launch_bounds__(STAGE_THREADS, 2)
+    stage_batch_kernel(const BatchSolve *solves, const BatchTile *tiles) {
+  const BatchTile t = tiles[blockIdx.x];
+  const BatchSolve &B = solves[t.solve];
+  stage_tile<STAGE, ROWS>(B.maps[STAGE - 1], B.args[STAGE - 1], t.c0, t.b0);
+}
+
 // ---- closure of stored planes (HighOrder/kern.cu:622-753) ------------------
 __device__ __forceinline__ double pole_val(const double *P, int N, int M, int even, int b, int a) {
   if (b >= 3 && b < M - 3) return P[static_cast<size_t>(b) * N + a];
@@ -497,10 +514,7 @@ __global__ void closure_ends_kernel(double *P, int N, int M) {
 }
 
 // ---- particle source patch (HighOrder/kern.cu:1185-1227, 2666-2683) ---------
-__global__ void source_patch_kernel(const SourceArgs A) {
-  grid_dependency_wait();
-  launch_dependents();
-  const int j = blockIdx.x, k = threadIdx.x;
+__device__ __forceinline__ void source_patch(const SourceArgs &A, const int j, const int k) {
   if (k >= A.PTSX) return;
   const StepRec &rec = A.recs[A.rs->k];
   const int row = j + rec.row0, col = k + rec.col0;
@@ -545,15 +559,27 @@ __global__ void source_patch_kernel(const SourceArgs A) {
   A.src[static_cast<size_t>(A.PTSY + j) * A.PTSX + k] = sim;
 }
 
+__global__ void source_patch_kernel(const SourceArgs A) {
+  grid_dependency_wait();
+  launch_dependents();
+  source_patch(A, blockIdx.x, threadIdx.x);
+}
+
+// Sourced solves of a batch: blockIdx.y picks the solve.
+__global__ void source_batch_kernel(const SourceArgs *args) {
+  grid_dependency_wait();
+  launch_dependents();
+  const SourceArgs &A = args[blockIdx.y];
+  if (static_cast<int>(blockIdx.x) < A.PTSY) source_patch(A, blockIdx.x, threadIdx.x);
+}
+
 // ---- extraction, integration, projection (HighOrder/body.cu:168-212) ------
 constexpr int kExtractThreads = 256;
 constexpr int kSums = 15;
 
-__global__ void __launch_bounds__(kExtractThreads) extract_kernel(const ExtractArgs A) {
+__device__ __forceinline__ void extract_body(const ExtractArgs &A) {
   __shared__ double red[kExtractThreads / 32][kSums];
   __shared__ int nan_flag;
-  grid_dependency_wait();
-  launch_dependents();
   const int tid = threadIdx.x;
   const int N = A.N, M = A.M;
   const size_t NM = static_cast<size_t>(N) * M;
@@ -613,6 +639,19 @@ __global__ void __launch_bounds__(kExtractThreads) extract_kernel(const ExtractA
     A.rs->timer += A.dt;
     A.rs->k = k + 1;
   }
+}
+
+__global__ void __launch_bounds__(kExtractThreads) extract_kernel(const ExtractArgs A) {
+  grid_dependency_wait();
+  launch_dependents();
+  extract_body(A);
+}
+
+// One block per solve of a batch.
+__global__ void __launch_bounds__(kExtractThreads) extract_batch_kernel(const ExtractArgs *args) {
+  grid_dependency_wait();
+  launch_dependents();
+  extract_body(args[blockIdx.x]);
 }
 
 }  // namespace
@@ -729,9 +768,41 @@ cudaError_t prepare_kernels() {
       (e = cudaFuncSetAttribute(stage_kernel<3, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
       (e = cudaFuncSetAttribute(stage_kernel<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)) ||
       (e = cudaFuncSetAttribute(stage_kernel<2, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)) ||
-      (e = cudaFuncSetAttribute(stage_kernel<3, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)))
+      (e = cudaFuncSetAttribute(stage_kernel<3, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)) ||
+      (e = cudaFuncSetAttribute(stage_batch_kernel<1, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
+      (e = cudaFuncSetAttribute(stage_batch_kernel<2, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
+      (e = cudaFuncSetAttribute(stage_batch_kernel<3, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
+      (e = cudaFuncSetAttribute(stage_batch_kernel<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)) ||
+      (e = cudaFuncSetAttribute(stage_batch_kernel<2, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)) ||
+      (e = cudaFuncSetAttribute(stage_batch_kernel<3, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)))
     return e;
   return cudaSuccess;
+}
+
+cudaError_t launch_stage_batch(int stage, int rows, const BatchSolve *solves, const BatchTile *tiles, int ntiles,
+                               cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  const dim3 grid(ntiles), block(32, STAGE_THREADS / 32);
+  if (rows == 8) {
+    const size_t smem = sizeof(StageSmem<8>) + 128;
+    if (stage == 1) return launch_pdl(stage_batch_kernel<1, 8>, grid, block, smem, st, solves, tiles);
+    if (stage == 2) return launch_pdl(stage_batch_kernel<2, 8>, grid, block, smem, st, solves, tiles);
+    return launch_pdl(stage_batch_kernel<3, 8>, grid, block, smem, st, solves, tiles);
+  }
+  const size_t smem = sizeof(StageSmem<16>) + 128;
+  if (stage == 1) return launch_pdl(stage_batch_kernel<1, 16>, grid, block, smem, st, solves, tiles);
+  if (stage == 2) return launch_pdl(stage_batch_kernel<2, 16>, grid, block, smem, st, solves, tiles);
+  return launch_pdl(stage_batch_kernel<3, 16>, grid, block, smem, st, solves, tiles);
+}
+
+cudaError_t launch_source_batch(const SourceArgs *args, int nsolves, int max_ptsy, int max_ptsx, cudaStream_t st) {
+  if (nsolves <= 0) return cudaSuccess;
+  return launch_pdl(source_batch_kernel, dim3(max_ptsy, nsolves), dim3(max_ptsx), 0, st, args);
+}
+
+cudaError_t launch_extract_batch(const ExtractArgs *args, int nsolves, cudaStream_t st) {
+  if (nsolves <= 0) return cudaSuccess;
+  return launch_pdl(extract_batch_kernel, dim3(nsolves), dim3(kExtractThreads), 0, st, args);
 }
 
 cudaError_t launch_source(const SourceArgs &a, cudaStream_t st) {

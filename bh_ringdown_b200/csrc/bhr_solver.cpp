@@ -11,6 +11,8 @@
 #include <cstring>
 #include <fstream>
 #include <array>
+#include <atomic>
+#include <thread>
 #include <mutex>
 #include <sstream>
 #include <string>
@@ -19,6 +21,7 @@
 #include "bhr.h"
 #include "bhr_host.h"
 #include "bhr_internal.h"
+#include "bhr_solver_impl.h"
 
 namespace bhr {
 
@@ -37,27 +40,6 @@ void set_error(const std::string &msg) { g_err = msg; }
 }  // namespace bhr
 
 using namespace bhr;
-
-struct bhr_solver {
-  bhr_params p{};
-  Grid g;
-  int nt = 0, Fr = 1, max_rows = 0, ext_col = 0;
-  bool even_m = true;
-  bool has_source = false;
-  cudaStream_t stream = nullptr;
-  // device memory
-  double *u0 = nullptr, *u1 = nullptr, *u2 = nullptr;
-  double *coltab = nullptr, *rowtab = nullptr, *ctab = nullptr, *rc = nullptr, *th = nullptr;
-  double *src = nullptr, *ext = nullptr, *integ = nullptr, *wproj = nullptr, *wdedt = nullptr, *rows = nullptr;
-  StepRec *recs = nullptr;
-  RunState *rs = nullptr;
-  size_t bytes = 0;
-  StageMaps maps[3];  // per stage input state (u^n, u1, u2)
-  int tile_rows = 16; // stage tile height chosen for this grid
-  int steps_done = 0;
-  // Captured step graphs: one step, and kGraphBatch steps in one launch.
-  cudaGraphExec_t g1 = nullptr, gb = nullptr;
-};
 
 static constexpr int kGraphBatch = 16;
 
@@ -123,9 +105,9 @@ double tortoise(double r, double a, double rpl, double rmn) {
 
 }  // namespace
 
-extern "C" {
-
 static int autotune_rows(bhr_solver *s);
+
+extern "C" {
 
 int bhr_abi_version(void) { return BHR_ABI_VERSION; }
 const char *bhr_last_error_string(void) { return g_err.c_str(); }
@@ -172,7 +154,13 @@ int bhr_grid(const bhr_params *p, double *x_c, double *r_c, double *theta) {
   return BHR_OK;
 }
 
-int bhr_solver_create(const bhr_params *pin, bhr_solver **out) {
+int bhr_solver_create(const bhr_params *pin, bhr_solver **out) { return bhr::solver_create(pin, 0, out); }
+
+}  // extern "C"
+
+static int encode_maps(bhr_solver *s, int rows);
+
+int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
   if (!pin || !out) {
     set_error("null argument");
     return BHR_INVALID_ARG;
@@ -253,7 +241,7 @@ int bhr_solver_create(const bhr_params *pin, bhr_solver **out) {
     delete s;
     return BHR_CUDA_ERROR;
   }
-  if (int st = autotune_rows(s)) {
+  if (int st = (tile_rows == 8 || tile_rows == 16) ? encode_maps(s, tile_rows) : autotune_rows(s)) {
     free_all(s);
     delete s;
     return st;
@@ -261,6 +249,8 @@ int bhr_solver_create(const bhr_params *pin, bhr_solver **out) {
   *out = s;
   return BHR_OK;
 }
+
+extern "C" {
 
 void bhr_solver_destroy(bhr_solver *s) {
   if (!s) return;
@@ -320,13 +310,17 @@ int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows) {
   } while (row[0] < timer && cursor < nrows);
   double rp = row[1];
   double tmp11 = 0.0, tmp22 = 0.0, tmp33 = 0.0;
+  // Sequential pass: particle state and turn-on factor of every step.
+  std::vector<bhr_particle> pts(s->nt);
+  std::vector<double> turn(s->nt);
   for (int k = 0; k < s->nt; k++) {
     const int c0 = cursor;
     rd();
     rd();
     if (cursor != c0) rp = row[1];
     rp = rp + 1e-6;
-    bhr_particle pt{};
+    bhr_particle &pt = pts[k];
+    pt = bhr_particle{};
     pt.rp = rp;
     pt.tp = row[2];
     pt.phip = row[6];
@@ -342,26 +336,54 @@ int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows) {
     tmp11 = row[3];
     tmp22 = row[4];
     tmp33 = row[5];
-    double cr[6], ci[6];
-    if (int st = bhr_source_coefficients(&pt, a, mass, p.m, cr, ci)) return st;
-    const double turn = std::pow(1.0 - std::exp(-(timer - start) / 25.0), 4);
-    StepRec &R = recs[k];
-    for (int i = 0; i < 6; i++) {
-      R.c_re[i] = cr[i] * turn;
-      R.c_im[i] = ci[i] * turn;
-    }
-    R.rp = rp;
-    R.tp = pt.tp;
-    R.wr = p.wr_fac * s->g.dx * (1.0 - rpl / rp);
-    const double xp = tortoise(rp, a, rpl, rmn);
-    const double ipd = (xp - p.Xmin) / s->g.dx, itd = pt.tp / s->g.dtheta;
-    if (!std::isfinite(ipd) || !std::isfinite(itd) || std::fabs(ipd) > 1e9 || std::fabs(itd) > 1e9) {
-      set_error("trajectory point outside the grid (non-finite tortoise coordinate)");
-      return BHR_INVALID_ARG;
-    }
-    R.col0 = static_cast<int>(ipd) - p.PTSX / 2;
-    R.row0 = static_cast<int>(itd) - p.PTSY / 2;
+    turn[k] = std::pow(1.0 - std::exp(-(timer - start) / 25.0), 4);
     timer += p.dt;
+  }
+  // Independent per step: source coefficients, width and patch origin,
+  // evaluated on all host threads.
+  std::atomic<int> first_bad{-1};
+  std::atomic<int> bad_status{BHR_OK};
+  auto work = [&](int k0, int k1) {
+    for (int k = k0; k < k1; k++) {
+      const bhr_particle &pt = pts[k];
+      StepRec &R = recs[k];
+      double cr[6], ci[6];
+      const int st = bhr_source_coefficients(&pt, a, mass, p.m, cr, ci);
+      const double xp = tortoise(pt.rp, a, rpl, rmn);
+      const double ipd = (xp - p.Xmin) / s->g.dx, itd = pt.tp / s->g.dtheta;
+      if (st != BHR_OK || !std::isfinite(ipd) || !std::isfinite(itd) || std::fabs(ipd) > 1e9 ||
+          std::fabs(itd) > 1e9) {
+        int expect = -1;
+        if (first_bad.compare_exchange_strong(expect, k)) bad_status = st != BHR_OK ? st : BHR_INVALID_ARG;
+        return;
+      }
+      for (int i = 0; i < 6; i++) {
+        R.c_re[i] = cr[i] * turn[k];
+        R.c_im[i] = ci[i] * turn[k];
+      }
+      R.rp = pt.rp;
+      R.tp = pt.tp;
+      R.wr = p.wr_fac * s->g.dx * (1.0 - rpl / pt.rp);
+      R.col0 = static_cast<int>(ipd) - p.PTSX / 2;
+      R.row0 = static_cast<int>(itd) - p.PTSY / 2;
+    }
+  };
+  const int nth = std::max(1, std::min(64, static_cast<int>(std::thread::hardware_concurrency())));
+  if (s->nt < 4096 || nth == 1) {
+    work(0, s->nt);
+  } else {
+    std::vector<std::thread> pool;
+    const int chunk = (s->nt + nth - 1) / nth;
+    for (int t = 0; t < nth; t++) {
+      const int k0 = t * chunk, k1 = std::min(s->nt, k0 + chunk);
+      if (k0 < k1) pool.emplace_back(work, k0, k1);
+    }
+    for (auto &th : pool) th.join();
+  }
+  if (first_bad.load() >= 0) {
+    set_error("trajectory step " + std::to_string(first_bad.load()) +
+              ": particle off the grid, inside the horizon or on a pole");
+    return bad_status.load();
   }
   cudaSetDevice(p.device);
   if (s->recs) cudaFree(s->recs), s->bytes -= sizeof(StepRec) * static_cast<size_t>(s->nt ? s->nt : 1);
@@ -397,6 +419,8 @@ int bhr_solver_load_trajectory(bhr_solver *s, const char *path) {
   return bhr_solver_set_trajectory(s, rows.data(), static_cast<int>(rows.size() / 10));
 }
 
+}  // extern "C"
+
 static int encode_maps(bhr_solver *s, int rows) {
   const bhr_params &p = s->p;
   double *bufs[3] = {s->u0, s->u1, s->u2};
@@ -414,7 +438,6 @@ static int encode_maps(bhr_solver *s, int rows) {
   return BHR_OK;
 }
 
-static StageArgs stage_args(bhr_solver *s);
 
 // Tile-height autotuner: per (device, N, M) the stage kernels are timed with
 // 8- and 16-row tiles on stages 1 and 2, which write only the solve's
@@ -436,7 +459,7 @@ static int autotune_rows(bhr_solver *s) {
   BHR_CUDA_TRY(cudaEventCreate(&e1));
   for (int rows : cands) {
     if (int st = encode_maps(s, rows)) return st;
-    StageArgs A = stage_args(s);
+    StageArgs A = solver_stage_args(s);
     A.src = nullptr;
     for (int rep = 0; rep < 6; rep++) {
       if (rep == 2) BHR_CUDA_TRY(cudaEventRecord(e0, s->stream));
@@ -463,7 +486,7 @@ static int autotune_rows(bhr_solver *s) {
   return encode_maps(s, best);
 }
 
-static StageArgs stage_args(bhr_solver *s) {
+StageArgs bhr::solver_stage_args(bhr_solver *s) {
   const bhr_params &p = s->p;
   const double odx = 1.0 / s->g.dx, odth = 1.0 / s->g.dtheta, odt = 1.0 / p.dt;
   const double third = 0.33333333333333333;
@@ -488,38 +511,27 @@ static StageArgs stage_args(bhr_solver *s) {
   return A;
 }
 
-static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
-  auto mark = [&](int i) { return ev ? cudaEventRecord(ev[i], s->stream) : cudaSuccess; };
+SourceArgs bhr::solver_source_args(bhr_solver *s) {
   const bhr_params &p = s->p;
-  StageArgs A = stage_args(s);
-  BHR_CUDA_TRY(mark(0));
-  if (s->has_source) {
-    SourceArgs S{};
-    S.src = s->src;
-    S.recs = s->recs;
-    S.rs = s->rs;
-    S.r_c = s->rc;
-    S.theta = s->th;
-    S.N = p.N;
-    S.M = p.M;
-    S.PTSX = p.PTSX;
-    S.PTSY = p.PTSY;
-    S.a = p.a;
-    S.mass = p.mass;
-    S.m = p.m;
-    S.wt = p.wt_fac * s->g.dtheta;
-    BHR_CUDA_TRY(launch_source(S, s->stream));
-  }
-  BHR_CUDA_TRY(mark(1));
-  A.vin = s->u0; A.un = s->u0; A.out = s->u1;
-  BHR_CUDA_TRY(launch_stage(1, s->maps[0], A, s->stream));
-  BHR_CUDA_TRY(mark(2));
-  A.vin = s->u1; A.un = s->u0; A.out = s->u2;
-  BHR_CUDA_TRY(launch_stage(2, s->maps[1], A, s->stream));
-  BHR_CUDA_TRY(mark(3));
-  A.vin = s->u2; A.un = s->u0; A.out = s->u0;
-  BHR_CUDA_TRY(launch_stage(3, s->maps[2], A, s->stream));
-  BHR_CUDA_TRY(mark(4));
+  SourceArgs S{};
+  S.src = s->src;
+  S.recs = s->recs;
+  S.rs = s->rs;
+  S.r_c = s->rc;
+  S.theta = s->th;
+  S.N = p.N;
+  S.M = p.M;
+  S.PTSX = p.PTSX;
+  S.PTSY = p.PTSY;
+  S.a = p.a;
+  S.mass = p.mass;
+  S.m = p.m;
+  S.wt = p.wt_fac * s->g.dtheta;
+  return S;
+}
+
+ExtractArgs bhr::solver_extract_args(bhr_solver *s) {
+  const bhr_params &p = s->p;
   ExtractArgs E{};
   E.u = s->u0;
   E.ext = s->ext;
@@ -537,7 +549,25 @@ static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
   E.dt = p.dt;
   E.out_start = p.out_start;
   E.Xmax = p.Xmax;
-  BHR_CUDA_TRY(launch_extract(E, s->stream));
+  return E;
+}
+
+static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
+  auto mark = [&](int i) { return ev ? cudaEventRecord(ev[i], s->stream) : cudaSuccess; };
+  StageArgs A = solver_stage_args(s);
+  BHR_CUDA_TRY(mark(0));
+  if (s->has_source) BHR_CUDA_TRY(launch_source(solver_source_args(s), s->stream));
+  BHR_CUDA_TRY(mark(1));
+  A.vin = s->u0; A.un = s->u0; A.out = s->u1;
+  BHR_CUDA_TRY(launch_stage(1, s->maps[0], A, s->stream));
+  BHR_CUDA_TRY(mark(2));
+  A.vin = s->u1; A.un = s->u0; A.out = s->u2;
+  BHR_CUDA_TRY(launch_stage(2, s->maps[1], A, s->stream));
+  BHR_CUDA_TRY(mark(3));
+  A.vin = s->u2; A.un = s->u0; A.out = s->u0;
+  BHR_CUDA_TRY(launch_stage(3, s->maps[2], A, s->stream));
+  BHR_CUDA_TRY(mark(4));
+  BHR_CUDA_TRY(launch_extract(solver_extract_args(s), s->stream));
   BHR_CUDA_TRY(mark(5));
   return BHR_OK;
 }
@@ -598,6 +628,8 @@ static int enqueue_steps(bhr_solver *s, int nsteps) {
   s->steps_done += nsteps;
   return BHR_OK;
 }
+
+extern "C" {
 
 int bhr_solver_step(bhr_solver *s, int nsteps) {
   if (!s || nsteps < 0) return BHR_INVALID_ARG;

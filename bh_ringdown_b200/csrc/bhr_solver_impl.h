@@ -1,0 +1,38 @@
+// bhr_solver_impl.h -- the solve object shared by the C ABI (bhr_solver.cpp)
+// and the batch engine (bhr_engine.cpp).  Not part of the public ABI.
+#pragma once
+
+#include "bhr.h"
+#include "bhr_host.h"
+#include "bhr_internal.h"
+
+struct bhr_solver {
+  bhr_params p{};
+  bhr::Grid g;
+  int nt = 0, Fr = 1, max_rows = 0, ext_col = 0;
+  bool even_m = true;
+  bool has_source = false;
+  cudaStream_t stream = nullptr;
+  // device memory
+  double *u0 = nullptr, *u1 = nullptr, *u2 = nullptr;
+  double *coltab = nullptr, *rowtab = nullptr, *ctab = nullptr, *rc = nullptr, *th = nullptr;
+  double *src = nullptr, *ext = nullptr, *integ = nullptr, *wproj = nullptr, *wdedt = nullptr, *rows = nullptr;
+  bhr::StepRec *recs = nullptr;
+  bhr::RunState *rs = nullptr;
+  size_t bytes = 0;
+  bhr::StageMaps maps[3];  // per stage input state (u^n, u1, u2)
+  int tile_rows = 16; // stage tile height chosen for this grid
+  int steps_done = 0;
+  // Captured step graphs: one step, and kGraphBatch steps in one launch.
+  cudaGraphExec_t g1 = nullptr, gb = nullptr;
+};
+
+
+namespace bhr {
+// Creates a solve; tile_rows 0 lets the autotuner pick 8 or 16.
+int solver_create(const bhr_params *p, int tile_rows, bhr_solver **out);
+// Launch arguments of the solve's kernels (stage pointers vin/un/out unset).
+StageArgs solver_stage_args(bhr_solver *s);
+SourceArgs solver_source_args(bhr_solver *s);
+ExtractArgs solver_extract_args(bhr_solver *s);
+}  // namespace bhr

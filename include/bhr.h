@@ -195,6 +195,48 @@ double bhr_swsh(double ell, double m, double theta);
  * overlap on the GPU (other streams, other host threads' streams) race. */
 int bhr_step_noalloc(const bhr_params *p, double *state, int nsteps, void *stream);
 
+/* ---- Batch engine: many solves per device, advanced together ----------
+ * No counterpart in the reference, which runs one body() per process and
+ * one process per (trajectory, m) job (HighOrder/main.c:65-70).  The
+ * engine queues requests, admits them in arrival order while their device
+ * memory fits `hbm_budget_bytes` (one is always admitted when none runs),
+ * and advances every running solve with one launch per RK stage over a
+ * (solve, tile) work-list.  Requests submitted while others run join at the
+ * next bhr_engine_step (continuous batching).  A request's waveform does
+ * not depend on the other requests in the batch: it is bit-identical to the
+ * same request run alone in an engine, and matches bhr_solver_step's to
+ * FP64 rounding. */
+typedef struct bhr_engine bhr_engine;
+
+typedef struct bhr_request_info {
+  int state;          /* 0 unknown, 1 queued, 2 running, 3 done, 4 failed */
+  int status;         /* bhr_status of a failed request */
+  int steps_total, steps_done, nrows;
+  double submit_s, start_s, finish_s; /* host steady clock, seconds */
+} bhr_request_info;
+
+typedef struct bhr_engine_counters {
+  int queued, running, finished, tiles;
+  long long batch_steps;  /* bhr_engine_step iterations run */
+  double point_updates;   /* grid points advanced one step, all solves */
+  size_t bytes_in_use, budget;
+} bhr_engine_counters;
+
+int bhr_engine_create(int device, size_t hbm_budget_bytes, bhr_engine **out);
+void bhr_engine_destroy(bhr_engine *e);
+/* Queues a solve; traj_rows (nrows x 10, the .traj columns) may be NULL for
+ * a source-free solve.  The request's tile height is fixed at 16 rows, so
+ * p->M must be a multiple of 16.  Thread-safe against bhr_engine_step. */
+int bhr_engine_submit(bhr_engine *e, const bhr_params *p, const double *traj_rows, int nrows, int64_t *id);
+/* Admits what fits, advances all running solves by
+ * min(max_steps, fewest steps any of them has left), retires the finished
+ * ones; *running = solves still running. */
+int bhr_engine_step(bhr_engine *e, int max_steps, int *running);
+int bhr_engine_poll(bhr_engine *e, int64_t id, bhr_request_info *info);
+/* Waveform rows of a finished request (layout of bhr_solver_waveform). */
+int bhr_engine_result(bhr_engine *e, int64_t id, double *t, double *h, double *dedt, int max_rows, int *nrows);
+int bhr_engine_stats(bhr_engine *e, bhr_engine_counters *st);
+
 const char *bhr_last_error_string(void);
 int bhr_abi_version(void);
 

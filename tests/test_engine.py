@@ -1,0 +1,148 @@
+"""Batch engine (bhr_engine_*): many solves advanced by one launch per RK
+stage over a (solve, tile) work-list.
+
+A request's waveform must not depend on what it shares the GPU with: the
+same request run alone in an engine and in a mixed batch (other grids,
+spins, m, sourced and source-free, different lengths, joining mid-run)
+gives bit-identical rows.  Against a lone bhr_solver the rows agree to the
+FP64 bar (relative L2 1e-12; times bit-identical), and one engine request is
+checked against the CPU oracle directly.
+"""
+import numpy as np
+import pytest
+
+import bh_ringdown_b200 as bhr
+from bh_ringdown_b200.trajectory import synthetic_plunge
+from oracle import pyoracle
+
+pytestmark = pytest.mark.gpu
+
+WAVE_TOL = 1e-12
+
+
+def gauss(N, M, Xmin, Xmax, a, m, T, center=5.0):
+    # extraction at x = Xmin + 0.65 (Xmax - Xmin), inside the region the
+    # pulse crosses within T
+    return bhr.Params(N=N, M=M, Xmin=Xmin, Xmax=Xmax, a=a, m=m, dt=0.25 * (Xmax - Xmin) / N, Fr=5, T=T,
+                      out_start=0.0, ext_col=N * 65 // 100, init_kind=bhr.BHR_INIT_GAUSSIAN,
+                      init_center=center, init_width=2.0, init_ell=max(2.0, abs(m)))
+
+
+def plunge(N, M, Xmin, Xmax, a, m, T):
+    dt = 0.25 * (Xmax - Xmin) / N
+    prm = bhr.Params(N=N, M=M, Xmin=Xmin, Xmax=Xmax, a=a, m=m, dt=dt, Fr=5, T=T, out_start=0.0,
+                     ext_col=N * 6 // 10)
+    return prm, synthetic_plunge(a, dt / 2.0, duration=T)
+
+
+def requests():
+    p1, tr1 = plunge(256, 32, -50.0, 50.0, 0.6, 2.0, 30.0)
+    return [
+        (gauss(256, 32, -50.0, 50.0, 0.5, 2.0, 20.0), None),
+        (gauss(512, 64, -50.0, 50.0, 0.9, -3.0, 25.0, center=3.0), None),
+        (p1, tr1),
+        (gauss(128, 16, -40.0, 40.0, 0.0, 1.0, 12.0), None),
+    ]
+
+
+def run_alone(prm, traj):
+    with bhr.Engine() as e:
+        rid = e.submit(prm, traj)
+        e.run_all()
+        info = e.poll(rid)
+        assert info["state"] == bhr.Engine.DONE, info
+        return e.result(rid)
+
+
+def test_mixed_batch_is_bit_identical_to_alone():
+    reqs = requests()
+    alone = [run_alone(p, t) for p, t in reqs]
+    with bhr.Engine() as e:
+        ids = [e.submit(p, t) for p, t in reqs]
+        chunks = 0
+        while True:
+            running = e.step(7)  # small chunks: membership changes as solves finish
+            chunks += 1
+            if running == 0 and e.stats()["queued"] == 0:
+                break
+        assert chunks > 4
+        for rid, (t0, h0, d0) in zip(ids, alone):
+            t, h, d = e.result(rid)
+            assert len(t) > 0 and np.max(np.abs(h0)) > 1e-8
+            assert np.array_equal(t, t0) and np.array_equal(h, h0) and np.array_equal(d, d0)
+        st = e.stats()
+        assert st["finished"] == len(reqs) and st["running"] == 0 and st["bytes_in_use"] == 0
+
+
+def test_request_joining_mid_run_is_bit_identical():
+    reqs = requests()
+    alone = run_alone(*reqs[2])
+    with bhr.Engine() as e:
+        first = e.submit(*reqs[1])
+        e.step(40)
+        assert e.poll(first)["state"] == bhr.Engine.RUNNING
+        late = e.submit(*reqs[2])
+        assert e.poll(late)["state"] == bhr.Engine.QUEUED
+        e.step(10)
+        info = e.poll(late)
+        assert info["state"] == bhr.Engine.RUNNING and info["steps_done"] == 10
+        e.run_all()
+        t, h, d = e.result(late)
+        assert np.array_equal(t, alone[0]) and np.array_equal(h, alone[1]) and np.array_equal(d, alone[2])
+        info = e.poll(late)
+        assert info["submit_s"] <= info["start_s"] <= info["finish_s"]
+
+
+def test_engine_matches_lone_solver():
+    for prm, traj in requests():
+        s = bhr.Solver(prm)
+        if traj is not None:
+            s.set_trajectory(traj)
+        s.run()
+        ts, hs, ds = s.waveform()
+        s.close()
+        t, h, d = run_alone(prm, traj)
+        assert np.array_equal(t, ts)
+        assert np.linalg.norm(h - hs) <= WAVE_TOL * np.linalg.norm(hs)
+
+
+def test_engine_request_matches_oracle():
+    prm = gauss(256, 32, -50.0, 50.0, 0.7, 2.0, 15.0)
+    t, h, d = run_alone(prm, None)
+    o = pyoracle.Oracle(prm.N, prm.M, prm.Xmin, prm.Xmax, prm.a, prm.m, prm.dt, T=prm.T, Fr=prm.Fr, out_start=0.0,
+                        ext_col=prm.ext_col)
+    o.init_gaussian(prm.init_center, prm.init_width, prm.init_ell)
+    with bhr.Solver(prm) as s:
+        nt = s.info()["nt"]
+    to, ho, do, steps, _, _ = o.run(nsteps=nt)
+    assert np.array_equal(t, to)
+    assert np.max(np.abs(ho)) > 1e-6  # the pulse has reached the extraction column
+    assert np.linalg.norm(h - ho) <= 1e-10 * np.linalg.norm(ho)
+
+
+def test_budget_admits_one_at_a_time_when_tight():
+    reqs = requests()[:2]
+    alone = [run_alone(p, t) for p, t in reqs]
+    with bhr.Engine(hbm_budget_bytes=1) as e:
+        ids = [e.submit(p, t) for p, t in reqs]
+        e.step(1)
+        st = e.stats()
+        assert st["running"] == 1 and st["queued"] == 1
+        e.run_all()
+        for rid, (t0, h0, d0) in zip(ids, alone):
+            t, h, d = e.result(rid)
+            assert np.array_equal(h, h0)
+
+
+def test_invalid_request_fails_alone():
+    good = requests()[0]
+    bad = gauss(200, 32, -50.0, 50.0, 0.5, 2.0, 10.0)  # N not a multiple of 64
+    with bhr.Engine() as e:
+        rb = e.submit(bad)
+        rg = e.submit(*good)
+        e.run_all()
+        assert e.poll(rb)["state"] == bhr.Engine.FAILED
+        assert e.poll(rb)["status"] == 1  # BHR_INVALID_ARG
+        with pytest.raises(bhr.BhrError):
+            e.result(rb)
+        assert e.poll(rg)["state"] == bhr.Engine.DONE
