@@ -378,6 +378,196 @@ def run_reference(args, rank, world):
     print(json.dumps(out))
 
 
+def _solve_steps(prm):
+    """Step count of a solve (the solver's own dt rule) without creating it."""
+    import bh_ringdown_b200 as bhr
+    if prm.dt > 0:
+        dt = prm.dt
+    else:
+        _, r, _ = bhr.grid(prm)
+        dt = prm.courant * min((prm.Xmax - prm.Xmin) / prm.N, r[0] * np.pi / prm.M)
+        if prm.out_every > 0:
+            dt = prm.out_every / np.ceil(prm.out_every / dt)
+    return int(prm.T / dt)
+
+
+def run_batch(args):
+    """Batched form: 64 seeded source-free solves of mixed size resident on
+    one GPU, advanced together by the engine (one launch per RK stage over
+    the (solve, tile) work-list, graph-captured), against the same solves
+    run one at a time through bhr_solver (each with its autotuned tile).
+
+    Throughput is device time (CUDA events) over `--steps` batch steps with
+    all 64 resident; the working set (GBs) is far above L2.  The plain
+    figure weights each solve's measured per-step time by its full step
+    count, so the ratio is the ratio of solves/s at equal work."""
+    import torch
+    import bh_ringdown_b200 as bhr
+    from bh_ringdown_b200.workloads import batch_requests
+    torch.cuda.set_device(0)
+    reqs = batch_requests(64)
+    nts = [_solve_steps(r.params) for r in reqs]
+    work = [nt * r.points() for nt, r in zip(nts, reqs)]
+    with bhr.Engine(hbm_budget_bytes=150 << 30) as e:
+        for r in reqs:
+            e.submit(r.params, r.traj)
+        e.step(args.warmup)
+        st0 = e.stats()
+        assert st0["running"] == len(reqs), st0
+        t0 = time.perf_counter()
+        with ClockSampler(0) as clk:
+            e.step(args.steps)
+        wall = time.perf_counter() - t0
+        st1 = e.stats()
+    dev_ms = st1["device_ms"] - st0["device_ms"]
+    pts = st1["point_updates"] - st0["point_updates"]
+    value = pts / (dev_ms / 1e3)
+    # one at a time, each solve alone
+    plain_ms = []
+    for r in reqs:
+        with bhr.Solver(r.params) as s:
+            s.time_steps(args.warmup)
+            plain_ms.append(s.time_steps(args.steps) / args.steps)
+    plain_value = sum(work) / (sum(nt * ms for nt, ms in zip(nts, plain_ms)) / 1e3)
+    mean_work = float(np.mean(work))
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "batch64: 64 seeded source-free FP64 solves, a~U[0,0.99], m~U{1..4}, "
+                               "N_r~{2048,4096,8192,16384}, N_theta~{64,128,256}, x in [-100,300], T=500",
+                   "points_per_batch_step": pts / args.steps, "l2": "working set > L2 (GBs)",
+                   "parallelism": "replicas x1"},
+        "solves_per_s": value / mean_work, "plain_value": plain_value, "plain_solves_per_s": plain_value / mean_work,
+        "speedup_vs_plain": value / plain_value,
+        "e2e": {"value": pts / wall, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "note": "wall clock around bhr_engine_step (host sync included)"},
+        "gpu_launches": args.steps * 4, "clocks": clk.summary(),
+    }
+    print(json.dumps(out))
+
+
+def run_serve(args):
+    """Served form: a seeded Poisson stream of solves (70 % source-free
+    2048-4096 x 64-128, 30 % plunge-driven 8192 x 128) submitted to the
+    engine as they arrive, at `--load` times the engine's measured capacity,
+    with a 150 GB admission budget.  Reports solves/s and p50/p99
+    time-to-waveform (submit -> waveform ready), beside the plain path that
+    serves the same stream one solve at a time (measured service times,
+    first-come first-served queue).  Final times are scaled by
+    `--time-scale` to bound the run."""
+    import threading
+    import torch
+    import bh_ringdown_b200 as bhr
+    from bh_ringdown_b200.workloads import serve_requests, with_arrivals
+    torch.cuda.set_device(0)
+    reqs = serve_requests(args.requests, 1.0, time_scale=args.time_scale)
+    nts = [_solve_steps(r.params) for r in reqs]
+    work = np.array([nt * r.points() for nt, r in zip(nts, reqs)], dtype=np.float64)
+    budget = 150 << 30
+
+    # capacity: a saturated engine on the first requests, device throughput
+    ncal = min(len(reqs), 48)
+    with bhr.Engine(hbm_budget_bytes=budget) as e:
+        for r in reqs[:ncal]:
+            e.submit(r.params, r.traj)
+        e.step(0)
+        e.step(20)
+        st0 = e.stats()
+        t0 = time.perf_counter()
+        while e.stats()["running"] == ncal and time.perf_counter() - t0 < 2.0:
+            e.step(50)
+        st1 = e.stats()
+    cal_rate = (st1["point_updates"] - st0["point_updates"]) / ((st1["device_ms"] - st0["device_ms"]) / 1e3)
+    capacity = cal_rate / float(np.mean(work))
+    rate = args.load * capacity
+    with_arrivals(reqs, rate)
+
+    # the stream through the engine
+    with bhr.Engine(hbm_budget_bytes=budget) as e:
+        ids = [None] * len(reqs)
+        start = time.perf_counter()
+
+        stop = threading.Event()
+
+        def submitter():
+            for i, r in enumerate(reqs):
+                delay = r.arrival_s - (time.perf_counter() - start)
+                if delay > 0 and stop.wait(delay):
+                    return
+                if stop.is_set():
+                    return
+                ids[i] = e.submit(r.params, r.traj)
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        try:
+            with ClockSampler(0) as clk:
+                while True:
+                    running = e.step(args.chunk)
+                    if running == 0:
+                        if not th.is_alive() and e.stats()["queued"] == 0:
+                            break
+                        time.sleep(0.0005)
+        finally:
+            # the engine must outlive the submitting thread
+            stop.set()
+            th.join()
+        makespan = time.perf_counter() - start
+        lat, fails = [], 0
+        for rid in ids:
+            info = e.poll(rid)
+            if info["state"] != bhr.Engine.DONE:
+                fails += 1
+                continue
+            lat.append(info["finish_s"] - info["submit_s"])
+        st = e.stats()
+    lat = np.array(lat)
+
+    # the plain path: the same requests one at a time through bhr_solver
+    nplain = min(len(reqs), args.plain_requests)
+    service = []
+    for r in reqs[:nplain]:
+        t0 = time.perf_counter()
+        with bhr.Solver(r.params) as s:
+            if r.traj is not None:
+                s.set_trajectory(r.traj)
+            s.run()
+            s.waveform()
+        service.append(time.perf_counter() - t0)
+    service = np.array(service)
+    # first-come first-served single server over the same arrivals; requests
+    # past the measured subset reuse the subset's service times in turn
+    svc = np.resize(service, len(reqs))
+    fin, plat = 0.0, []
+    for r, sv in zip(reqs, svc):
+        fin = max(fin, r.arrival_s) + sv
+        plat.append(fin - r.arrival_s)
+    plat = np.array(plat)
+    plain_capacity = 1.0 / float(np.mean(service))
+    engine_capacity = capacity
+    out = {
+        "metric": METRIC, "value": len(lat) / makespan, "unit": "solves/s", "n_gpus": 1,
+        "steps": int(st["batch_steps"]), "warmup": 0, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"serve: {len(reqs)} seeded Poisson arrivals at {args.load:.0%} of measured capacity, "
+                               f"70% source-free (N_r 2048/4096, N_theta 64-128), 30% plunge (8192x128); "
+                               f"final times x{args.time_scale}", "hbm_budget_gb": budget / 2**30,
+                   "chunk_steps": args.chunk, "arrival_rate_per_s": rate, "parallelism": "replicas x1"},
+        "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)), "failed": fails,
+        "capacity_solves_per_s": engine_capacity,
+        "device_pt_updates_per_s": st["point_updates"] / (st["device_ms"] / 1e3),
+        "plain": {"capacity_solves_per_s": plain_capacity, "p50_s": float(np.percentile(plat, 50)),
+                  "p99_s": float(np.percentile(plat, 99)), "measured_requests": nplain,
+                  "note": "bhr_solver one request at a time, wall-clock service times, FCFS queue"},
+        "capacity_vs_plain": engine_capacity / plain_capacity,
+        "e2e": {"value": len(lat) / makespan, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "note": "wall clock of the whole stream through bhr_engine_submit/step/poll"},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -387,13 +577,22 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2000)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="plunge")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch64", "serve"], default="plunge")
+    ap.add_argument("--requests", type=int, default=200, help="serve: requests in the stream")
+    ap.add_argument("--time-scale", type=float, default=0.02, help="serve: factor on every request's final time")
+    ap.add_argument("--load", type=float, default=0.8, help="serve: arrival rate / measured capacity")
+    ap.add_argument("--chunk", type=int, default=64, help="serve: steps per engine call")
+    ap.add_argument("--plain-requests", type=int, default=60, help="serve: requests timed on the plain path")
     args = ap.parse_args()
-    global WORKLOAD
-    WORKLOAD = WORKLOADS[args.workload]
     if args.warmup < 3:
         args.warmup = 3
     rank, local_rank, world = env_rank()
+    if args.workload in ("batch64", "serve"):
+        if rank == 0:
+            (run_batch if args.workload == "batch64" else run_serve)(args)
+        return
+    global WORKLOAD
+    WORKLOAD = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, rank, world)
     else:

@@ -66,7 +66,7 @@ class _RequestInfo(C.Structure):
 
 class _EngineStats(C.Structure):
     _fields_ = [("queued", I), ("running", I), ("finished", I), ("tiles", I), ("batch_steps", C.c_longlong),
-                ("point_updates", D), ("bytes_in_use", C.c_size_t), ("budget", C.c_size_t)]
+                ("point_updates", D), ("device_ms", D), ("bytes_in_use", C.c_size_t), ("budget", C.c_size_t)]
 
 
 @dataclass

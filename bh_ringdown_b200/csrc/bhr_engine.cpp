@@ -89,10 +89,12 @@ struct bhr_engine {
   SourceArgs *d_src = nullptr;
   int cap_solves = 0, cap_tiles = 0, ntiles = 0, nsrc = 0, max_ptsx = 1, max_ptsy = 1;
   cudaGraphExec_t graph = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool dirty = true;
   // totals
   long long batch_steps = 0;
   double point_updates = 0.0;
+  double device_ms = 0.0;
   int finished = 0;
 };
 
@@ -176,29 +178,31 @@ int rebuild(bhr_engine *e) {
   // Blocks are ordered solve by solve, row block by row block.
   e->ntiles = static_cast<int>(tiles.size());
   e->nsrc = static_cast<int>(src.size());
-  auto grow = [&](auto **ptr, int need, int &cap) -> cudaError_t {
-    if (need <= cap) return cudaSuccess;
-    if (*ptr) cudaFree(*ptr);
-    *ptr = nullptr;
-    const int c = std::max(need, cap * 2);
-    cudaError_t err = cudaMalloc(reinterpret_cast<void **>(ptr), sizeof(**ptr) * static_cast<size_t>(c));
-    cap = err == cudaSuccess ? c : 0;
-    return err;
-  };
-  int cap_e = e->cap_solves, cap_s = e->cap_solves;
+  // The per-solve tables share one capacity; the work-list has its own.
   cudaError_t err = cudaSuccess;
   if (n > e->cap_solves) {
+    const int c = std::max(n, 2 * e->cap_solves);
+    if (e->d_solves) cudaFree(e->d_solves);
     if (e->d_ext) cudaFree(e->d_ext);
     if (e->d_src) cudaFree(e->d_src);
+    e->d_solves = nullptr;
     e->d_ext = nullptr;
     e->d_src = nullptr;
-    cap_e = cap_s = 0;
-    if ((err = grow(&e->d_ext, n, cap_e)) || (err = grow(&e->d_src, n, cap_s)) ||
-        (err = grow(&e->d_solves, n, e->cap_solves)))
+    e->cap_solves = 0;
+    if ((err = cudaMalloc(&e->d_solves, sizeof(BatchSolve) * c)) ||
+        (err = cudaMalloc(&e->d_ext, sizeof(ExtractArgs) * c)) || (err = cudaMalloc(&e->d_src, sizeof(SourceArgs) * c)))
       return set_fail(BHR_OUT_OF_MEMORY, std::string("engine tables: ") + cudaGetErrorString(err));
+    e->cap_solves = c;
   }
-  if ((err = grow(&e->d_tiles, e->ntiles, e->cap_tiles)))
-    return set_fail(BHR_OUT_OF_MEMORY, std::string("engine work-list: ") + cudaGetErrorString(err));
+  if (e->ntiles > e->cap_tiles) {
+    const int c = std::max(e->ntiles, 2 * e->cap_tiles);
+    if (e->d_tiles) cudaFree(e->d_tiles);
+    e->d_tiles = nullptr;
+    e->cap_tiles = 0;
+    if ((err = cudaMalloc(&e->d_tiles, sizeof(BatchTile) * c)))
+      return set_fail(BHR_OUT_OF_MEMORY, std::string("engine work-list: ") + cudaGetErrorString(err));
+    e->cap_tiles = c;
+  }
   if ((err = cudaMemcpyAsync(e->d_solves, solves.data(), sizeof(BatchSolve) * n, cudaMemcpyHostToDevice, e->stream)) ||
       (err = cudaMemcpyAsync(e->d_tiles, tiles.data(), sizeof(BatchTile) * tiles.size(), cudaMemcpyHostToDevice,
                              e->stream)) ||
@@ -317,7 +321,8 @@ int bhr_engine_create(int device, size_t hbm_budget_bytes, bhr_engine **out) {
   e->device = device;
   e->budget = hbm_budget_bytes;
   if (cudaSetDevice(device) != cudaSuccess || prepare_kernels() != cudaSuccess ||
-      cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&e->ev0) != cudaSuccess || cudaEventCreate(&e->ev1) != cudaSuccess) {
     delete e;
     return set_fail(BHR_CUDA_ERROR, "engine set-up failed");
   }
@@ -333,6 +338,8 @@ void bhr_engine_destroy(bhr_engine *e) {
   for (auto &R : e->active) bhr_solver_destroy(R.s);
   e->active.clear();
   release_tables(e);
+  if (e->ev0) cudaEventDestroy(e->ev0);
+  if (e->ev1) cudaEventDestroy(e->ev1);
   cudaStreamDestroy(e->stream);
   delete e;
 }
@@ -360,12 +367,13 @@ int bhr_engine_step(bhr_engine *e, int max_steps, int *running) {
   int n = max_steps;
   for (auto &R : e->active) n = std::min(n, R.remaining);
   if (!e->active.empty() && n > 0) {
-    for (int i = 0; i < n; i++) {
-      cudaError_t err = cudaGraphLaunch(e->graph, e->stream);
-      if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("graph launch: ") + cudaGetErrorString(err));
-    }
-    cudaError_t err = cudaStreamSynchronize(e->stream);
+    cudaError_t err = cudaEventRecord(e->ev0, e->stream);
+    for (int i = 0; i < n && err == cudaSuccess; i++) err = cudaGraphLaunch(e->graph, e->stream);
+    if (err == cudaSuccess) err = cudaEventRecord(e->ev1, e->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
     if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("engine step: ") + cudaGetErrorString(err));
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, e->ev0, e->ev1) == cudaSuccess) e->device_ms += ms;
     double pts = 0.0;
     for (auto &R : e->active) {
       R.remaining -= n;
@@ -442,6 +450,7 @@ int bhr_engine_stats(bhr_engine *e, bhr_engine_counters *st) {
   st->finished = e->finished;
   st->batch_steps = e->batch_steps;
   st->point_updates = e->point_updates;
+  st->device_ms = e->device_ms;
   st->bytes_in_use = e->used;
   st->budget = e->budget;
   st->tiles = e->ntiles;

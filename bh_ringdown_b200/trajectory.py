@@ -59,25 +59,31 @@ def synthetic_plunge(a: float, dt_row: float, duration: float, r_offset: float =
     r_stop_above_horizon of r+; after that the file simply ends (a reader
     past the end keeps the last row, as the reference's fscanf loop does).
     """
+    from scipy.integrate import solve_ivp
+
     r_isco, E, L = isco_prograde(a)
     r_plus = 1 + np.sqrt(1 - a * a)
-    y = np.array([r_isco - r_offset, 0.0])
-    sub = 8
-    h = dt_row / sub
-    rows = []
-    t = 0.0
     n = int(np.floor(duration / dt_row)) + 1
+    t_rows = np.arange(n) * dt_row
+    # Dense output of an 8th-order Dormand-Prince integration (relative
+    # tolerance 1e-13), sampled at the row times.
+    # The integration ends where r reaches r+ + r_stop_above_horizon / 2,
+    # past the last row kept.
+    def near_horizon(t, y):
+        return y[0] - (r_plus + 0.5 * r_stop_above_horizon)
+
+    near_horizon.terminal = True
+    sol = solve_ivp(lambda t, y: _rhs(y, a, E, L), (0.0, t_rows[-1] if n > 1 else dt_row),
+                    np.array([r_isco - r_offset, 0.0]), method="DOP853", rtol=1e-13, atol=1e-13,
+                    dense_output=True, events=near_horizon)
+    t_rows = t_rows[t_rows <= sol.t[-1]]
+    n = len(t_rows)
+    y = sol.sol(t_rows)
+    rows = []
     for i in range(n):
-        r, phi = y
+        r, phi = y[0, i], y[1, i]
         if r < r_plus + r_stop_above_horizon:
             break
-        rdot, phidot = _rhs(y, a, E, L)
-        rows.append((t, r, np.pi / 2, rdot, 0.0, phidot, phi, E, L, 0.0))
-        for _ in range(sub):
-            k1 = _rhs(y, a, E, L)
-            k2 = _rhs(y + 0.5 * h * k1, a, E, L)
-            k3 = _rhs(y + 0.5 * h * k2, a, E, L)
-            k4 = _rhs(y + h * k3, a, E, L)
-            y = y + h / 6 * (k1 + 2 * k2 + 2 * k3 + k4)
-        t = (i + 1) * dt_row
+        rdot, phidot = _rhs((r, phi), a, E, L)
+        rows.append((t_rows[i], r, np.pi / 2, rdot, 0.0, phidot, phi, E, L, 0.0))
     return np.array(rows, dtype=np.float64)

@@ -219,6 +219,7 @@ typedef struct bhr_engine_counters {
   int queued, running, finished, tiles;
   long long batch_steps;  /* bhr_engine_step iterations run */
   double point_updates;   /* grid points advanced one step, all solves */
+  double device_ms;       /* device time of the batch steps (CUDA events) */
   size_t bytes_in_use, budget;
 } bhr_engine_counters;
 

@@ -93,6 +93,22 @@ def test_request_joining_mid_run_is_bit_identical():
         assert info["submit_s"] <= info["start_s"] <= info["finish_s"]
 
 
+def test_membership_growing_one_by_one():
+    """Requests joining one per call (the device tables regrow as the batch
+    grows) and leaving at different steps."""
+    reqs = [(gauss(128, 16, -40.0, 40.0, 0.1 * i, 1.0 + i % 3, 6.0 + i), None) for i in range(7)]
+    alone = [run_alone(p, t) for p, t in reqs]
+    with bhr.Engine() as e:
+        ids = []
+        for p, t in reqs:
+            ids.append(e.submit(p, t))
+            e.step(3)
+        e.run_all()
+        for rid, (t0, h0, d0) in zip(ids, alone):
+            t, h, d = e.result(rid)
+            assert np.array_equal(t, t0) and np.array_equal(h, h0) and np.array_equal(d, d0)
+
+
 def test_engine_matches_lone_solver():
     for prm, traj in requests():
         s = bhr.Solver(prm)
