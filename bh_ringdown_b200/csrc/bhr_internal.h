@@ -99,7 +99,7 @@ struct ExtractArgs {
 // coefficient planes (bb with column halo; 1/bir and ee) and the column
 // factor table.
 struct StageMaps {
-  CUtensorMap q, p, u, coef_bb, coef_ie, colf;
+  CUtensorMap q, p, u, coef_bb, coef_ie, colf, rowf;
 };
 
 // A batch of solves advanced together: per solve, the tensor maps and
@@ -122,7 +122,8 @@ cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, c
 // and the tensor maps over them and over the column table.
 cudaError_t launch_coef_tables(const double *coltab, const double *rowtab, double *ctab, int N, int M,
                                cudaStream_t st);
-cudaError_t encode_coef_maps(double *ctab, const double *coltab, int N, int M, int rows, StageMaps *maps);
+cudaError_t encode_coef_maps(double *ctab, const double *coltab, const double *rowtab, int N, int M, int rows,
+                             StageMaps *maps);
 cudaError_t launch_source(const SourceArgs &a, cudaStream_t st);
 cudaError_t launch_stage_batch(int stage, int rows, const BatchSolve *solves, const BatchTile *tiles, int ntiles,
                                cudaStream_t st);

@@ -135,7 +135,9 @@ struct __align__(128) StageSmem {
   double ie[2][ROWS][TC];       // TMA box {TC, ROWS, 2}: 1/bir and ee on the tile columns
   double cf[kColFields][TC];    // TMA box {TC, 9}: column factors of the tile columns
   double un[4][ROWS][TC];       // TMA box {TC, ROWS, 4}: u^n (stages 2 and 3)
+  double rf[3][ROWS];           // TMA box {ROWS, 3}: row factors cos, g, ctan of the tile rows
   uint64_t bar;
+  int src_c0, src_r0;           // source patch corner of this step
 };
 
 // Time-independent per-point coefficients bb, 1/bir and ee
@@ -176,13 +178,14 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
   __syncthreads();
   if (tid == 0) {
     const uint32_t bytes = static_cast<uint32_t>(sizeof(S.q) + sizeof(S.p) + sizeof(S.bb) + sizeof(S.ie) +
-                                                 sizeof(S.cf) + (STAGE == 1 ? 0 : sizeof(S.un)));
+                                                 sizeof(S.cf) + sizeof(S.rf) + (STAGE == 1 ? 0 : sizeof(S.un)));
     mbar_expect_tx(&S.bar, bytes);
-    // Coefficient planes and column factors are written once, at set-up:
-    // they can be requested before the previous kernel has finished.
+    // Coefficient planes and column/row factors are written once, at
+    // set-up: they can be requested before the previous kernel has finished.
     tma_load_3d(&S.bb[0][0], &T.coef_bb, c0 - 4, b0, 0, &S.bar);
     tma_load_3d(&S.ie[0][0][0], &T.coef_ie, c0, b0, 1, &S.bar);
     tma_load_2d(&S.cf[0][0], &T.colf, c0, CF_CCN, &S.bar);
+    tma_load_2d(&S.rf[0][0], &T.rowf, b0, RF_COS, &S.bar);
   }
   // Everything below reads what the earlier kernels of the step wrote.
   grid_dependency_wait();
@@ -191,9 +194,13 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
     tma_load_3d(&S.q[0][0][0], &T.q, c0 - 4, b0 - 3, 0, &S.bar);
     tma_load_3d(&S.p[0][0][0], &T.p, c0 - 4, b0, 2, &S.bar);
     if (STAGE != 1) tma_load_3d(&S.un[0][0][0], &T.u, c0, b0, 0, &S.bar);
+    // The step's source record, read while the tiles are in flight.
+    if (A.src != nullptr) {
+      const StepRec &rec = A.recs[A.rs->k];
+      S.src_c0 = rec.col0;
+      S.src_r0 = rec.row0;
+    }
   }
-
-  const double *rt = A.rowtab;
 
   const bool ok = mbar_wait_bounded(&S.bar, 0);
   if (!__syncthreads_and(ok)) {
@@ -260,9 +267,8 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
   int src_c0 = 0, src_r0 = 0;
   bool tile_src = false;
   if (A.src != nullptr) {
-    const StepRec &rec = A.recs[A.rs->k];
-    src_c0 = rec.col0;
-    src_r0 = rec.row0;
+    src_c0 = S.src_c0;
+    src_r0 = S.src_r0;
     tile_src = (src_c0 < c0 + TC) && (src_c0 + A.PTSX > c0) && (src_r0 < b0 + TR) && (src_r0 + A.PTSY > b0);
   }
 
@@ -281,7 +287,7 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
     if (!inner && (a0 + 1 < 3 || a0 >= N - 3)) continue;
 
     // Theta derivatives of q (HighOrder/kern.cu:206-226).
-    const double ctan_cy = __ldg(rt + RF_CTAN * M + b) * A.cy;
+    const double ctan_cy = S.rf[RF_CTAN - RF_COS][r] * A.cy;
     double ll[2][2];
 #pragma unroll
     for (int pl = 0; pl < 2; pl++) {
@@ -302,8 +308,8 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
     }
 
     // Coefficients at the two points (HighOrder/kern.cu:132-158, 192-197).
-    const double cs = __ldg(rt + RF_COS * M + b);
-    const double gth = __ldg(rt + RF_G * M + b);
+    const double cs = S.rf[0][r];
+    const double gth = S.rf[RF_G - RF_COS][r];
     double kbb[2], kee[2], kdre[2], kdim[2], kare[2], kaim[2], kvre[2], kvim[2];
     double res[4][2];
     // bb on columns a0-4 .. a0+5, and the per-column arrays, as 16-byte pairs
@@ -514,55 +520,91 @@ __global__ void closure_ends_kernel(double *P, int N, int M) {
 }
 
 // ---- particle source patch (HighOrder/kern.cu:1185-1227, 2666-2683) ---------
-__device__ __forceinline__ void source_patch(const SourceArgs &A, const int j, const int k) {
+// The smeared delta is separable: the radial Gaussian factors R0..R2, the
+// tilde-phi phase and Delta depend on the column only, the angular factors
+// T0..T2 on the row only.  A block takes kSrcRows patch rows: each thread
+// forms its column's factors once, the first threads form the rows'
+// factors, and the per-point work is the bilinear sum and the epilogue.
+constexpr int kSrcRows = 4;
+
+__device__ __forceinline__ void source_rows(const SourceArgs &A, const int j0, const int k) {
+  __shared__ double rowf[kSrcRows][5];  // T0, T1, T2, cos theta, sin theta
+  __shared__ int rok[kSrcRows];
+  // By value: the stores to the patch below must not force reloads.
+  const StepRec rec = A.recs[A.rs->k];
+  double *__restrict__ src = A.src;
+  const double a = A.a, mass = A.mass;
+  if (k < kSrcRows) {
+    const int row = j0 + k + rec.row0;
+    const bool ok = (j0 + k < A.PTSY) && row > 0 && row < A.M;
+    rok[k] = ok;
+    if (ok) {
+      const double g0 = 1.0 / sqrt(2.0 * kPie);
+      const double th = A.theta[row], wt = A.wt;
+      const double dth = th - rec.tp;
+      const double T0 = g0 * exp(-dth * dth / (2.0 * wt * wt)) / wt;
+      rowf[k][0] = T0;
+      rowf[k][1] = -dth / (wt * wt) * T0;
+      rowf[k][2] = (-1.0 / (wt * wt) + dth * dth / (wt * wt * wt * wt)) * T0;
+      rowf[k][3] = cos(th);
+      rowf[k][4] = sin(th);
+    }
+  }
+  __syncthreads();
   if (k >= A.PTSX) return;
-  const StepRec &rec = A.recs[A.rs->k];
-  const int row = j + rec.row0, col = k + rec.col0;
-  double sre = 0.0, sim = 0.0;
-  if (col > 0 && col < A.N && row > 0 && row < A.M) {
-    const double a = A.a, mass = A.mass;
+  const int col = k + rec.col0;
+  const bool cok = col > 0 && col < A.N;
+  double r = 0.0, R0 = 0.0, R1 = 0.0, R2 = 0.0, cph = 0.0, sph = 0.0, delta = 0.0, c8 = 0.0, ra2 = 0.0;
+  if (cok) {
     const double rpl = mass + sqrt(mass * mass - a * a), rmn = mass - sqrt(mass * mass - a * a);
     const double g0 = 1.0 / sqrt(2.0 * kPie);
-    const double th = A.theta[row], r = A.r_c[col];
-    const double st = sin(th), ctv = cos(th);
-    const double wt = A.wt, wr = rec.wr;
-    const double dth = th - rec.tp;
-    const double T0 = g0 * exp(-dth * dth / (2.0 * wt * wt)) / wt;
-    const double T1 = -dth / (wt * wt) * T0;
-    const double T2 = (-1.0 / (wt * wt) + dth * dth / (wt * wt * wt * wt)) * T0;
+    const double wr = rec.wr;
+    r = A.r_c[col];
     const double dr = r - rec.rp;
-    const double R0 = g0 * exp(-dr * dr / (2.0 * wr * wr)) / wr;
-    const double R1 = -dr / (wr * wr) * R0;
-    const double R2 = (-1.0 / (wr * wr) + dr * dr / (wr * wr * wr * wr)) * R0;
-    const double bas[6] = {R0 * T0, R0 * T1, R0 * T2, R1 * T0, R1 * T1, R2 * T0};
-    double tr = 0.0, ti = 0.0;
-#pragma unroll
-    for (int i = 0; i < 6; i++) {
-      tr += rec.c_re[i] * bas[i];
-      ti += rec.c_im[i] * bas[i];
-    }
-    // TT = Sigma * t / rho^4 with rho = -1/(r - i a cos): 1/rho^4 = (r - i a cos)^4.
-    const double x = r, y = -a * ctv;
-    const double x2 = x * x - y * y, y2 = 2.0 * x * y;        // (x+iy)^2
-    const double x4 = x2 * x2 - y2 * y2, y4 = 2.0 * x2 * y2;  // (x+iy)^4
-    const double sig = r * r + a * a * ctv * ctv;
-    double Tr = sig * (tr * x4 - ti * y4), Ti = sig * (tr * y4 + ti * x4);
+    R0 = g0 * exp(-dr * dr / (2.0 * wr * wr)) / wr;
+    R1 = -dr / (wr * wr) * R0;
+    R2 = (-1.0 / (wr * wr) + dr * dr / (wr * wr * wr * wr)) * R0;
     const double ph = -A.m * a / (rpl - rmn) * log((r - rpl) / (r - rmn));
-    const double cph = cos(ph), sph = sin(ph);
-    const double Ur = Tr * cph - Ti * sph, Ui = Tr * sph + Ti * cph;
-    const double delta = r * r + a * a - 2.0 * mass * r;
-    const double cs2 = (r * r + a * a) * (r * r + a * a) - a * a * delta * st * st;
-    sre = 8.0 * kPie * delta * Ur / cs2 / (r * r * r);
-    sim = 8.0 * kPie * delta * Ui / cs2 / (r * r * r);
+    sincos(ph, &sph, &cph);
+    delta = r * r + a * a - 2.0 * mass * r;
+    c8 = 8.0 * kPie * delta / (r * r * r);  // 8 pi Delta / r^3
+    ra2 = (r * r + a * a) * (r * r + a * a);
   }
-  A.src[static_cast<size_t>(j) * A.PTSX + k] = sre;
-  A.src[static_cast<size_t>(A.PTSY + j) * A.PTSX + k] = sim;
+#pragma unroll
+  for (int jj = 0; jj < kSrcRows; jj++) {
+    const int j = j0 + jj;
+    if (j >= A.PTSY) break;
+    double sre = 0.0, sim = 0.0;
+    if (cok && rok[jj]) {
+      const double T0 = rowf[jj][0], T1 = rowf[jj][1], T2 = rowf[jj][2], ctv = rowf[jj][3], st = rowf[jj][4];
+      const double bas[6] = {R0 * T0, R0 * T1, R0 * T2, R1 * T0, R1 * T1, R2 * T0};
+      double tr = 0.0, ti = 0.0;
+#pragma unroll
+      for (int i = 0; i < 6; i++) {
+        tr += rec.c_re[i] * bas[i];
+        ti += rec.c_im[i] * bas[i];
+      }
+      // TT = Sigma * t / rho^4 with rho = -1/(r - i a cos): 1/rho^4 = (r - i a cos)^4.
+      const double x = r, y = -a * ctv;
+      const double x2 = x * x - y * y, y2 = 2.0 * x * y;        // (x+iy)^2
+      const double x4 = x2 * x2 - y2 * y2, y4 = 2.0 * x2 * y2;  // (x+iy)^4
+      const double sig = r * r + a * a * ctv * ctv;
+      const double Tr = sig * (tr * x4 - ti * y4), Ti = sig * (tr * y4 + ti * x4);
+      const double Ur = Tr * cph - Ti * sph, Ui = Tr * sph + Ti * cph;
+      // 8 pi Delta U / (((r^2+a^2)^2 - a^2 Delta sin^2) r^3)
+      const double f = c8 / (ra2 - a * a * delta * st * st);
+      sre = f * Ur;
+      sim = f * Ui;
+    }
+    src[static_cast<size_t>(j) * A.PTSX + k] = sre;
+    src[static_cast<size_t>(A.PTSY + j) * A.PTSX + k] = sim;
+  }
 }
 
 __global__ void source_patch_kernel(const SourceArgs A) {
   grid_dependency_wait();
   launch_dependents();
-  source_patch(A, blockIdx.x, threadIdx.x);
+  source_rows(A, blockIdx.x * kSrcRows, threadIdx.x);
 }
 
 // Sourced solves of a batch: blockIdx.y picks the solve.
@@ -570,36 +612,51 @@ __global__ void source_batch_kernel(const SourceArgs *args) {
   grid_dependency_wait();
   launch_dependents();
   const SourceArgs &A = args[blockIdx.y];
-  if (static_cast<int>(blockIdx.x) < A.PTSY) source_patch(A, blockIdx.x, threadIdx.x);
+  if (static_cast<int>(blockIdx.x) * kSrcRows < A.PTSY) source_rows(A, blockIdx.x * kSrcRows, threadIdx.x);
 }
 
 // ---- extraction, integration, projection (HighOrder/body.cu:168-212) ------
 constexpr int kExtractThreads = 256;
 constexpr int kSums = 15;
 
+// Every kernel of a step calls griddepcontrol.wait before it lets its
+// dependents start, so when this kernel starts, the previous step's
+// extraction (the only writer of integ, rows and the RunState) has
+// completed: those, and the weights written at set-up, are read before the
+// wait; only psi at the extraction column waits for stage 3.
 __device__ __forceinline__ void extract_body(const ExtractArgs &A) {
   __shared__ double red[kExtractThreads / 32][kSums];
-  __shared__ int nan_flag;
   const int tid = threadIdx.x;
   const int N = A.N, M = A.M;
   const size_t NM = static_cast<size_t>(N) * M;
   const int k = A.rs->k;
+  const int nrow = A.rs->nrow;
+  const double timer = A.rs->timer;
   const bool out_step = ((k % A.Fr) == 0) && (static_cast<double>(k) * A.dt >= A.out_start);
-  if (tid == 0) nan_flag = 0;
-  __syncthreads();
+  int bad = 0;
   double acc[kSums];
 #pragma unroll
   for (int i = 0; i < kSums; i++) acc[i] = 0.0;
   for (int b = tid; b < M; b += kExtractThreads) {
+    double in[4], wl[7], we = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) in[i] = A.integ[i * M + b];
+#pragma unroll
+    for (int l = 0; l < 7; l++) wl[l] = out_step ? A.wproj[l * M + b] : 0.0;
+    if (out_step) we = A.wdedt[b];
+    if (b == tid) {
+      grid_dependency_wait();
+      launch_dependents();
+    }
     const double psr = closed_val(A.u, N, M, A.even_m, b, A.ext_col);
     const double psi = closed_val(A.u + NM, N, M, A.even_m, b, A.ext_col);
-    if (!isfinite(psr) || !isfinite(psi)) nan_flag = 1;
+    if (!isfinite(psr) || !isfinite(psi)) bad = 1;
     A.ext[b] = psr;
     A.ext[M + b] = psi;
-    const double ir = A.integ[b] + psr * A.dt;
-    const double ii = A.integ[M + b] + psi * A.dt;
-    const double dr = A.integ[2 * M + b] + ir * A.dt;
-    const double di = A.integ[3 * M + b] + ii * A.dt;
+    const double ir = in[0] + psr * A.dt;
+    const double ii = in[1] + psi * A.dt;
+    const double dr = in[2] + ir * A.dt;
+    const double di = in[3] + ii * A.dt;
     A.integ[b] = ir;
     A.integ[M + b] = ii;
     A.integ[2 * M + b] = dr;
@@ -607,12 +664,15 @@ __device__ __forceinline__ void extract_body(const ExtractArgs &A) {
     if (out_step) {
 #pragma unroll
       for (int l = 0; l < 7; l++) {
-        const double wl = A.wproj[l * M + b];
-        acc[2 * l] += wl * dr;
-        acc[2 * l + 1] -= wl * di;
+        acc[2 * l] += wl[l] * dr;
+        acc[2 * l + 1] -= wl[l] * di;
       }
-      acc[14] += (ir * ir + ii * ii) * A.wdedt[b];
+      acc[14] += (ir * ir + ii * ii) * we;
     }
+  }
+  if (tid >= M) {  // threads without a row still wait before the block ends
+    grid_dependency_wait();
+    launch_dependents();
   }
   if (out_step) {
 #pragma unroll
@@ -623,34 +683,28 @@ __device__ __forceinline__ void extract_body(const ExtractArgs &A) {
       if ((tid & 31) == 0) red[tid >> 5][i] = v;
     }
   }
-  __syncthreads();
+  const int any_bad = __syncthreads_or(bad);
   if (tid == 0) {
-    if (nan_flag) atomicCAS(&A.rs->err, 0, 4 /* BHR_NAN_DETECTED */);
-    if (out_step && A.rs->nrow < A.max_rows) {
-      double *row = A.rows + static_cast<size_t>(A.rs->nrow) * 16;
-      row[0] = A.rs->timer - A.Xmax;
+    if (any_bad) atomicCAS(&A.rs->err, 0, 4 /* BHR_NAN_DETECTED */);
+    if (out_step && nrow < A.max_rows) {
+      double *row = A.rows + static_cast<size_t>(nrow) * 16;
+      row[0] = timer - A.Xmax;
       for (int i = 0; i < kSums; i++) {
         double v = 0.0;
         for (int w = 0; w < kExtractThreads / 32; w++) v += red[w][i];
         row[1 + i] = v;
       }
-      A.rs->nrow += 1;
+      A.rs->nrow = nrow + 1;
     }
-    A.rs->timer += A.dt;
+    A.rs->timer = timer + A.dt;
     A.rs->k = k + 1;
   }
 }
 
-__global__ void __launch_bounds__(kExtractThreads) extract_kernel(const ExtractArgs A) {
-  grid_dependency_wait();
-  launch_dependents();
-  extract_body(A);
-}
+__global__ void __launch_bounds__(kExtractThreads) extract_kernel(const ExtractArgs A) { extract_body(A); }
 
 // One block per solve of a batch.
 __global__ void __launch_bounds__(kExtractThreads) extract_batch_kernel(const ExtractArgs *args) {
-  grid_dependency_wait();
-  launch_dependents();
   extract_body(args[blockIdx.x]);
 }
 
@@ -671,7 +725,8 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return encode;
 }
 
-cudaError_t encode_coef_maps(double *ctab, const double *coltab, int N, int M, int rows, StageMaps *maps) {
+cudaError_t encode_coef_maps(double *ctab, const double *coltab, const double *rowtab, int N, int M, int rows,
+                             StageMaps *maps) {
   const cuuint32_t TRb = static_cast<cuuint32_t>(rows);
   auto encode = tensor_map_encoder();
   if (!encode) return cudaErrorNotSupported;
@@ -692,7 +747,14 @@ cudaError_t encode_coef_maps(double *ctab, const double *coltab, int N, int M, i
   CUresult r3 = encode(&maps->colf, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(coltab), cdims, cstrides,
                        box_cf, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  return (r1 == CUDA_SUCCESS && r2 == CUDA_SUCCESS && r3 == CUDA_SUCCESS) ? cudaSuccess : cudaErrorInvalidValue;
+  const cuuint64_t rdims[2] = {static_cast<cuuint64_t>(M), RF_COUNT};
+  const cuuint64_t rstrides[1] = {static_cast<cuuint64_t>(M) * 8};
+  const cuuint32_t box_rf[2] = {TRb, 3};
+  CUresult r4 = encode(&maps->rowf, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(rowtab), rdims, rstrides,
+                       box_rf, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                       CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return (r1 == CUDA_SUCCESS && r2 == CUDA_SUCCESS && r3 == CUDA_SUCCESS && r4 == CUDA_SUCCESS) ? cudaSuccess
+                                                                                              : cudaErrorInvalidValue;
 }
 
 cudaError_t launch_coef_tables(const double *coltab, const double *rowtab, double *ctab, int N, int M,
@@ -797,7 +859,8 @@ cudaError_t launch_stage_batch(int stage, int rows, const BatchSolve *solves, co
 
 cudaError_t launch_source_batch(const SourceArgs *args, int nsolves, int max_ptsy, int max_ptsx, cudaStream_t st) {
   if (nsolves <= 0) return cudaSuccess;
-  return launch_pdl(source_batch_kernel, dim3(max_ptsy, nsolves), dim3(max_ptsx), 0, st, args);
+  return launch_pdl(source_batch_kernel, dim3((max_ptsy + kSrcRows - 1) / kSrcRows, nsolves),
+                    dim3(std::max(max_ptsx, kSrcRows)), 0, st, args);
 }
 
 cudaError_t launch_extract_batch(const ExtractArgs *args, int nsolves, cudaStream_t st) {
@@ -806,7 +869,8 @@ cudaError_t launch_extract_batch(const ExtractArgs *args, int nsolves, cudaStrea
 }
 
 cudaError_t launch_source(const SourceArgs &a, cudaStream_t st) {
-  return launch_pdl(source_patch_kernel, dim3(a.PTSY), dim3(a.PTSX), 0, st, a);
+  return launch_pdl(source_patch_kernel, dim3((a.PTSY + kSrcRows - 1) / kSrcRows), dim3(std::max(a.PTSX, kSrcRows)), 0,
+                    st, a);
 }
 
 cudaError_t launch_extract(const ExtractArgs &a, cudaStream_t st) {

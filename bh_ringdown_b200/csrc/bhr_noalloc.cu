@@ -94,7 +94,7 @@ extern "C" int bhr_step_noalloc(const bhr_params *p, double *state, int nsteps, 
     CUtensorMap unused_q, unused_p;
     if (encode_state_maps(state, N, M, TR, &unused_q, &unused_p, &maps[i].u) != cudaSuccess ||
         encode_state_maps(bufs[i], N, M, TR, &maps[i].q, &maps[i].p, nullptr) != cudaSuccess ||
-        encode_coef_maps(ctab, coltab, N, M, TR, &maps[i]) != cudaSuccess)
+        encode_coef_maps(ctab, coltab, rowtab, N, M, TR, &maps[i]) != cudaSuccess)
       return fail(BHR_CUDA_ERROR, "bhr_step_noalloc: cuTensorMapEncodeTiled failed (state must be 16-byte aligned)");
   }
   // The tables must be current for this call; the flag must start at zero.

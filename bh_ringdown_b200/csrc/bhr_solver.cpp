@@ -429,7 +429,7 @@ static int encode_maps(bhr_solver *s, int rows) {
     CUtensorMap unused_q, unused_p;
     if (encode_state_maps(s->u0, p.N, p.M, rows, &unused_q, &unused_p, &m.u) != cudaSuccess ||
         encode_state_maps(bufs[i], p.N, p.M, rows, &m.q, &m.p, nullptr) != cudaSuccess ||
-        encode_coef_maps(s->ctab, s->coltab, p.N, p.M, rows, &m) != cudaSuccess) {
+        encode_coef_maps(s->ctab, s->coltab, s->rowtab, p.N, p.M, rows, &m) != cudaSuccess) {
       set_error("cuTensorMapEncodeTiled failed");
       return BHR_CUDA_ERROR;
     }
