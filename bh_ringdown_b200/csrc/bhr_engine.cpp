@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <mutex>
@@ -88,6 +89,8 @@ struct bhr_engine {
   ExtractArgs *d_ext = nullptr;
   SourceArgs *d_src = nullptr;
   int cap_solves = 0, cap_tiles = 0, ntiles = 0, nsrc = 0, max_ptsx = 1, max_ptsy = 1;
+  int persist = 1;          // persistent stage kernels over the work-list
+  int *d_err = nullptr;     // BHR_TIMEOUT from a bounded wait in a stage kernel
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool dirty = true;
@@ -128,7 +131,8 @@ int enqueue_batch_step(bhr_engine *e) {
     if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("source batch: ") + cudaGetErrorString(err));
   }
   for (int stage = 1; stage <= 3; stage++) {
-    cudaError_t err = launch_stage_batch(stage, e->rows, e->d_solves, e->d_tiles, e->ntiles, e->stream);
+    cudaError_t err =
+        launch_stage_batch(stage, e->rows, e->persist, e->d_solves, e->d_tiles, e->ntiles, e->d_err, e->stream);
     if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("stage batch: ") + cudaGetErrorString(err));
   }
   cudaError_t err = launch_extract_batch(e->d_ext, n, e->stream);
@@ -322,10 +326,13 @@ int bhr_engine_create(int device, size_t hbm_budget_bytes, bhr_engine **out) {
   e->budget = hbm_budget_bytes;
   if (cudaSetDevice(device) != cudaSuccess || prepare_kernels() != cudaSuccess ||
       cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&e->ev0) != cudaSuccess || cudaEventCreate(&e->ev1) != cudaSuccess) {
+      cudaEventCreate(&e->ev0) != cudaSuccess || cudaEventCreate(&e->ev1) != cudaSuccess ||
+      cudaMalloc(&e->d_err, sizeof(int)) != cudaSuccess || cudaMemset(e->d_err, 0, sizeof(int)) != cudaSuccess) {
     delete e;
     return set_fail(BHR_CUDA_ERROR, "engine set-up failed");
   }
+  // BHR_ENGINE_TILING=block selects the one-tile-per-block stage kernels.
+  if (const char *v = std::getenv("BHR_ENGINE_TILING")) e->persist = std::strcmp(v, "block") != 0;
   *out = e;
   return BHR_OK;
 }
@@ -340,6 +347,7 @@ void bhr_engine_destroy(bhr_engine *e) {
   release_tables(e);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
+  if (e->d_err) cudaFree(e->d_err);
   cudaStreamDestroy(e->stream);
   delete e;
 }
@@ -374,6 +382,9 @@ int bhr_engine_step(bhr_engine *e, int max_steps, int *running) {
     if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("engine step: ") + cudaGetErrorString(err));
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, e->ev0, e->ev1) == cudaSuccess) e->device_ms += ms;
+    int derr = 0;
+    if (cudaMemcpy(&derr, e->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess || derr != 0)
+      return set_fail(BHR_TIMEOUT, "engine step: a bounded device wait gave up");
     double pts = 0.0;
     for (auto &R : e->active) {
       R.remaining -= n;

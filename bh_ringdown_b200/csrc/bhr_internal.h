@@ -68,6 +68,7 @@ struct StageArgs {
   int N, M, PTSX, PTSY;
   int even_m;
   int rows;             // tile height: 8 or 16 theta rows
+  int persist;          // 1: 16-row tiles walked by one persistent block per SM
   double dt, cx, cy, cyy, cko;
 };
 
@@ -99,7 +100,8 @@ struct ExtractArgs {
 // coefficient planes (bb with column halo; 1/bir and ee) and the column
 // factor table.
 struct StageMaps {
-  CUtensorMap q, p, u, coef_bb, coef_ie, colf, rowf;
+  CUtensorMap q, p, u, coef_bb, colf, rowf;
+  CUtensorMap o;  // stage output planes, box {TC, rows, 4} (TMA stores)
 };
 
 // A batch of solves advanced together: per solve, the tensor maps and
@@ -125,8 +127,10 @@ cudaError_t launch_coef_tables(const double *coltab, const double *rowtab, doubl
 cudaError_t encode_coef_maps(double *ctab, const double *coltab, const double *rowtab, int N, int M, int rows,
                              StageMaps *maps);
 cudaError_t launch_source(const SourceArgs &a, cudaStream_t st);
-cudaError_t launch_stage_batch(int stage, int rows, const BatchSolve *solves, const BatchTile *tiles, int ntiles,
-                               cudaStream_t st);
+// persist = 1 walks the work-list with one block per SM (16-row tiles);
+// err receives BHR_TIMEOUT if a bounded wait gives up.
+cudaError_t launch_stage_batch(int stage, int rows, int persist, const BatchSolve *solves, const BatchTile *tiles,
+                               int ntiles, int *err, cudaStream_t st);
 cudaError_t launch_source_batch(const SourceArgs *args, int nsolves, int max_ptsy, int max_ptsx, cudaStream_t st);
 cudaError_t launch_extract_batch(const ExtractArgs *args, int nsolves, cudaStream_t st);
 cudaError_t launch_extract(const ExtractArgs &a, cudaStream_t st);

@@ -88,6 +88,23 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
+// 3D tiled TMA store from shared memory, tracked by this thread's bulk group.
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, const void *src, int x, int y, int z) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// The bulk stores of this thread have finished reading shared memory.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// The bulk stores of this thread are complete.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void named_barrier_sync(int id, int threads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
 // ---- stencils (HighOrder/kern.cu:192-261) ---------------------------------
 __device__ __forceinline__ double d1c(const double *v, int c) {
   return 45.0 * (v[c + 1] - v[c - 1]) - 9.0 * (v[c + 2] - v[c - 2]) + (v[c + 3] - v[c - 3]);
@@ -121,10 +138,6 @@ __device__ __forceinline__ double sqrt_nr(double x) {
   return x > 0.0 ? s : 0.0;
 }
 
-// Column factors the main pass reads per point: rows CF_CCN..CF_CIN of the
-// column table, in enum order.
-constexpr int kColFields = CF_COUNT - CF_CCN;
-enum { K_CCN = 0, K_XR, K_YR, K_CR0, K_CR1, K_BI0, K_BI1, K_BRI, K_CIN };
 
 // Shared memory of one tile of ROWS theta rows (8 or 16).
 template <int ROWS>
@@ -132,89 +145,91 @@ struct __align__(128) StageSmem {
   double q[2][ROWS + 6][WC];    // TMA box {WC, ROWS+6, 2}: planes q_re, q_im with halo
   double p[2][ROWS][WC];        // TMA box {WC, ROWS, 2}: planes p_re, p_im with column halo
   double bb[ROWS][WC];          // TMA box {WC, ROWS, 1}: bb on the window columns
-  double ie[2][ROWS][TC];       // TMA box {TC, ROWS, 2}: 1/bir and ee on the tile columns
-  double cf[kColFields][TC];    // TMA box {TC, 9}: column factors of the tile columns
+  double cf[CF_COUNT][TC];      // TMA box {TC, CF_COUNT}: column factors of the tile columns
   double un[4][ROWS][TC];       // TMA box {TC, ROWS, 4}: u^n (stages 2 and 3)
-  double rf[3][ROWS];           // TMA box {ROWS, 3}: row factors cos, g, ctan of the tile rows
+  double rf[RF_COUNT][ROWS];    // TMA box {ROWS, RF_COUNT}: row factors of the tile rows
   uint64_t bar;
   int src_c0, src_r0;           // source patch corner of this step
+  int done;                     // persistent kernels: warps done with this buffer's tile
+  int issued;                   // persistent kernels: load phases issued into this buffer
+  int abort;                    // persistent kernels (buffer 0): a bounded wait gave up
 };
 
-// Time-independent per-point coefficients bb, 1/bir and ee
-// (HighOrder/kern.cu:132-149) for the interior rows, once per solve.
+// 1/bir = 1/(B0 + B1 sin^2 theta) (HighOrder/kern.cu:132-149).
+__device__ __forceinline__ double inv_bir(double b0, double b1, double s2) { return rcp_nr(fma(b1, s2, b0)); }
+
+// The time-independent per-point coefficient bb (HighOrder/kern.cu:141-147),
+// which the stage kernels need on a stencil window, for the interior rows,
+// once per solve.  1/bir and ee = Ataurho + bb are formed per point by the
+// stage kernels from the column and row factors with the same arithmetic.
 __global__ void coef_table_kernel(const double *coltab, const double *rowtab, double *ctab, int N, int M) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   const int b = blockIdx.y;
   if (a >= N) return;
-  const size_t NM = static_cast<size_t>(N) * M, id = static_cast<size_t>(b) * N + a;
-  double bb = 0.0, ib = 0.0, ee = 0.0;
+  const size_t id = static_cast<size_t>(b) * N + a;
+  double bb = 0.0;
   if (b >= 3 && b < M - 3) {
-    ib = rcp_nr(fma(coltab[CF_B1 * N + a], rowtab[RF_S2 * M + b], coltab[CF_B0 * N + a]));
+    const double ib = inv_bir(coltab[CF_B0 * N + a], coltab[CF_B1 * N + a], rowtab[RF_S2 * M + b]);
     const double At = coltab[CF_ATN * N + a] * ib, Ar = coltab[CF_ARN * N + a] * ib;
     bb = -(At + sqrt_nr(fma(At, At, 4.0 * Ar))) * 0.5;
-    ee = At + bb;
   }
   ctab[id] = bb;
-  ctab[NM + id] = ib;
-  ctab[2 * NM + id] = ee;
 }
 
 // One tile (columns c0..c0+63, rows b0..b0+ROWS-1) of one SSP-RK3 stage.
+// A stage tile is processed in four steps, shared by the one-tile-per-block
+// kernels and the persistent ones: thread 0 arms the tile's mbarrier and
+// requests the set-up data, then (after the grid dependency) the stage
+// input; all threads wait, rebuild the closure rows in shared memory and
+// compute the tile's rows.
+
+// Thread 0: arm the barrier for every byte of the tile and request the
+// coefficient planes and column/row factors (written once, at set-up, so
+// they may be requested before the previous kernel has finished).
 template <int STAGE, int ROWS>
-__device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &A, const int c0, const int b0) {
-  constexpr int TR = ROWS;           // tile rows
-  constexpr int RPT = ROWS / 8;      // rows per thread
-  extern __shared__ unsigned char smem_raw[];
-  StageSmem<ROWS> &S = *reinterpret_cast<StageSmem<ROWS> *>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+__device__ __forceinline__ void tile_issue_setup(StageSmem<ROWS> &S, const StageMaps &T, const int c0, const int b0) {
+  const uint32_t bytes = static_cast<uint32_t>(sizeof(S.q) + sizeof(S.p) + sizeof(S.bb) + sizeof(S.cf) +
+                                               sizeof(S.rf) + (STAGE == 1 ? 0 : sizeof(S.un)));
+  mbar_expect_tx(&S.bar, bytes);
+  tma_load_3d(&S.bb[0][0], &T.coef_bb, c0 - 4, b0, 0, &S.bar);
+  tma_load_2d(&S.cf[0][0], &T.colf, c0, 0, &S.bar);
+  tma_load_2d(&S.rf[0][0], &T.rowf, b0, 0, &S.bar);
+}
+
+// Thread 0, before arming the tile's barrier (so the barrier publishes it):
+// this step's source patch corner.  The step counter is final when any
+// stage kernel starts: its predecessor (the source kernel of a sourced
+// step, or a stage kernel) starts its dependents only after its own grid
+// dependency on the previous step's extraction was satisfied.
+template <int ROWS>
+__device__ __forceinline__ void tile_note_source(StageSmem<ROWS> &S, const StageArgs &A) {
+  if (A.src != nullptr) {
+    const StepRec &rec = A.recs[A.rs->k];
+    S.src_c0 = rec.col0;
+    S.src_r0 = rec.row0;
+  }
+}
+
+// Thread 0, after the grid dependency: request the stage input (and u^n).
+template <int STAGE, int ROWS>
+__device__ __forceinline__ void tile_issue_state(StageSmem<ROWS> &S, const StageMaps &T, const int c0, const int b0) {
+  tma_load_3d(&S.q[0][0][0], &T.q, c0 - 4, b0 - 3, 0, &S.bar);
+  tma_load_3d(&S.p[0][0][0], &T.p, c0 - 4, b0, 2, &S.bar);
+  if (STAGE != 1) tma_load_3d(&S.un[0][0][0], &T.u, c0, b0, 0, &S.bar);
+}
+
+// All threads: the closure of the stage input, rebuilt in shared memory.
+template <int ROWS, int THREADS>
+__device__ __forceinline__ void tile_close(StageSmem<ROWS> &S, const StageArgs &A, const int c0, const int b0,
+                                           const int tid) {
+  constexpr int TR = ROWS;
   const int N = A.N, M = A.M;
-  const size_t NM = static_cast<size_t>(N) * M;
-
-  if (tid == 0) {
-    mbar_init(&S.bar, 1);
-    fence_barrier_init();
-  }
-  __syncthreads();
-  if (tid == 0) {
-    const uint32_t bytes = static_cast<uint32_t>(sizeof(S.q) + sizeof(S.p) + sizeof(S.bb) + sizeof(S.ie) +
-                                                 sizeof(S.cf) + sizeof(S.rf) + (STAGE == 1 ? 0 : sizeof(S.un)));
-    mbar_expect_tx(&S.bar, bytes);
-    // Coefficient planes and column/row factors are written once, at
-    // set-up: they can be requested before the previous kernel has finished.
-    tma_load_3d(&S.bb[0][0], &T.coef_bb, c0 - 4, b0, 0, &S.bar);
-    tma_load_3d(&S.ie[0][0][0], &T.coef_ie, c0, b0, 1, &S.bar);
-    tma_load_2d(&S.cf[0][0], &T.colf, c0, CF_CCN, &S.bar);
-    tma_load_2d(&S.rf[0][0], &T.rowf, b0, RF_COS, &S.bar);
-  }
-  // Everything below reads what the earlier kernels of the step wrote.
-  grid_dependency_wait();
-  launch_dependents();
-  if (tid == 0) {
-    tma_load_3d(&S.q[0][0][0], &T.q, c0 - 4, b0 - 3, 0, &S.bar);
-    tma_load_3d(&S.p[0][0][0], &T.p, c0 - 4, b0, 2, &S.bar);
-    if (STAGE != 1) tma_load_3d(&S.un[0][0][0], &T.u, c0, b0, 0, &S.bar);
-    // The step's source record, read while the tiles are in flight.
-    if (A.src != nullptr) {
-      const StepRec &rec = A.recs[A.rs->k];
-      S.src_c0 = rec.col0;
-      S.src_r0 = rec.row0;
-    }
-  }
-
-  const bool ok = mbar_wait_bounded(&S.bar, 0);
-  if (!__syncthreads_and(ok)) {
-    if (tid == 0) atomicCAS(A.err, 0, 5 /* BHR_TIMEOUT */);
-    mbar_wait_bounded(&S.bar, 0);
-    return;
-  }
-
   // Closure of the stage input rebuilt in shared memory.
   // Poles, q only (HighOrder/kern.cu:320-409): rows 2,1,0 from 3,4 and
   // M-3,M-2,M-1 from M-4,M-5 on columns 3..N-4; zero for odd m.
   const bool lo_rows = (b0 == 0), hi_rows = (b0 + TR + 3 > M - 3);
   if (lo_rows || hi_rows) {
-    for (int i = tid; i < 2 * WC; i += STAGE_THREADS) {
+    for (int i = tid; i < 2 * WC; i += THREADS) {
       const int pl = i / WC, w = i - pl * WC;
       const int a = c0 - 4 + w;
       if (a < 3 || a >= N - 3) continue;
@@ -243,7 +258,7 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
   // Radial ends, all four planes, tile rows (HighOrder/kern.cu:412-449).
   const bool lo_cols = (c0 == 0), hi_cols = (c0 + TC + 4 > N - 3);
   if (lo_cols || hi_cols) {
-    for (int i = tid; i < 4 * TR; i += STAGE_THREADS) {
+    for (int i = tid; i < 4 * TR; i += THREADS) {
       const int pl = i / TR, r = i - pl * TR;
       const int b = b0 + r;
       if (b < 3 || b >= M - 3) continue;
@@ -261,15 +276,26 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
       }
     }
   }
-  __syncthreads();
+}
 
-  // Source patch placement for this step.
+// All threads: the right-hand side and the Shu-Osher combination of the
+// tile's rows, written to the stage output.
+// TO_SMEM (tiles without closure points): the outputs overwrite u^n in the
+// tile buffer (each thread reads its u^n before writing there) for a TMA
+// store of the whole tile.
+template <int STAGE, int ROWS, int THREADS, bool TO_SMEM>
+__device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs &A, const int c0, const int b0,
+                                             const int tx, const int ty) {
+  constexpr int RPT = ROWS / (THREADS / 32);  // rows per thread
+  const int N = A.N, M = A.M;
+  const size_t NM = static_cast<size_t>(N) * M;
+  const bool lo_cols = (c0 == 0), hi_cols = (c0 + TC + 4 > N - 3);
   int src_c0 = 0, src_r0 = 0;
   bool tile_src = false;
   if (A.src != nullptr) {
     src_c0 = S.src_c0;
     src_r0 = S.src_r0;
-    tile_src = (src_c0 < c0 + TC) && (src_c0 + A.PTSX > c0) && (src_r0 < b0 + TR) && (src_r0 + A.PTSY > b0);
+    tile_src = (src_c0 < c0 + TC) && (src_c0 + A.PTSX > c0) && (src_r0 < b0 + ROWS) && (src_r0 + A.PTSY > b0);
   }
 
   const int a0 = c0 + 2 * tx;  // this thread's columns a0, a0+1
@@ -287,7 +313,7 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
     if (!inner && (a0 + 1 < 3 || a0 >= N - 3)) continue;
 
     // Theta derivatives of q (HighOrder/kern.cu:206-226).
-    const double ctan_cy = S.rf[RF_CTAN - RF_COS][r] * A.cy;
+    const double ctan_cy = S.rf[RF_CTAN][r] * A.cy;
     double ll[2][2];
 #pragma unroll
     for (int pl = 0; pl < 2; pl++) {
@@ -308,8 +334,9 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
     }
 
     // Coefficients at the two points (HighOrder/kern.cu:132-158, 192-197).
-    const double cs = S.rf[0][r];
-    const double gth = S.rf[RF_G - RF_COS][r];
+    const double cs = S.rf[RF_COS][r];
+    const double gth = S.rf[RF_G][r];
+    const double s2 = S.rf[RF_S2][r];
     double kbb[2], kee[2], kdre[2], kdim[2], kare[2], kaim[2], kvre[2], kvim[2];
     double res[4][2];
     // bb on columns a0-4 .. a0+5, and the per-column arrays, as 16-byte pairs
@@ -321,15 +348,17 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
       bw[2 * j + 1] = t.y;
     }
     auto pair = [&](const double *base) { return *reinterpret_cast<const double2 *>(base + 2 * tx); };
-    const double2 ib2 = pair(S.ie[0][r]), ee2 = pair(S.ie[1][r]);
-    const double2 f0 = pair(S.cf[K_CCN]), f1 = pair(S.cf[K_XR]), f2 = pair(S.cf[K_YR]), f3 = pair(S.cf[K_BI0]),
-                  f4 = pair(S.cf[K_BI1]), f5 = pair(S.cf[K_BRI]), f6 = pair(S.cf[K_CR0]), f7 = pair(S.cf[K_CR1]),
-                  f8 = pair(S.cf[K_CIN]);
+    const double2 g0 = pair(S.cf[CF_B0]), g1 = pair(S.cf[CF_B1]), g2 = pair(S.cf[CF_ATN]);
+    const double2 f0 = pair(S.cf[CF_CCN]), f1 = pair(S.cf[CF_XR]), f2 = pair(S.cf[CF_YR]), f3 = pair(S.cf[CF_BI0]),
+                  f4 = pair(S.cf[CF_BI1]), f5 = pair(S.cf[CF_BRI]), f6 = pair(S.cf[CF_CR0]), f7 = pair(S.cf[CF_CR1]),
+                  f8 = pair(S.cf[CF_CIN]);
 #pragma unroll
     for (int c = 0; c < 2; c++) {
       const int a = a0 + c;
       auto pk = [&](double2 v) { return c ? v.y : v.x; };
-      const double bb = bw[4 + c], ib = pk(ib2), ee = pk(ee2);
+      const double bb = bw[4 + c];
+      const double ib = inv_bir(pk(g0), pk(g1), s2);
+      const double ee = pk(g2) * ib + bb;  // Ataurho + bb
       const double dbdx = d1c(bw, 4 + c) * A.cx;
       const double cc = pk(f0) * ib;
       const double btr = pk(f1) * ib;
@@ -418,6 +447,10 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
           o[1] = kThird * (u.y + 2.0 * fc[pl][1] + 2.0 * dt * res[pl][1]);
         }
       }
+      if (TO_SMEM) {
+        *reinterpret_cast<double2 *>(&S.un[pl][r][2 * tx]) = make_double2(o[0], o[1]);
+        continue;
+      }
       double *dst = A.out + pl * NM + base;
       if (both) {
         *reinterpret_cast<double2 *>(dst) = make_double2(o[0], o[1]);
@@ -430,25 +463,219 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
   };
   if (!lo_cols && !hi_cols) rows(std::true_type{});
   else rows(std::false_type{});
-
 }
 
-// One solve: the grid is the solve's tiles.
+// One tile per block (grid N/64 x M/ROWS, two blocks per SM).
+template <int STAGE, int ROWS>
+__device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &A, const int c0, const int b0) {
+  extern __shared__ unsigned char smem_raw[];
+  StageSmem<ROWS> &S = *reinterpret_cast<StageSmem<ROWS> *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+  if (tid == 0) {
+    mbar_init(&S.bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    tile_note_source(S, A);
+    tile_issue_setup<STAGE>(S, T, c0, b0);
+  }
+  // Everything below reads what the earlier kernels of the step wrote.
+  grid_dependency_wait();
+  launch_dependents();
+  if (tid == 0) tile_issue_state<STAGE>(S, T, c0, b0);
+  const bool ok = mbar_wait_bounded(&S.bar, 0);
+  if (!__syncthreads_and(ok)) {
+    if (tid == 0) atomicCAS(A.err, 0, 5 /* BHR_TIMEOUT */);
+    mbar_wait_bounded(&S.bar, 0);
+    return;
+  }
+  tile_close<ROWS, STAGE_THREADS>(S, A, c0, b0, tid);
+  __syncthreads();
+  tile_compute<STAGE, ROWS, STAGE_THREADS, false>(S, A, c0, b0, tx, ty);
+}
+
 template <int STAGE, int ROWS>
 __global__ void __launch_bounds__(STAGE_THREADS, 2)
     stage_kernel(const __grid_constant__ StageMaps T, const StageArgs A) {
   stage_tile<STAGE, ROWS>(T, A, blockIdx.x * TC, blockIdx.y * ROWS);
 }
 
-// Many solves advanced together: block i takes entry i of the work-list of
-// (solve, tile) pairs; tensor maps and arguments come from the solve table
-// in device memory.
+// Several solves advanced together: block -> (solve, tile) from the work-list.
 template <int STAGE, int ROWS>
 __global__ void __launch_bounds__(STAGE_THREADS, 2)
     stage_batch_kernel(const BatchSolve *solves, const BatchTile *tiles) {
   const BatchTile t = tiles[blockIdx.x];
   const BatchSolve &B = solves[t.solve];
   stage_tile<STAGE, ROWS>(B.maps[STAGE - 1], B.args[STAGE - 1], t.c0, t.b0);
+}
+
+// ---- persistent stage kernels -------------------------------------------
+// One block of kPersistThreads per SM walks the tiles blockIdx.x,
+// blockIdx.x + gridDim.x, ... through two shared-memory tile buffers: the
+// loads of tile i+2 are issued as soon as tile i is computed, so they run
+// under the computation of tile i+1 and the SM's share of HBM bandwidth is
+// kept busy.  Tile work is the same code as the one-tile-per-block kernels.
+constexpr int kPersistThreads = 512;
+constexpr int kPersistRows = 16;
+
+// Work item i of this block: the solve's maps and arguments and the tile
+// corner.  Single solve: tiles in row-major order over the N/64 x M/16 grid.
+struct SingleWork {
+  const StageMaps *T;
+  const StageArgs *A;
+  int ntiles, tiles_x;
+  __device__ __forceinline__ int count() const { return ntiles; }
+  __device__ __forceinline__ void get(int t, const StageMaps *&tm, const StageArgs *&ta, int &c0, int &b0) const {
+    tm = T;
+    ta = A;
+    c0 = (t % tiles_x) * TC;
+    b0 = (t / tiles_x) * kPersistRows;
+  }
+};
+template <int STAGE>
+struct BatchWork {
+  const BatchSolve *solves;
+  const BatchTile *tiles;
+  int ntiles;
+  __device__ __forceinline__ int count() const { return ntiles; }
+  __device__ __forceinline__ void get(int t, const StageMaps *&tm, const StageArgs *&ta, int &c0, int &b0) const {
+    const BatchTile w = tiles[t];
+    tm = &solves[w.solve].maps[STAGE - 1];
+    ta = &solves[w.solve].args[STAGE - 1];
+    c0 = w.c0;
+    b0 = w.b0;
+  }
+};
+
+// Warps are not held together between tiles: each waits for the tile's
+// data itself, and the last warp to finish a tile (a shared counter) stores
+// it (TMA, for tiles without closure points) and refills the buffer with
+// tile i+2.  Tiles with closure points rebuild them first, behind a named
+// barrier all warps reach in the same order.  After a bounded wait gives up
+// the block records BHR_TIMEOUT, issues nothing more and lets the loads in
+// flight land before it exits.
+template <int STAGE, class Work>
+__device__ __forceinline__ void stage_persistent(const Work &W, int *err) {
+  constexpr int ROWS = kPersistRows, NWARPS = kPersistThreads / 32;
+  extern __shared__ unsigned char smem_raw[];
+  StageSmem<ROWS> *buf = reinterpret_cast<StageSmem<ROWS> *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+  const int ntiles = W.count(), stride = gridDim.x, first = blockIdx.x;
+  volatile int *abort_flag = &buf[0].abort;
+  if (tid == 0) {
+    for (int j = 0; j < 2; j++) {
+      mbar_init(&buf[j].bar, 1);
+      buf[j].done = 0;
+      buf[j].issued = 0;
+    }
+    buf[0].abort = 0;
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const StageMaps *tm;
+  const StageArgs *ta;
+  int c0, b0;
+  if (tid == 0) {
+    for (int j = 0; j < 2; j++) {
+      const int t = first + j * stride;
+      if (t < ntiles) {
+        W.get(t, tm, ta, c0, b0);
+        tile_note_source(buf[j], *ta);
+        tile_issue_setup<STAGE>(buf[j], *tm, c0, b0);
+        buf[j].issued = 1;
+      }
+    }
+  }
+  grid_dependency_wait();
+  launch_dependents();
+  if (tid == 0) {
+    for (int j = 0; j < 2; j++) {
+      const int t = first + j * stride;
+      if (t < ntiles) {
+        W.get(t, tm, ta, c0, b0);
+        tile_issue_state<STAGE>(buf[j], *tm, c0, b0);
+      }
+    }
+  }
+  int i = 0;
+  for (int t = first; t < ntiles; t += stride, i++) {
+    StageSmem<ROWS> &S = buf[i & 1];
+    bool stop = *abort_flag != 0;
+    if (!stop && !mbar_wait_bounded(&S.bar, (i >> 1) & 1)) {
+      if (tx == 0) {
+        atomicExch(&buf[0].abort, 1);
+        atomicCAS(err, 0, 5 /* BHR_TIMEOUT */);
+      }
+      stop = true;
+    }
+    stop = __any_sync(0xffffffffu, stop);
+    W.get(t, tm, ta, c0, b0);
+    const int N = ta->N, M = ta->M;
+    const bool edge = (b0 == 0) || (b0 + ROWS + 3 > M - 3) || (c0 == 0) || (c0 + TC + 4 > N - 3);
+    const bool full = (b0 >= 3) && (b0 + ROWS <= M - 3) && (c0 >= 3) && (c0 + TC <= N - 3);
+    if (edge) {
+      if (!stop) tile_close<ROWS, kPersistThreads>(S, *ta, c0, b0, tid);
+      named_barrier_sync(1, kPersistThreads);
+    }
+    if (!stop) {
+      if (full) {
+        tile_compute<STAGE, ROWS, kPersistThreads, true>(S, *ta, c0, b0, tx, ty);
+        fence_proxy_async();  // this thread's outputs, for the TMA store
+      } else {
+        tile_compute<STAGE, ROWS, kPersistThreads, false>(S, *ta, c0, b0, tx, ty);
+      }
+    }
+    __syncwarp();
+    if (tx == 0) {
+      __threadfence_block();
+      if (atomicAdd(&S.done, 1) == NWARPS - 1) {
+        __threadfence_block();
+        S.done = 0;
+        const bool ab = *abort_flag != 0;
+        if (full && !ab) {
+          tma_store_3d(&tm->o, &S.un[0][0][0], c0, b0, 0);
+          bulk_commit();
+          bulk_wait_read();
+        }
+        const int tn = t + 2 * stride;
+        if (tn < ntiles && !ab) {
+          fence_proxy_async();
+          const StageMaps *tm2;
+          const StageArgs *ta2;
+          int c2, b2;
+          W.get(tn, tm2, ta2, c2, b2);
+          tile_note_source(S, *ta2);
+          tile_issue_setup<STAGE>(S, *tm2, c2, b2);
+          tile_issue_state<STAGE>(S, *tm2, c2, b2);
+          S.issued += 1;
+        }
+      }
+    }
+  }
+  // The TMA stores this thread issued, then (after a failure) the loads
+  // still in flight.
+  if (tx == 0) bulk_wait_all();
+  __syncthreads();
+  if (tid == 0 && *abort_flag != 0)
+    for (int j = 0; j < 2; j++)
+      if (buf[j].issued > 0) mbar_wait_bounded(&buf[j].bar, (buf[j].issued - 1) & 1);
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(kPersistThreads, 1)
+    stage_persistent_kernel(const __grid_constant__ StageMaps T, const __grid_constant__ StageArgs A) {
+  SingleWork W{&T, &A, (A.N / TC) * (A.M / kPersistRows), A.N / TC};
+  stage_persistent<STAGE>(W, A.err);
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(kPersistThreads, 1)
+    stage_persistent_batch_kernel(const BatchSolve *solves, const BatchTile *tiles, int ntiles, int *err) {
+  BatchWork<STAGE> W{solves, tiles, ntiles};
+  stage_persistent<STAGE>(W, err);
 }
 
 // ---- closure of stored planes (HighOrder/kern.cu:622-753) ------------------
@@ -730,18 +957,14 @@ cudaError_t encode_coef_maps(double *ctab, const double *coltab, const double *r
   const cuuint32_t TRb = static_cast<cuuint32_t>(rows);
   auto encode = tensor_map_encoder();
   if (!encode) return cudaErrorNotSupported;
-  const cuuint64_t dims[3] = {static_cast<cuuint64_t>(N), static_cast<cuuint64_t>(M), 3};
+  const cuuint64_t dims[3] = {static_cast<cuuint64_t>(N), static_cast<cuuint64_t>(M), 1};
   const cuuint64_t strides[2] = {static_cast<cuuint64_t>(N) * 8, static_cast<cuuint64_t>(N) * M * 8};
   const cuuint32_t estr[3] = {1, 1, 1};
   const cuuint32_t box_bb[3] = {WC, TRb, 1};
-  const cuuint32_t box_ie[3] = {TC, TRb, 2};
   const cuuint64_t cdims[2] = {static_cast<cuuint64_t>(N), CF_COUNT};
   const cuuint64_t cstrides[1] = {static_cast<cuuint64_t>(N) * 8};
-  const cuuint32_t box_cf[2] = {TC, kColFields};
+  const cuuint32_t box_cf[2] = {TC, CF_COUNT};
   CUresult r1 = encode(&maps->coef_bb, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, ctab, dims, strides, box_bb, estr,
-                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  CUresult r2 = encode(&maps->coef_ie, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, ctab, dims, strides, box_ie, estr,
                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   CUresult r3 = encode(&maps->colf, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(coltab), cdims, cstrides,
@@ -749,12 +972,11 @@ cudaError_t encode_coef_maps(double *ctab, const double *coltab, const double *r
                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   const cuuint64_t rdims[2] = {static_cast<cuuint64_t>(M), RF_COUNT};
   const cuuint64_t rstrides[1] = {static_cast<cuuint64_t>(M) * 8};
-  const cuuint32_t box_rf[2] = {TRb, 3};
+  const cuuint32_t box_rf[2] = {TRb, RF_COUNT};
   CUresult r4 = encode(&maps->rowf, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(rowtab), rdims, rstrides,
                        box_rf, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  return (r1 == CUDA_SUCCESS && r2 == CUDA_SUCCESS && r3 == CUDA_SUCCESS && r4 == CUDA_SUCCESS) ? cudaSuccess
-                                                                                              : cudaErrorInvalidValue;
+  return (r1 == CUDA_SUCCESS && r3 == CUDA_SUCCESS && r4 == CUDA_SUCCESS) ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 cudaError_t launch_coef_tables(const double *coltab, const double *rowtab, double *ctab, int N, int M,
@@ -817,7 +1039,30 @@ static cudaError_t launch_rows(int stage, const StageMaps &maps, const StageArgs
   return launch_pdl(stage_kernel<3, ROWS>, grid, block, smem, st, maps, a);
 }
 
+// Multiprocessors of the current device (cached per device).
+static int sm_count() {
+  static int counts[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (counts[dev] == 0) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    counts[dev] = n > 0 ? n : 148;
+  }
+  return counts[dev];
+}
+
+static size_t persist_smem_bytes() { return 2 * sizeof(StageSmem<kPersistRows>) + 128; }
+
 cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st) {
+  if (a.persist) {
+    const int ntiles = (a.N / TC) * (a.M / kPersistRows);
+    const dim3 grid(std::min(ntiles, sm_count())), block(32, kPersistThreads / 32);
+    const size_t smem = persist_smem_bytes();
+    if (stage == 1) return launch_pdl(stage_persistent_kernel<1>, grid, block, smem, st, maps, a);
+    if (stage == 2) return launch_pdl(stage_persistent_kernel<2>, grid, block, smem, st, maps, a);
+    return launch_pdl(stage_persistent_kernel<3>, grid, block, smem, st, maps, a);
+  }
   return a.rows == 8 ? launch_rows<8>(stage, maps, a, st) : launch_rows<16>(stage, maps, a, st);
 }
 
@@ -838,12 +1083,27 @@ cudaError_t prepare_kernels() {
       (e = cudaFuncSetAttribute(stage_batch_kernel<2, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)) ||
       (e = cudaFuncSetAttribute(stage_batch_kernel<3, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)))
     return e;
+  const int sp = static_cast<int>(persist_smem_bytes());
+  if ((e = cudaFuncSetAttribute(stage_persistent_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp)) ||
+      (e = cudaFuncSetAttribute(stage_persistent_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp)) ||
+      (e = cudaFuncSetAttribute(stage_persistent_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp)) ||
+      (e = cudaFuncSetAttribute(stage_persistent_batch_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp)) ||
+      (e = cudaFuncSetAttribute(stage_persistent_batch_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp)) ||
+      (e = cudaFuncSetAttribute(stage_persistent_batch_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp)))
+    return e;
   return cudaSuccess;
 }
 
-cudaError_t launch_stage_batch(int stage, int rows, const BatchSolve *solves, const BatchTile *tiles, int ntiles,
-                               cudaStream_t st) {
+cudaError_t launch_stage_batch(int stage, int rows, int persist, const BatchSolve *solves, const BatchTile *tiles,
+                               int ntiles, int *err, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
+  if (persist) {
+    const dim3 grid(std::min(ntiles, sm_count())), block(32, kPersistThreads / 32);
+    const size_t smem = persist_smem_bytes();
+    if (stage == 1) return launch_pdl(stage_persistent_batch_kernel<1>, grid, block, smem, st, solves, tiles, ntiles, err);
+    if (stage == 2) return launch_pdl(stage_persistent_batch_kernel<2>, grid, block, smem, st, solves, tiles, ntiles, err);
+    return launch_pdl(stage_persistent_batch_kernel<3>, grid, block, smem, st, solves, tiles, ntiles, err);
+  }
   const dim3 grid(ntiles), block(32, STAGE_THREADS / 32);
   if (rows == 8) {
     const size_t smem = sizeof(StageSmem<8>) + 128;

@@ -25,13 +25,13 @@ constexpr int kNoAllocMaxPoints = 131072;  // N*M
 constexpr int kNoAllocMaxN = 16384;
 constexpr int kNoAllocMaxM = 1024;
 constexpr size_t kStageDoubles = 4 * static_cast<size_t>(kNoAllocMaxPoints);
-constexpr size_t kCoefOff = 2 * kStageDoubles;  // per-point coefficient planes
-constexpr size_t kColOff = kCoefOff + 3 * static_cast<size_t>(kNoAllocMaxPoints);
+constexpr size_t kCoefOff = 2 * kStageDoubles;  // per-point coefficient plane bb
+constexpr size_t kColOff = kCoefOff + static_cast<size_t>(kNoAllocMaxPoints);
 constexpr size_t kRowOff = kColOff + static_cast<size_t>(CF_COUNT) * kNoAllocMaxN;
 constexpr size_t kFlagOff = kRowOff + static_cast<size_t>(RF_COUNT) * kNoAllocMaxM;
-constexpr size_t kScratchDoubles = kFlagOff + 32;  // about 13.3 MB in all
+constexpr size_t kScratchDoubles = kFlagOff + 32;  // about 11.2 MB in all
 
-// Scratch: [u1 | u2 | coefficient planes | column tables | row tables | error flag].  In host code
+// Scratch: [u1 | u2 | coefficient plane bb | column tables | row tables | error flag].  In host code
 // this name is only a stand-in for the device symbol; the device address
 // comes from cudaGetSymbolAddress below.
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
@@ -93,6 +93,7 @@ extern "C" int bhr_step_noalloc(const bhr_params *p, double *state, int nsteps, 
   for (int i = 0; i < 3; i++) {
     CUtensorMap unused_q, unused_p;
     if (encode_state_maps(state, N, M, TR, &unused_q, &unused_p, &maps[i].u) != cudaSuccess ||
+        encode_state_maps(bufs[(i + 1) % 3], N, M, TR, &unused_q, &unused_p, &maps[i].o) != cudaSuccess ||
         encode_state_maps(bufs[i], N, M, TR, &maps[i].q, &maps[i].p, nullptr) != cudaSuccess ||
         encode_coef_maps(ctab, coltab, rowtab, N, M, TR, &maps[i]) != cudaSuccess)
       return fail(BHR_CUDA_ERROR, "bhr_step_noalloc: cuTensorMapEncodeTiled failed (state must be 16-byte aligned)");

@@ -210,7 +210,7 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
   }
   if ((st = dalloc(s, &s->u0, 4 * NM)) || (st = dalloc(s, &s->u1, 4 * NM)) || (st = dalloc(s, &s->u2, 4 * NM)) ||
       (st = dalloc(s, &s->coltab, static_cast<size_t>(CF_COUNT) * p.N)) ||
-      (st = dalloc(s, &s->rowtab, static_cast<size_t>(RF_COUNT) * p.M)) || (st = dalloc(s, &s->ctab, 3 * NM)) ||
+      (st = dalloc(s, &s->rowtab, static_cast<size_t>(RF_COUNT) * p.M)) || (st = dalloc(s, &s->ctab, NM)) ||
       (st = dalloc(s, &s->rc, p.N)) ||
       (st = dalloc(s, &s->th, p.M)) || (st = dalloc(s, &s->src, 2 * static_cast<size_t>(p.PTSX) * p.PTSY)) ||
       (st = dalloc(s, &s->ext, 2 * static_cast<size_t>(p.M))) || (st = dalloc(s, &s->integ, 4 * static_cast<size_t>(p.M))) ||
@@ -240,6 +240,18 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
     free_all(s);
     delete s;
     return BHR_CUDA_ERROR;
+  }
+  // BHR_STAGE_TILING=block8|block16|persistent fixes the stage tiling of
+  // solves whose tiling is not fixed by the caller.
+  if (tile_rows == 0) {
+    if (const char *v = std::getenv("BHR_STAGE_TILING")) {
+      if (!std::strcmp(v, "block8")) tile_rows = 8;
+      if (!std::strcmp(v, "block16")) tile_rows = 16;
+      if (!std::strcmp(v, "persistent")) {
+        tile_rows = 16;
+        s->persist = 1;
+      }
+    }
   }
   if (int st = (tile_rows == 8 || tile_rows == 16) ? encode_maps(s, tile_rows) : autotune_rows(s)) {
     free_all(s);
@@ -277,6 +289,7 @@ int bhr_solver_info(const bhr_solver *s, bhr_info *info) {
   info->r_plus = s->g.r_plus;
   info->device_bytes = s->bytes;
   info->tile_rows = s->tile_rows;
+  info->persistent = s->persist;
   return BHR_OK;
 }
 
@@ -428,6 +441,7 @@ static int encode_maps(bhr_solver *s, int rows) {
     StageMaps &m = s->maps[i];
     CUtensorMap unused_q, unused_p;
     if (encode_state_maps(s->u0, p.N, p.M, rows, &unused_q, &unused_p, &m.u) != cudaSuccess ||
+        encode_state_maps(bufs[(i + 1) % 3], p.N, p.M, rows, &unused_q, &unused_p, &m.o) != cudaSuccess ||
         encode_state_maps(bufs[i], p.N, p.M, rows, &m.q, &m.p, nullptr) != cudaSuccess ||
         encode_coef_maps(s->ctab, s->coltab, s->rowtab, p.N, p.M, rows, &m) != cudaSuccess) {
       set_error("cuTensorMapEncodeTiled failed");
@@ -439,26 +453,31 @@ static int encode_maps(bhr_solver *s, int rows) {
 }
 
 
-// Tile-height autotuner: per (device, N, M) the stage kernels are timed with
-// 8- and 16-row tiles on stages 1 and 2, which write only the solve's
-// scratch stages (u1, u2), and the faster height is kept for the process.
+// Stage tiling autotuner: per (device, N, M) the stage kernels are timed
+// with 8- and 16-row tiles one per block and with the persistent 16-row
+// kernels, on stages 1 and 2 (which write only the solve's scratch stages
+// u1, u2); the fastest is kept for the process.
 static int autotune_rows(bhr_solver *s) {
   static std::mutex mu;
-  static std::vector<std::array<int, 4>> cache;  // device, N, M, rows
+  static std::vector<std::array<int, 5>> cache;  // device, N, M, rows, persist
   const bhr_params &p = s->p;
   {
     std::lock_guard<std::mutex> lock(mu);
     for (auto &c : cache)
-      if (c[0] == p.device && c[1] == p.N && c[2] == p.M) return encode_maps(s, c[3]);
+      if (c[0] == p.device && c[1] == p.N && c[2] == p.M) {
+        s->persist = c[4];
+        return encode_maps(s, c[3]);
+      }
   }
-  static const int cands[2] = {8, 16};
+  static const int cands[3][2] = {{8, 0}, {16, 0}, {16, 1}};
   double best_ms = 1e30;
-  int best = 16;
+  int best = 1;
   cudaEvent_t e0, e1;
   BHR_CUDA_TRY(cudaEventCreate(&e0));
   BHR_CUDA_TRY(cudaEventCreate(&e1));
-  for (int rows : cands) {
-    if (int st = encode_maps(s, rows)) return st;
+  for (int c = 0; c < 3; c++) {
+    s->persist = cands[c][1];
+    if (int st = encode_maps(s, cands[c][0])) return st;
     StageArgs A = solver_stage_args(s);
     A.src = nullptr;
     for (int rep = 0; rep < 6; rep++) {
@@ -474,16 +493,17 @@ static int autotune_rows(bhr_solver *s) {
     BHR_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
     if (ms < best_ms) {
       best_ms = ms;
-      best = rows;
+      best = c;
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   {
     std::lock_guard<std::mutex> lock(mu);
-    cache.push_back({p.device, p.N, p.M, best});
+    cache.push_back({p.device, p.N, p.M, cands[best][0], cands[best][1]});
   }
-  return encode_maps(s, best);
+  s->persist = cands[best][1];
+  return encode_maps(s, cands[best][0]);
 }
 
 StageArgs bhr::solver_stage_args(bhr_solver *s) {
@@ -503,6 +523,7 @@ StageArgs bhr::solver_stage_args(bhr_solver *s) {
   A.PTSY = p.PTSY;
   A.even_m = s->even_m ? 1 : 0;
   A.rows = s->tile_rows;
+  A.persist = s->persist;
   A.dt = p.dt;
   A.cx = 0.016666666666667 * odx;
   A.cy = 0.05 * third * odth;

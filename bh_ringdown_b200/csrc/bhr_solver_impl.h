@@ -22,6 +22,7 @@ struct bhr_solver {
   size_t bytes = 0;
   bhr::StageMaps maps[3];  // per stage input state (u^n, u1, u2)
   int tile_rows = 16; // stage tile height chosen for this grid
+  int persist = 0;     // 1: persistent stage kernels (16-row tiles, one block per SM)
   int steps_done = 0;
   // Captured step graphs: one step, and kGraphBatch steps in one launch.
   cudaGraphExec_t g1 = nullptr, gb = nullptr;
@@ -29,7 +30,9 @@ struct bhr_solver {
 
 
 namespace bhr {
-// Creates a solve; tile_rows 0 lets the autotuner pick 8 or 16.
+// Creates a solve; tile_rows 0 lets the autotuner pick the stage tiling
+// (8- or 16-row tiles one per block, or persistent), 8 or 16 fixes
+// one-tile-per-block kernels of that height.
 int solver_create(const bhr_params *p, int tile_rows, bhr_solver **out);
 // Launch arguments of the solve's kernels (stage pointers vin/un/out unset).
 StageArgs solver_stage_args(bhr_solver *s);

@@ -101,6 +101,7 @@ typedef struct bhr_info {
   double r_plus;
   size_t device_bytes;
   int tile_rows;      /* stage tile height the autotuner chose (8 or 16)   */
+  int persistent;     /* 1: persistent stage kernels (one block per SM)      */
 } bhr_info;
 
 typedef struct bhr_solver bhr_solver;
@@ -185,7 +186,7 @@ double bhr_swsh(double ell, double m, double theta);
  * (16-byte aligned); it is advanced nsteps steps in place on `stream` (a
  * cudaStream_t, NULL for the default stream) and closed again on return.
  * p->dt must be > 0.  The two intermediate stages and the coefficient
- * tables live in one fixed file-scope device array of about 13 MB, so
+ * tables live in one fixed file-scope device array of about 11 MB, so
  * grids are limited to N*M <= 131072, N <= 16384, M <= 1024; larger ones
  * are rejected with BHR_INVALID_ARG.  Every GPU that loads the library
  * holds that array until the process exits.  The first call on a device

@@ -156,3 +156,23 @@ def test_headline_workload_grid_matches_oracle():
     s.step(40)
     o.run(traj=rows, coef_fn=product_coef_fn(), nsteps=40, max_rows=10)
     assert rel_field_err(s.get_state(), o.get_state()) <= FIELD_TOL
+
+
+@pytest.mark.parametrize("tiling", ["block8", "block16", "persistent"])
+def test_every_stage_tiling_matches_oracle(tiling, monkeypatch):
+    """Each stage tiling (8- and 16-row tiles one per block, persistent
+    blocks walking 16-row tiles through two buffers) on a sourced plunge
+    whose grid has several tiles per persistent block and a patch that
+    crosses tile edges."""
+    monkeypatch.setenv("BHR_STAGE_TILING", tiling)
+    s, o, rows, coef = traj_pair(1024, 64, -50.0, 50.0, 0.7, 2.0, ext_col=640)
+    info = s.info()
+    assert info["persistent"] == (tiling == "persistent")
+    assert info["tile_rows"] == (8 if tiling == "block8" else 16)
+    n = 120
+    s.step(n)
+    t, h, dedt, steps, _, _ = o.run(traj=rows, coef_fn=coef, nsteps=n)
+    ts, hs, es = s.waveform()
+    assert np.array_equal(ts, t)
+    assert rel_field_err(s.get_state(), o.get_state()) <= FIELD_TOL
+    assert np.linalg.norm(hs - h) <= WAVE_TOL * np.linalg.norm(h)
