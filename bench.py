@@ -22,6 +22,7 @@ ranks and value is the sum of all ranks' updates over that time.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import sys
@@ -42,6 +43,11 @@ WORKLOADS = {
 }
 WORKLOAD = WORKLOADS["plunge"]
 BYTES_PER_PT = 256.0  # FP64 SSP-RK3 algorithmic bytes per point per step (coefficients recomputed)
+# Mixed precision: stage 1 reads u^n and writes u1 (FP64) and delta1 (FP32),
+# stage 2 reads delta1 and writes eps2 (FP32), stage 3 reads eps2 and u1 and
+# writes u^{n+1}: 80 + 32 + 80 bytes per point.
+BYTES_PER_PT_MIXED = 192.0
+PRECISION = "fp64"
 
 
 def env_rank():
@@ -148,7 +154,7 @@ def make_params(device=0, dt=None):
     w = WORKLOAD
     return bhr.Params(N=w["N"], M=w["M"], Xmin=w["Xmin"], Xmax=w["Xmax"], a=w["a"], m=w["m"], T=w["T"],
                       dt=0.0 if dt is None else dt, courant=w["courant"], Fr=50, out_start=0.0, device=device,
-                      init_kind=bhr.BHR_INIT_ZERO)
+                      init_kind=bhr.BHR_INIT_ZERO, precision=bhr.BHR_MIXED if PRECISION == "mixed" else bhr.BHR_FP64)
 
 
 def workload_inputs(with_source, device=0):
@@ -225,7 +231,8 @@ def run_ours(args, rank, local_rank, world):
     ms_per_step = total_ms / args.steps
     stage_ms = per_kernel[1:4] / args.steps
     peak, peak_kind = measured_peak()
-    achieved = BYTES_PER_PT * N * M / (float(stage_ms.sum()) / 1e3) / 1e9
+    bytes_pt = BYTES_PER_PT_MIXED if PRECISION == "mixed" else BYTES_PER_PT
+    achieved = bytes_pt * N * M / (float(stage_ms.sum()) / 1e3) / 1e9
     traffic_pp = profile_traffic()
 
     # End to end through the public API: host params + host trajectory in,
@@ -256,8 +263,9 @@ def run_ours(args, rank, local_rank, world):
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: FP64 s=-2 m=2 a=0.9, {N}x{M} on [-200,600]"
+            "vs_baseline": None, "dtype": "f64" if PRECISION == "fp64" else "f64+f32", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {'FP64' if PRECISION == 'fp64' else 'mixed FP64/FP32'} "
+                                   f"s=-2 m=2 a=0.9, {N}x{M} on [-200,600]"
                                    + (", plunge source" if with_source else ", source-free (Gaussian pulse initial data)"),
                        "N_r": N, "N_theta": M, "dt": prm.dt, "integrator": "SSP-RK3",
                        "source": "synthetic prograde equatorial plunge from ISCO" if with_source else "none",
@@ -265,7 +273,8 @@ def run_ours(args, rank, local_rank, world):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": None if traffic_pp is None else traffic_pp * N * M,
-                         "kernel": "stage_kernel<1,2,3> (one SSP-RK3 step, 256 B/pt algorithmic)"},
+                         "kernel": ("stage_kernel<1,2,3> (one SSP-RK3 step, 256 B/pt algorithmic)" if PRECISION == "fp64"
+                                    else "FP64 stage 1 + FP32 mixed_stage_kernel<2,3> (192 B/pt algorithmic)")},
             "kernel_ms": {"source": per_kernel[0] / args.steps, "stage1": stage_ms[0], "stage2": stage_ms[1],
                           "stage3": stage_ms[2], "extract": per_kernel[4] / args.steps},
             "gpu_launches": args.steps * (5 if with_source else 4),
@@ -405,12 +414,14 @@ def run_batch(args):
     import bh_ringdown_b200 as bhr
     from bh_ringdown_b200.workloads import batch_requests
     torch.cuda.set_device(0)
-    reqs = batch_requests(64)
+    reqs = batch_requests(64, precision=bhr.BHR_MIXED if PRECISION == "mixed" else bhr.BHR_FP64)
     nts = [_solve_steps(r.params) for r in reqs]
     work = [nt * r.points() for nt, r in zip(nts, reqs)]
     with bhr.Engine(hbm_budget_bytes=150 << 30) as e:
         for r in reqs:
             e.submit(r.params, r.traj)
+        while e.stats()["queued"] > 0:  # requests are prepared off the stepping thread
+            e.step(0)
         e.step(args.warmup)
         st0 = e.stats()
         assert st0["running"] == len(reqs), st0
@@ -425,7 +436,7 @@ def run_batch(args):
     # one at a time, each solve alone
     plain_ms = []
     for r in reqs:
-        with bhr.Solver(r.params) as s:
+        with bhr.Solver(dataclasses.replace(r.params, precision=bhr.BHR_FP64)) as s:
             s.time_steps(args.warmup)
             plain_ms.append(s.time_steps(args.steps) / args.steps)
     plain_value = sum(work) / (sum(nt * ms for nt, ms in zip(nts, plain_ms)) / 1e3)
@@ -433,8 +444,8 @@ def run_batch(args):
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "batch64: 64 seeded source-free FP64 solves, a~U[0,0.99], m~U{1..4}, "
+        "dtype": "f64" if PRECISION == "fp64" else "f64+f32", "data": "synthetic",
+        "config": {"workload": f"batch64 ({PRECISION}): 64 seeded source-free solves, a~U[0,0.99], m~U{{1..4}}, "
                                "N_r~{2048,4096,8192,16384}, N_theta~{64,128,256}, x in [-100,300], T=500",
                    "points_per_batch_step": pts / args.steps, "l2": "working set > L2 (GBs)",
                    "parallelism": "replicas x1"},
@@ -461,7 +472,8 @@ def run_serve(args):
     import bh_ringdown_b200 as bhr
     from bh_ringdown_b200.workloads import serve_requests, with_arrivals
     torch.cuda.set_device(0)
-    reqs = serve_requests(args.requests, 1.0, time_scale=args.time_scale)
+    reqs = serve_requests(args.requests, 1.0, time_scale=args.time_scale,
+                          precision=bhr.BHR_MIXED if PRECISION == "mixed" else bhr.BHR_FP64)
     nts = [_solve_steps(r.params) for r in reqs]
     work = np.array([nt * r.points() for nt, r in zip(nts, reqs)], dtype=np.float64)
     budget = 150 << 30
@@ -471,7 +483,8 @@ def run_serve(args):
     with bhr.Engine(hbm_budget_bytes=budget) as e:
         for r in reqs[:ncal]:
             e.submit(r.params, r.traj)
-        e.step(0)
+        while e.stats()["queued"] > 0:
+            e.step(0)
         e.step(20)
         st0 = e.stats()
         t0 = time.perf_counter()
@@ -506,7 +519,8 @@ def run_serve(args):
                 while True:
                     running = e.step(args.chunk)
                     if running == 0:
-                        if not th.is_alive() and e.stats()["queued"] == 0:
+                        st_now = e.stats()
+                        if not th.is_alive() and st_now["queued"] == 0 and st_now["running"] == 0:
                             break
                         time.sleep(0.0005)
         finally:
@@ -529,7 +543,7 @@ def run_serve(args):
     service = []
     for r in reqs[:nplain]:
         t0 = time.perf_counter()
-        with bhr.Solver(r.params) as s:
+        with bhr.Solver(dataclasses.replace(r.params, precision=bhr.BHR_FP64)) as s:
             if r.traj is not None:
                 s.set_trajectory(r.traj)
             s.run()
@@ -549,8 +563,8 @@ def run_serve(args):
     out = {
         "metric": METRIC, "value": len(lat) / makespan, "unit": "solves/s", "n_gpus": 1,
         "steps": int(st["batch_steps"]), "warmup": 0, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"serve: {len(reqs)} seeded Poisson arrivals at {args.load:.0%} of measured capacity, "
+        "vs_baseline": None, "dtype": "f64" if PRECISION == "fp64" else "f64+f32", "data": "synthetic",
+        "config": {"workload": f"serve ({PRECISION}): {len(reqs)} seeded Poisson arrivals at {args.load:.0%} of measured capacity, "
                                f"70% source-free (N_r 2048/4096, N_theta 64-128), 30% plunge (8192x128); "
                                f"final times x{args.time_scale}", "hbm_budget_gb": budget / 2**30,
                    "chunk_steps": args.chunk, "arrival_rate_per_s": rate, "parallelism": "replicas x1"},
@@ -578,12 +592,16 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch64", "serve"], default="plunge")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
+                    help="fp64, or mixed: FP64 state and stage 1, FP32 corrections in stages 2 and 3")
     ap.add_argument("--requests", type=int, default=200, help="serve: requests in the stream")
     ap.add_argument("--time-scale", type=float, default=0.02, help="serve: factor on every request's final time")
     ap.add_argument("--load", type=float, default=0.8, help="serve: arrival rate / measured capacity")
     ap.add_argument("--chunk", type=int, default=64, help="serve: steps per engine call")
     ap.add_argument("--plain-requests", type=int, default=60, help="serve: requests timed on the plain path")
     args = ap.parse_args()
+    global PRECISION
+    PRECISION = args.precision
     if args.warmup < 3:
         args.warmup = 3
     rank, local_rank, world = env_rank()

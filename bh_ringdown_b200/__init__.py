@@ -369,11 +369,11 @@ class Engine:
         return {f[0]: getattr(st, f[0]) for f in _EngineStats._fields_}
 
     def run_all(self, chunk: int = 1 << 30) -> None:
-        """Steps until nothing is queued or running."""
+        """Steps until nothing is queued, running or being released."""
         while True:
             running = self.step(chunk)
             st = self.stats()
-            if running == 0 and st["queued"] == 0:
+            if running == 0 and st["queued"] == 0 and st["running"] == 0:
                 return
 
 

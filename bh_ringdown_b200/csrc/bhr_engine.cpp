@@ -9,15 +9,23 @@
 // step boundary (continuous batching); finished solves leave with their
 // waveform.  Each tile is computed by the same code as a lone solve, so a
 // request's result does not depend on what it shares the GPU with.
+//
+// Host work per request (grid, tables, initial data, trajectory records,
+// device allocations; waveform readback and release at the end) runs on a
+// worker thread with its own streams and stream-ordered allocations, so the
+// stepping thread only swaps prepared solves in and finished ones out.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "bhr.h"
@@ -62,7 +70,8 @@ double now_s() {
 // source records), estimated before creating it.
 size_t solve_bytes(const bhr_params &p, int traj_rows) {
   const size_t NM = static_cast<size_t>(p.N) * p.M;
-  size_t b = NM * 8 * (12 + 3);                                  // u0, u1, u2 (4 planes each), coefficient planes
+  size_t b = NM * 8 * (12 + 1);  // u0, u1, u2 (4 planes each), bb
+  if (p.precision == BHR_MIXED) b += NM * 4 * (4 + 4 + 4);  // delta1, eps2, FP32 coefficient planes
   b += static_cast<size_t>(CF_COUNT + 2) * p.N * 8 + static_cast<size_t>(RF_COUNT + 12) * p.M * 8;
   b += static_cast<size_t>(2) * p.PTSX * p.PTSY * 8;
   if (traj_rows > 0 && p.dt > 0) b += static_cast<size_t>(p.T / p.dt + 2) * sizeof(StepRec);
@@ -74,31 +83,46 @@ size_t solve_bytes(const bhr_params &p, int traj_rows) {
 
 struct bhr_engine {
   int device = 0;
-  size_t budget = 0, used = 0;
+  size_t budget = 0;
   int rows = 16;
   cudaStream_t stream = nullptr;
-  std::mutex qmu;  // the submission queue
+  // Requests and the worker (lock wmu): the queue, solves being prepared,
+  // prepared solves waiting to join, finished solves waiting to be
+  // released, and the bytes all of these and the running solves hold.
+  std::mutex wmu;
+  std::condition_variable wcv;   // worker: work arrived
+  std::condition_variable rcv;   // stepping thread: a prepared solve arrived
   std::deque<Request> queue;
+  std::unordered_set<int64_t> preparing;
+  std::vector<Running> ready;
+  std::vector<Running> to_release;
+  int releasing = 0;  // finished solves being read back and released
+  size_t used = 0;
   int64_t next_id = 1;
-  std::mutex mu;   // everything else
-  std::vector<Running> active;
+  bool stop = false;
+  std::thread worker;
+  // Results (lock dmu).
+  std::mutex dmu;
   std::unordered_map<int64_t, Finished> done;
-  // device work tables
+  int finished = 0;
+  // Stepping state (lock mu).
+  std::mutex mu;
+  std::vector<Running> active;
   BatchSolve *d_solves = nullptr;
   BatchTile *d_tiles = nullptr;
   ExtractArgs *d_ext = nullptr;
   SourceArgs *d_src = nullptr;
+  MixedBatch *d_mixed = nullptr;  // mixed-precision solves' stage 2/3 tables
   int cap_solves = 0, cap_tiles = 0, ntiles = 0, nsrc = 0, max_ptsx = 1, max_ptsy = 1;
+  int ntiles64 = 0;  // tiles of FP64 solves, first in the work-list; mixed solves' tiles follow
   int persist = 1;          // persistent stage kernels over the work-list
   int *d_err = nullptr;     // BHR_TIMEOUT from a bounded wait in a stage kernel
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool dirty = true;
-  // totals
   long long batch_steps = 0;
   double point_updates = 0.0;
   double device_ms = 0.0;
-  int finished = 0;
 };
 
 namespace {
@@ -111,14 +135,14 @@ int set_fail(int status, const std::string &msg) {
 void release_tables(bhr_engine *e) {
   if (e->graph) cudaGraphExecDestroy(e->graph);
   e->graph = nullptr;
-  if (e->d_solves) cudaFree(e->d_solves);
-  if (e->d_tiles) cudaFree(e->d_tiles);
-  if (e->d_ext) cudaFree(e->d_ext);
-  if (e->d_src) cudaFree(e->d_src);
+  for (void *q : {static_cast<void *>(e->d_solves), static_cast<void *>(e->d_tiles), static_cast<void *>(e->d_ext),
+                  static_cast<void *>(e->d_src), static_cast<void *>(e->d_mixed)})
+    if (q) cudaFreeAsync(q, e->stream);
   e->d_solves = nullptr;
   e->d_tiles = nullptr;
   e->d_ext = nullptr;
   e->d_src = nullptr;
+  e->d_mixed = nullptr;
   e->cap_solves = e->cap_tiles = 0;
 }
 
@@ -130,9 +154,15 @@ int enqueue_batch_step(bhr_engine *e) {
     cudaError_t err = launch_source_batch(e->d_src, e->nsrc, e->max_ptsy, e->max_ptsx, e->stream);
     if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("source batch: ") + cudaGetErrorString(err));
   }
+  // Stage 1 is FP64 for every solve; stages 2 and 3 run FP64 solves'
+  // tiles through the FP64 kernels and mixed solves' tiles through the
+  // FP32 ones.
   for (int stage = 1; stage <= 3; stage++) {
+    const int n64 = stage == 1 ? e->ntiles : e->ntiles64;
     cudaError_t err =
-        launch_stage_batch(stage, e->rows, e->persist, e->d_solves, e->d_tiles, e->ntiles, e->d_err, e->stream);
+        launch_stage_batch(stage, e->rows, e->persist, e->d_solves, e->d_tiles, n64, e->d_err, e->stream);
+    if (err == cudaSuccess && stage > 1 && e->ntiles > e->ntiles64)
+      err = launch_mixed_batch(stage, e->d_mixed, e->d_tiles + e->ntiles64, e->ntiles - e->ntiles64, e->stream);
     if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("stage batch: ") + cudaGetErrorString(err));
   }
   cudaError_t err = launch_extract_batch(e->d_ext, n, e->stream);
@@ -154,9 +184,10 @@ int rebuild(bhr_engine *e) {
     return BHR_OK;
   }
   std::vector<BatchSolve> solves(n);
-  std::vector<BatchTile> tiles;
+  std::vector<BatchTile> tiles, mtiles;
   std::vector<ExtractArgs> ext(n);
   std::vector<SourceArgs> src;
+  std::vector<MixedBatch> mixed;
   e->max_ptsx = 1;
   e->max_ptsy = 1;
   for (int i = 0; i < n; i++) {
@@ -170,8 +201,21 @@ int rebuild(bhr_engine *e) {
       B.args[k].un = s->u0;
       B.args[k].out = out[k];
     }
+    int mix_index = 0;
+    if (s->mixed) {
+      B.args[0].dout = s->d1f;
+      MixedBatch X{};
+      X.maps[0] = s->mmaps[0];
+      X.maps[1] = s->mmaps[1];
+      X.args[0] = X.args[1] = solver_mixed_args(s);
+      X.args[0].e_out = s->e2f;
+      X.args[1].u_out = s->u0;
+      mix_index = static_cast<int>(mixed.size());
+      mixed.push_back(X);
+    }
+    std::vector<BatchTile> &dst = s->mixed ? mtiles : tiles;
     for (int b0 = 0; b0 < s->p.M; b0 += e->rows)
-      for (int c0 = 0; c0 < s->p.N; c0 += TC) tiles.push_back({i, c0, b0, 0});
+      for (int c0 = 0; c0 < s->p.N; c0 += TC) dst.push_back({i, c0, b0, mix_index});
     ext[i] = solver_extract_args(s);
     if (s->has_source) {
       src.push_back(solver_source_args(s));
@@ -179,31 +223,37 @@ int rebuild(bhr_engine *e) {
       e->max_ptsy = std::max(e->max_ptsy, s->p.PTSY);
     }
   }
-  // Blocks are ordered solve by solve, row block by row block.
+  // Blocks are ordered solve by solve, row block by row block, FP64 solves
+  // first.
+  e->ntiles64 = static_cast<int>(tiles.size());
+  tiles.insert(tiles.end(), mtiles.begin(), mtiles.end());
   e->ntiles = static_cast<int>(tiles.size());
   e->nsrc = static_cast<int>(src.size());
   // The per-solve tables share one capacity; the work-list has its own.
   cudaError_t err = cudaSuccess;
   if (n > e->cap_solves) {
     const int c = std::max(n, 2 * e->cap_solves);
-    if (e->d_solves) cudaFree(e->d_solves);
-    if (e->d_ext) cudaFree(e->d_ext);
-    if (e->d_src) cudaFree(e->d_src);
+    if (e->d_solves) cudaFreeAsync(e->d_solves, e->stream);
+    if (e->d_ext) cudaFreeAsync(e->d_ext, e->stream);
+    if (e->d_src) cudaFreeAsync(e->d_src, e->stream);
+    if (e->d_mixed) cudaFreeAsync(e->d_mixed, e->stream);
     e->d_solves = nullptr;
     e->d_ext = nullptr;
     e->d_src = nullptr;
+    e->d_mixed = nullptr;
     e->cap_solves = 0;
-    if ((err = cudaMalloc(&e->d_solves, sizeof(BatchSolve) * c)) ||
-        (err = cudaMalloc(&e->d_ext, sizeof(ExtractArgs) * c)) || (err = cudaMalloc(&e->d_src, sizeof(SourceArgs) * c)))
+    if ((err = cudaMallocAsync(&e->d_solves, sizeof(BatchSolve) * c, e->stream)) ||
+        (err = cudaMallocAsync(&e->d_ext, sizeof(ExtractArgs) * c, e->stream)) || (err = cudaMallocAsync(&e->d_src, sizeof(SourceArgs) * c, e->stream)) ||
+        (err = cudaMallocAsync(&e->d_mixed, sizeof(MixedBatch) * c, e->stream)))
       return set_fail(BHR_OUT_OF_MEMORY, std::string("engine tables: ") + cudaGetErrorString(err));
     e->cap_solves = c;
   }
   if (e->ntiles > e->cap_tiles) {
     const int c = std::max(e->ntiles, 2 * e->cap_tiles);
-    if (e->d_tiles) cudaFree(e->d_tiles);
+    if (e->d_tiles) cudaFreeAsync(e->d_tiles, e->stream);
     e->d_tiles = nullptr;
     e->cap_tiles = 0;
-    if ((err = cudaMalloc(&e->d_tiles, sizeof(BatchTile) * c)))
+    if ((err = cudaMallocAsync(&e->d_tiles, sizeof(BatchTile) * c, e->stream)))
       return set_fail(BHR_OUT_OF_MEMORY, std::string("engine work-list: ") + cudaGetErrorString(err));
     e->cap_tiles = c;
   }
@@ -213,6 +263,8 @@ int rebuild(bhr_engine *e) {
       (err = cudaMemcpyAsync(e->d_ext, ext.data(), sizeof(ExtractArgs) * n, cudaMemcpyHostToDevice, e->stream)) ||
       (e->nsrc > 0 && (err = cudaMemcpyAsync(e->d_src, src.data(), sizeof(SourceArgs) * e->nsrc,
                                              cudaMemcpyHostToDevice, e->stream))) ||
+      (!mixed.empty() && (err = cudaMemcpyAsync(e->d_mixed, mixed.data(), sizeof(MixedBatch) * mixed.size(),
+                                                cudaMemcpyHostToDevice, e->stream))) ||
       (err = cudaStreamSynchronize(e->stream)))
     return set_fail(BHR_CUDA_ERROR, std::string("engine upload: ") + cudaGetErrorString(err));
   // Capture one batch step.
@@ -232,80 +284,139 @@ int rebuild(bhr_engine *e) {
   return BHR_OK;
 }
 
-void fail_request(bhr_engine *e, const Request &r, int status, const std::string &msg) {
+// Reads back a finished solve's waveform and releases it.
+Finished finish(bhr_solver *s, const Running &R) {
   Finished f;
-  f.state = 4;
-  f.status = status;
-  f.error = msg;
-  f.t_submit = r.t_submit;
-  f.t_start = f.t_finish = now_s();
-  e->done[r.id] = std::move(f);
+  f.t_submit = R.t_submit;
+  f.t_start = R.t_start;
+  f.steps = s->nt;
+  bhr_info inf{};
+  bhr_solver_info(s, &inf);
+  f.t.resize(inf.rows_done);
+  f.h.resize(static_cast<size_t>(inf.rows_done) * 14);
+  f.dedt.resize(inf.rows_done);
+  int nrows = 0;
+  f.status = bhr_solver_waveform(s, f.t.data(), f.h.data(), f.dedt.data(), inf.rows_done, &nrows);
+  if (f.status == BHR_OK) {
+    RunState rs{};
+    if (cudaMemcpy(&rs, s->rs, sizeof(rs), cudaMemcpyDeviceToHost) != cudaSuccess)
+      f.status = BHR_CUDA_ERROR;
+    else if (rs.err)
+      f.status = rs.err;
+  }
+  f.state = f.status == BHR_OK ? 3 : 4;
+  if (f.status != BHR_OK) f.error = bhr_last_error_string();
+  f.t_finish = now_s();
+  bhr_solver_destroy(s);
+  return f;
 }
 
-// Admits queued requests in arrival order while they fit the budget.
-int admit(bhr_engine *e) {
+// The worker: releases finished solves, then prepares queued requests in
+// arrival order while their estimated bytes fit the budget (one always
+// when nothing else holds memory).
+void worker_loop(bhr_engine *e) {
+  cudaSetDevice(e->device);
+  std::unique_lock<std::mutex> lock(e->wmu);
   for (;;) {
-    Request r;
-    {
-      std::lock_guard<std::mutex> lock(e->qmu);
-      if (e->queue.empty()) return BHR_OK;
-      const size_t need = solve_bytes(e->queue.front().p, static_cast<int>(e->queue.front().traj.size() / 10));
-      if (e->used + need > e->budget && !e->active.empty()) return BHR_OK;  // wait for memory
-      r = std::move(e->queue.front());
-      e->queue.pop_front();
+    auto fits = [&] {
+      if (e->queue.empty()) return false;
+      const Request &r = e->queue.front();
+      const size_t need = solve_bytes(r.p, static_cast<int>(r.traj.size() / 10));
+      const bool idle = e->used == 0;
+      return idle || e->used + need <= e->budget;
+    };
+    e->wcv.wait(lock, [&] { return e->stop || !e->to_release.empty() || fits(); });
+    if (e->stop) return;
+    if (!e->to_release.empty()) {
+      std::vector<Running> rel;
+      rel.swap(e->to_release);
+      e->releasing += static_cast<int>(rel.size());
+      lock.unlock();
+      for (Running &R : rel) {
+        const size_t bytes = R.s->bytes;
+        Finished f = finish(R.s, R);
+        {
+          std::lock_guard<std::mutex> dl(e->dmu);
+          e->done[R.id] = std::move(f);
+          e->finished++;
+        }
+        lock.lock();
+        e->used -= std::min(e->used, bytes);
+        e->releasing--;
+        e->rcv.notify_all();
+        lock.unlock();
+      }
+      lock.lock();
+      continue;
     }
+    Request r = std::move(e->queue.front());
+    e->queue.pop_front();
+    const size_t need = solve_bytes(r.p, static_cast<int>(r.traj.size() / 10));
+    e->used += need;
+    e->preparing.insert(r.id);
+    lock.unlock();
     r.p.device = e->device;
     bhr_solver *s = nullptr;
     int st = solver_create(&r.p, e->rows, &s);
     if (st == BHR_OK && !r.traj.empty())
       st = bhr_solver_set_trajectory(s, r.traj.data(), static_cast<int>(r.traj.size() / 10));
+    std::string msg;
     if (st != BHR_OK) {
-      const std::string msg = bhr_last_error_string();
+      msg = bhr_last_error_string();
       if (s) bhr_solver_destroy(s);
-      fail_request(e, r, st, msg);
-      continue;
+      s = nullptr;
+      Finished f;
+      f.state = 4;
+      f.status = st;
+      f.error = msg;
+      f.t_submit = r.t_submit;
+      f.t_start = f.t_finish = now_s();
+      std::lock_guard<std::mutex> dl(e->dmu);
+      e->done[r.id] = std::move(f);
     }
-    e->used += s->bytes;
-    e->active.push_back({r.id, s, r.t_submit, now_s(), s->nt - s->steps_done});
-    e->dirty = true;
+    lock.lock();
+    e->preparing.erase(r.id);
+    e->used -= std::min(e->used, need);
+    if (s) {
+      e->used += s->bytes;
+      e->ready.push_back({r.id, s, r.t_submit, now_s(), s->nt - s->steps_done});
+    }
+    e->rcv.notify_all();
   }
 }
 
-// Retires solves whose last step has run.
-int retire(bhr_engine *e) {
+// Moves prepared solves into the running set (mu held).  When none is
+// running but some are being prepared, waits a little for them.
+void join_ready(bhr_engine *e) {
+  std::unique_lock<std::mutex> lock(e->wmu);
+  if (e->active.empty() && e->ready.empty() &&
+      (!e->preparing.empty() || !e->queue.empty() || !e->to_release.empty() || e->releasing > 0))
+    e->rcv.wait_for(lock, std::chrono::milliseconds(200), [&] { return !e->ready.empty(); });
+  if (e->ready.empty()) return;
+  for (Running &R : e->ready) {
+    R.t_start = now_s();
+    e->active.push_back(R);
+  }
+  e->ready.clear();
+  e->dirty = true;
+}
+
+// Hands solves whose last step has run to the worker (mu held).
+void hand_off_finished(bhr_engine *e) {
+  std::vector<Running> fin;
   for (size_t i = 0; i < e->active.size();) {
-    Running &R = e->active[i];
-    if (R.remaining > 0) {
+    if (e->active[i].remaining > 0) {
       i++;
       continue;
     }
-    Finished f;
-    f.t_submit = R.t_submit;
-    f.t_start = R.t_start;
-    f.steps = R.s->nt;
-    bhr_info inf{};
-    bhr_solver_info(R.s, &inf);
-    f.t.resize(inf.rows_done);
-    f.h.resize(static_cast<size_t>(inf.rows_done) * 14);
-    f.dedt.resize(inf.rows_done);
-    int nrows = 0;
-    f.status = bhr_solver_waveform(R.s, f.t.data(), f.h.data(), f.dedt.data(), inf.rows_done, &nrows);
-    if (f.status == BHR_OK) {
-      RunState rs{};
-      cudaMemcpy(&rs, R.s->rs, sizeof(rs), cudaMemcpyDeviceToHost);
-      if (rs.err) f.status = rs.err;
-    }
-    f.state = f.status == BHR_OK ? 3 : 4;
-    if (f.status != BHR_OK) f.error = bhr_last_error_string();
-    f.t_finish = now_s();
-    e->used -= std::min(e->used, R.s->bytes);
-    bhr_solver_destroy(R.s);
-    e->done[R.id] = std::move(f);
-    e->finished++;
+    fin.push_back(e->active[i]);
     e->active.erase(e->active.begin() + static_cast<long>(i));
     e->dirty = true;
   }
-  return BHR_OK;
+  if (fin.empty()) return;
+  std::lock_guard<std::mutex> lock(e->wmu);
+  e->to_release.insert(e->to_release.end(), fin.begin(), fin.end());
+  e->wcv.notify_all();
 }
 
 }  // namespace
@@ -325,6 +436,7 @@ int bhr_engine_create(int device, size_t hbm_budget_bytes, bhr_engine **out) {
   e->device = device;
   e->budget = hbm_budget_bytes;
   if (cudaSetDevice(device) != cudaSuccess || prepare_kernels() != cudaSuccess ||
+      prepare_mixed_kernels() != cudaSuccess ||
       cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&e->ev0) != cudaSuccess || cudaEventCreate(&e->ev1) != cudaSuccess ||
       cudaMalloc(&e->d_err, sizeof(int)) != cudaSuccess || cudaMemset(e->d_err, 0, sizeof(int)) != cudaSuccess) {
@@ -333,18 +445,28 @@ int bhr_engine_create(int device, size_t hbm_budget_bytes, bhr_engine **out) {
   }
   // BHR_ENGINE_TILING=block selects the one-tile-per-block stage kernels.
   if (const char *v = std::getenv("BHR_ENGINE_TILING")) e->persist = std::strcmp(v, "block") != 0;
+  e->worker = std::thread(worker_loop, e);
   *out = e;
   return BHR_OK;
 }
 
 void bhr_engine_destroy(bhr_engine *e) {
   if (!e) return;
+  {
+    std::lock_guard<std::mutex> lock(e->wmu);
+    e->stop = true;
+    e->wcv.notify_all();
+  }
+  if (e->worker.joinable()) e->worker.join();
   std::lock_guard<std::mutex> lock(e->mu);
   cudaSetDevice(e->device);
   cudaStreamSynchronize(e->stream);
   for (auto &R : e->active) bhr_solver_destroy(R.s);
+  for (auto &R : e->ready) bhr_solver_destroy(R.s);
+  for (auto &R : e->to_release) bhr_solver_destroy(R.s);
   e->active.clear();
   release_tables(e);
+  cudaStreamSynchronize(e->stream);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
   if (e->d_err) cudaFree(e->d_err);
@@ -358,10 +480,11 @@ int bhr_engine_submit(bhr_engine *e, const bhr_params *p, const double *traj_row
   r.p = *p;
   if (traj_rows) r.traj.assign(traj_rows, traj_rows + static_cast<size_t>(nrows) * 10);
   r.t_submit = now_s();
-  std::lock_guard<std::mutex> lock(e->qmu);
+  std::lock_guard<std::mutex> lock(e->wmu);
   r.id = e->next_id++;
   *id = r.id;
   e->queue.push_back(std::move(r));
+  e->wcv.notify_all();
   return BHR_OK;
 }
 
@@ -369,7 +492,7 @@ int bhr_engine_step(bhr_engine *e, int max_steps, int *running) {
   if (!e || max_steps < 0) return set_fail(BHR_INVALID_ARG, "bad step arguments");
   std::lock_guard<std::mutex> lock(e->mu);
   if (cudaSetDevice(e->device) != cudaSuccess) return set_fail(BHR_CUDA_ERROR, "cudaSetDevice failed");
-  if (int st = admit(e)) return st;
+  join_ready(e);
   if (e->dirty)
     if (int st = rebuild(e)) return st;
   int n = max_steps;
@@ -394,8 +517,12 @@ int bhr_engine_step(bhr_engine *e, int max_steps, int *running) {
     e->batch_steps += n;
     e->point_updates += pts * n;
   }
-  if (int st = retire(e)) return st;
-  if (running) *running = static_cast<int>(e->active.size());
+  hand_off_finished(e);
+  if (running) {
+    std::lock_guard<std::mutex> wl(e->wmu);
+    *running = static_cast<int>(e->active.size() + e->ready.size() + e->preparing.size() + e->to_release.size() +
+                                e->releasing);
+  }
   return BHR_OK;
 }
 
@@ -403,26 +530,51 @@ int bhr_engine_poll(bhr_engine *e, int64_t id, bhr_request_info *info) {
   if (!e || !info) return set_fail(BHR_INVALID_ARG, "bad poll arguments");
   std::memset(info, 0, sizeof(*info));
   {
-    std::lock_guard<std::mutex> lock(e->qmu);
+    std::lock_guard<std::mutex> lock(e->wmu);
     for (auto &r : e->queue)
       if (r.id == id) {
         info->state = 1;
         info->submit_s = r.t_submit;
         return BHR_OK;
       }
-  }
-  std::lock_guard<std::mutex> lock(e->mu);
-  for (auto &R : e->active)
-    if (R.id == id) {
-      info->state = 2;
-      info->steps_total = R.s->nt;
-      info->steps_done = R.s->steps_done;
-      info->submit_s = R.t_submit;
-      info->start_s = R.t_start;
+    if (e->preparing.count(id)) {
+      info->state = 1;
       return BHR_OK;
     }
+    for (auto &R : e->ready)
+      if (R.id == id) {
+        info->state = 2;
+        info->steps_total = R.s->nt;
+        info->submit_s = R.t_submit;
+        return BHR_OK;
+      }
+  }
+  {
+    std::lock_guard<std::mutex> lock(e->mu);
+    for (auto &R : e->active)
+      if (R.id == id) {
+        info->state = 2;
+        info->steps_total = R.s->nt;
+        info->steps_done = R.s->steps_done;
+        info->submit_s = R.t_submit;
+        info->start_s = R.t_start;
+        return BHR_OK;
+      }
+  }
+  std::lock_guard<std::mutex> lock(e->dmu);
   auto it = e->done.find(id);
-  if (it == e->done.end()) return BHR_OK;  // unknown: state 0
+  if (it == e->done.end()) {
+    // finished but not yet released by the worker: still reported running
+    std::lock_guard<std::mutex> wl(e->wmu);
+    for (auto &R : e->to_release)
+      if (R.id == id) {
+        info->state = 2;
+        info->steps_total = info->steps_done = R.s->nt;
+        info->submit_s = R.t_submit;
+        info->start_s = R.t_start;
+      }
+    return BHR_OK;
+  }
   const Finished &f = it->second;
   info->state = f.state;
   info->status = f.status;
@@ -436,7 +588,7 @@ int bhr_engine_poll(bhr_engine *e, int64_t id, bhr_request_info *info) {
 
 int bhr_engine_result(bhr_engine *e, int64_t id, double *t, double *h, double *dedt, int max_rows, int *nrows) {
   if (!e) return set_fail(BHR_INVALID_ARG, "null engine");
-  std::lock_guard<std::mutex> lock(e->mu);
+  std::lock_guard<std::mutex> lock(e->dmu);
   auto it = e->done.find(id);
   if (it == e->done.end()) return set_fail(BHR_INVALID_ARG, "request not finished");
   const Finished &f = it->second;
@@ -453,16 +605,20 @@ int bhr_engine_stats(bhr_engine *e, bhr_engine_counters *st) {
   if (!e || !st) return set_fail(BHR_INVALID_ARG, "bad stats arguments");
   std::memset(st, 0, sizeof(*st));
   {
-    std::lock_guard<std::mutex> lock(e->qmu);
-    st->queued = static_cast<int>(e->queue.size());
+    std::lock_guard<std::mutex> lock(e->wmu);
+    st->queued = static_cast<int>(e->queue.size() + e->preparing.size());
+    st->running = static_cast<int>(e->ready.size() + e->to_release.size() + e->releasing);
+    st->bytes_in_use = e->used;
+  }
+  {
+    std::lock_guard<std::mutex> lock(e->dmu);
+    st->finished = e->finished;
   }
   std::lock_guard<std::mutex> lock(e->mu);
-  st->running = static_cast<int>(e->active.size());
-  st->finished = e->finished;
+  st->running += static_cast<int>(e->active.size());
   st->batch_steps = e->batch_steps;
   st->point_updates = e->point_updates;
   st->device_ms = e->device_ms;
-  st->bytes_in_use = e->used;
   st->budget = e->budget;
   st->tiles = e->ntiles;
   return BHR_OK;

@@ -216,9 +216,9 @@ void make_dedt_weights(const bhr_params &p, const Grid &g, std::vector<double> &
   }
 }
 
-void apply_closure_host(double *planes, int N, int M, bool even_m) {
+void apply_closure_host(double *planes, int N, int M, bool even_m, int nplanes) {
   const size_t NM = static_cast<size_t>(N) * M;
-  for (int f = 0; f < 4; f++) {
+  for (int f = 0; f < nplanes; f++) {
     double *P = planes + f * NM;
     for (int a = 3; a < N - 3; a++) {
       auto at = [&](int b) -> double & { return P[static_cast<size_t>(b) * N + a]; };
@@ -248,18 +248,19 @@ void apply_closure_host(double *planes, int N, int M, bool even_m) {
 // Initial data: zero (HighOrder/kern.cu:164-167) or the Gaussian pulse
 // psi = exp(-(x-c)^2/(2w^2)) swsh(l, m, theta), Pi = 0, closed by the
 // boundary extrapolation so every stored state satisfies the closure.
-void make_initial_data(const bhr_params &p, const Grid &g, std::vector<double> &planes) {
+void make_initial_data(const bhr_params &p, const Grid &g, std::vector<double> &qre) {
   const size_t NM = static_cast<size_t>(p.N) * p.M;
-  planes.assign(4 * NM, 0.0);
+  qre.clear();
   if (p.init_kind != BHR_INIT_GAUSSIAN) return;
+  qre.assign(NM, 0.0);
   for (int b = 0; b < p.M; b++) {
     const double y = swsh(p.init_ell, p.m, g.theta[b]);
     for (int a = 0; a < p.N; a++) {
       const double x = g.x_c[a] - p.init_center;
-      planes[static_cast<size_t>(b) * p.N + a] = std::exp(-x * x / (2.0 * p.init_width * p.init_width)) * y;
+      qre[static_cast<size_t>(b) * p.N + a] = std::exp(-x * x / (2.0 * p.init_width * p.init_width)) * y;
     }
   }
-  apply_closure_host(planes.data(), p.N, p.M, (static_cast<int>(p.m) % 2) == 0);
+  apply_closure_host(qre.data(), p.N, p.M, (static_cast<int>(p.m) % 2) == 0, 1);
 }
 
 }  // namespace bhr

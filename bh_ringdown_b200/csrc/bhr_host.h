@@ -35,10 +35,11 @@ double swsh(double ell, double ml, double the);
 void make_projection_weights(const bhr_params &p, const Grid &g, std::vector<double> &w7);
 // Weights of dE/dt = sum_b |int psi|^2 * E[b] (HighOrder/body.cu:174-184).
 void make_dedt_weights(const bhr_params &p, const Grid &g, std::vector<double> &e);
-// Closed initial data planes (q_re, q_im, p_re, p_im) for init_kind.
-void make_initial_data(const bhr_params &p, const Grid &g, std::vector<double> &planes);
-// Reference closure (kernel_boundary2a then 2b) applied on host planes.
-void apply_closure_host(double *planes, int N, int M, bool even_m);
+// Closed initial q_re plane for init_kind (empty for zero data; q_im, p_re
+// and p_im start at zero in both cases).
+void make_initial_data(const bhr_params &p, const Grid &g, std::vector<double> &qre);
+// Reference closure (kernel_boundary2a then 2b) applied on nplanes host planes.
+void apply_closure_host(double *planes, int N, int M, bool even_m, int nplanes = 4);
 
 void set_error(const std::string &msg);
 

@@ -69,6 +69,7 @@ struct StageArgs {
   int even_m;
   int rows;             // tile height: 8 or 16 theta rows
   int persist;          // 1: 16-row tiles walked by one persistent block per SM
+  float *dout;          // mixed precision, stage 1: delta1 = dt L(u^n) in FP32, or nullptr
   double dt, cx, cy, cyy, cko;
 };
 
@@ -103,6 +104,42 @@ struct StageMaps {
   CUtensorMap q, p, u, coef_bb, colf, rowf;
   CUtensorMap o;  // stage output planes, box {TC, rows, 4} (TMA stores)
 };
+
+// Mixed precision (BHR_MIXED): SSP-RK3 rearranged so that FP32 carries only
+// O(dt^2) corrections.  With delta1 = dt L(u^n) (L with the source) and L0
+// the homogeneous operator,
+//   u1      = u^n + delta1                       (FP64, the FP64 stage 1)
+//   eps2    = dt/4 L0(delta1)                    (FP32 stage 2)
+//   u^{n+1} = u1 + 2 eps2 + (2/3) dt L0(eps2)    (FP32 stage 3, FP64 sum)
+// which is the Shu-Osher scheme exactly in exact arithmetic (L is affine).
+struct MixedMaps {
+  CUtensorMap q, p;     // FP32 input planes (delta1 or eps2), halo boxes
+  CUtensorMap bb;       // FP32 planes bb, ee, d_re, d_im (tile box)
+  CUtensorMap colf, rowf;  // FP32 column / row factor tables
+  CUtensorMap u1;       // stage 3: FP64 u1 planes, tile box
+};
+struct MixedArgs {
+  float *e_out;         // stage 2: eps2 planes
+  double *u_out;        // stage 3: u^{n+1} planes
+  int *err;
+  int N, M, even_m;
+  float dt, cx, cy, cyy, cko;
+};
+struct MixedBatch {
+  MixedMaps maps[2];    // stages 2 and 3
+  MixedArgs args[2];
+};
+cudaError_t encode_mixed_maps(const float *in, const float *bbf, const float *colf, const float *rowf,
+                              const double *u1, int N, int M, MixedMaps *maps);
+cudaError_t launch_mixed_stage(int stage, const MixedMaps &maps, const MixedArgs &a, cudaStream_t st);
+struct BatchTile;
+cudaError_t launch_mixed_batch(int stage, const MixedBatch *solves, const BatchTile *tiles, int ntiles,
+                               cudaStream_t st);
+cudaError_t launch_to_float(const double *src, float *dst, size_t n, cudaStream_t st);
+// kc[4][M][N] (FP32): bb, ee, d_re, d_im formed in FP64 from the tables.
+cudaError_t launch_mixed_coef(const double *coltab, const double *rowtab, const double *bbt, float *kc, int N, int M,
+                              double cx, cudaStream_t st);
+cudaError_t prepare_mixed_kernels();
 
 // A batch of solves advanced together: per solve, the tensor maps and
 // arguments of its three stages; per block, one (solve, tile) work item.

@@ -19,11 +19,13 @@
 // 3 <= a < N-3 are stored; the boundary rows and columns of every stage are
 // the reference's extrapolation closure of the interior and are rebuilt by
 // whoever reads them.
+#include "bhr_device.cuh"
 #include "bhr_internal.h"
 
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <type_traits>
 #include <utility>
 
@@ -31,132 +33,36 @@ namespace bhr {
 
 namespace {
 
-constexpr double kThird = 0.33333333333333333;   // HighOrder/kern.cu:46
-constexpr double kPie = 3.141592653589793;       // HighOrder/kern.cu:1188
-constexpr long long kMaxWaitIters = 1LL << 22;   // bounded mbarrier wait
-
-// ---- PTX helpers ---------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void fence_barrier_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t phase) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(phase)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase) {
-  for (long long i = 0; i < kMaxWaitIters; i++)
-    if (mbar_try_wait(bar, phase)) return true;
-  return false;
-}
-// Programmatic dependent launch: wait for the kernels this one depends on
-// (their writes become visible), and let the next kernel start launching.
-__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-
-// 3D tiled TMA load, no multicast.
-__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-      : "memory");
-}
-
-// 3D tiled TMA store from shared memory, tracked by this thread's bulk group.
-__device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, const void *src, int x, int y, int z) {
-  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
-                   reinterpret_cast<uint64_t>(map)),
-               "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
-               : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// The bulk stores of this thread have finished reading shared memory.
-__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-// The bulk stores of this thread are complete.
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void named_barrier_sync(int id, int threads) {
-  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
-}
-
-// ---- stencils (HighOrder/kern.cu:192-261) ---------------------------------
-__device__ __forceinline__ double d1c(const double *v, int c) {
-  return 45.0 * (v[c + 1] - v[c - 1]) - 9.0 * (v[c + 2] - v[c - 2]) + (v[c + 3] - v[c - 3]);
-}
-__device__ __forceinline__ double ko8c(const double *v, int c) {
-  return (v[c + 4] + v[c - 4]) - 8.0 * (v[c + 3] + v[c - 3]) + 28.0 * (v[c + 2] + v[c - 2]) -
-         56.0 * (v[c + 1] + v[c - 1]) + 70.0 * v[c];
-}
-
-// Reciprocal by Newton-Raphson iteration y <- y (2 - x y) from the hardware
-// approximation (two steps take its ~2^-22 relative error below 1 ulp).
-__device__ __forceinline__ double rcp_nr(double x) {
-  double y;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-  double e = fma(-x, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-x, y, 1.0);
-  return fma(y, e, y);
-}
-
-// Square root of x >= 0: Newton-Raphson for 1/sqrt(x), y <- y (3/2 - x y^2 / 2),
-// from the hardware approximation, then one correction of s = x y by the
-// residual x - s^2.
-__device__ __forceinline__ double sqrt_nr(double x) {
-  double y;
-  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-  y = y * fma(-0.5 * x * y, y, 1.5);
-  y = y * fma(-0.5 * x * y, y, 1.5);
-  double s = x * y;
-  s = fma(fma(-s, s, x), 0.5 * y, s);
-  return x > 0.0 ? s : 0.0;
-}
-
+// Constants, PTX helpers, stencils: bhr_device.cuh.
 
 // Shared memory of one tile of ROWS theta rows (8 or 16).
 template <int ROWS>
 struct __align__(128) StageSmem {
-  double q[2][ROWS + 6][WC];    // TMA box {WC, ROWS+6, 2}: planes q_re, q_im with halo
-  double p[2][ROWS][WC];        // TMA box {WC, ROWS, 2}: planes p_re, p_im with column halo
-  double bb[ROWS][WC];          // TMA box {WC, ROWS, 1}: bb on the window columns
-  double cf[CF_COUNT][TC];      // TMA box {TC, CF_COUNT}: column factors of the tile columns
-  double un[4][ROWS][TC];       // TMA box {TC, ROWS, 4}: u^n (stages 2 and 3)
-  double rf[RF_COUNT][ROWS];    // TMA box {ROWS, RF_COUNT}: row factors of the tile rows
+  // Every TMA destination (and TMA store source) starts on a 128-byte boundary.
+  alignas(128) double q[2][ROWS + 6][WC];    // TMA box {WC, ROWS+6, 2}: planes q_re, q_im with halo
+  alignas(128) double p[2][ROWS][WC];        // TMA box {WC, ROWS, 2}: planes p_re, p_im with column halo
+  alignas(128) double bb[ROWS][WC];          // TMA box {WC, ROWS, 1}: bb on the window columns
+  alignas(128) double cf[CF_COUNT][TC];      // TMA box {TC, CF_COUNT}: column factors of the tile columns
+  alignas(128) double un[4][ROWS][TC];       // TMA box {TC, ROWS, 4}: u^n (stages 2 and 3)
+  alignas(128) double rf[RF_COUNT][ROWS];    // TMA box {ROWS, RF_COUNT}: row factors of the tile rows
   uint64_t bar;
   int src_c0, src_r0;           // source patch corner of this step
   int done;                     // persistent kernels: warps done with this buffer's tile
   int issued;                   // persistent kernels: load phases issued into this buffer
   int abort;                    // persistent kernels (buffer 0): a bounded wait gave up
 };
-
-// 1/bir = 1/(B0 + B1 sin^2 theta) (HighOrder/kern.cu:132-149).
-__device__ __forceinline__ double inv_bir(double b0, double b1, double s2) { return rcp_nr(fma(b1, s2, b0)); }
+#define BHR_TMA_ALIGNED(T, m) static_assert(offsetof(T, m) % 128 == 0, "TMA destination " #m " not 128-byte aligned")
+BHR_TMA_ALIGNED(StageSmem<8>, p);
+BHR_TMA_ALIGNED(StageSmem<8>, bb);
+BHR_TMA_ALIGNED(StageSmem<8>, cf);
+BHR_TMA_ALIGNED(StageSmem<8>, un);
+BHR_TMA_ALIGNED(StageSmem<8>, rf);
+BHR_TMA_ALIGNED(StageSmem<16>, p);
+BHR_TMA_ALIGNED(StageSmem<16>, bb);
+BHR_TMA_ALIGNED(StageSmem<16>, cf);
+BHR_TMA_ALIGNED(StageSmem<16>, un);
+BHR_TMA_ALIGNED(StageSmem<16>, rf);
+static_assert(sizeof(StageSmem<16>) % 128 == 0, "persistent buffers must stay 128-byte aligned");
 
 // The time-independent per-point coefficient bb (HighOrder/kern.cu:141-147),
 // which the stage kernels need on a stencil window, for the interior rows,
@@ -437,6 +343,16 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
       if (STAGE == 1) {
         o[0] = fc[pl][0] + dt * res[pl][0];
         o[1] = fc[pl][1] + dt * res[pl][1];
+        if (A.dout != nullptr) {  // mixed precision: delta1 in FP32
+          const float d0 = static_cast<float>(dt * res[pl][0]), d1 = static_cast<float>(dt * res[pl][1]);
+          float *fd = A.dout + pl * NM + base;
+          if (both) {
+            *reinterpret_cast<float2 *>(fd) = make_float2(d0, d1);
+          } else {
+            if (a0 >= 3 && a0 < N - 3) fd[0] = d0;
+            if (a0 + 1 >= 3 && a0 + 1 < N - 3) fd[1] = d1;
+          }
+        }
       } else {
         const double2 u = *reinterpret_cast<const double2 *>(&S.un[pl][r][2 * tx]);
         if (STAGE == 2) {
@@ -1011,24 +927,6 @@ cudaError_t encode_state_maps(void *planes, int N, int M, int rows, CUtensorMap 
   return (r1 == CUDA_SUCCESS && r2 == CUDA_SUCCESS && r3 == CUDA_SUCCESS) ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-// Launch with programmatic stream serialisation allowed: the kernel may
-// begin while its predecessor on the stream drains, and holds every read
-// of the predecessor's results behind grid_dependency_wait().
-template <class... KArgs, class... Args>
-static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                              Args &&...args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
-}
 
 template <int ROWS>
 static cudaError_t launch_rows(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st) {

@@ -66,8 +66,8 @@ int validate(const bhr_params &p) {
     set_error("PTSX in [1,1024], PTSY >= 1");
     return BHR_INVALID_ARG;
   }
-  if (p.precision != BHR_FP64 || p.integrator != BHR_SSPRK3) {
-    set_error("only FP64 SSP-RK3 is built in this library");
+  if ((p.precision != BHR_FP64 && p.precision != BHR_MIXED) || p.integrator != BHR_SSPRK3) {
+    set_error("precision must be BHR_FP64 or BHR_MIXED and the integrator BHR_SSPRK3");
     return BHR_INVALID_ARG;
   }
   return BHR_OK;
@@ -76,9 +76,12 @@ int validate(const bhr_params &p) {
 template <class T>
 int dalloc(bhr_solver *s, T **ptr, size_t count) {
   const size_t nbytes = sizeof(T) * (count ? count : 1);
-  cudaError_t e = cudaMalloc(reinterpret_cast<void **>(ptr), nbytes);
+  // Stream-ordered allocation from the device's pool: neither this nor the
+  // matching cudaFreeAsync synchronizes the device, so solves can be
+  // created and destroyed while others are stepping.
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(ptr), nbytes, s->stream);
   if (e != cudaSuccess) {
-    set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    set_error(std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
     return e == cudaErrorMemoryAllocation ? BHR_OUT_OF_MEMORY : BHR_CUDA_ERROR;
   }
   s->bytes += nbytes;
@@ -86,14 +89,34 @@ int dalloc(bhr_solver *s, T **ptr, size_t count) {
 }
 
 void free_all(bhr_solver *s) {
-  void *ptrs[] = {s->u0, s->u1, s->u2, s->coltab, s->rowtab, s->ctab, s->rc, s->th, s->src, s->ext,
-                  s->integ, s->wproj, s->wdedt, s->rows, s->recs, s->rs};
+  void *ptrs[] = {s->u0,    s->u1,   s->u2,     s->coltab, s->rowtab, s->ctab,   s->rc,     s->th,
+                  s->src,   s->ext,  s->integ,  s->wproj,  s->wdedt,  s->rows,   s->recs,   s->rs,
+                  s->d1f,   s->e2f,  s->colf32, s->rowf32, s->bbf};
   for (void *q : ptrs)
-    if (q) cudaFree(q);
+    if (q) cudaFreeAsync(q, s->stream);
   if (s->g1) cudaGraphExecDestroy(s->g1);
   if (s->gb) cudaGraphExecDestroy(s->gb);
   s->g1 = s->gb = nullptr;
-  if (s->stream) cudaStreamDestroy(s->stream);
+  if (s->stream) {
+    cudaStreamSynchronize(s->stream);
+    cudaStreamDestroy(s->stream);
+  }
+}
+
+// The device's default memory pool keeps freed blocks for reuse instead of
+// returning them to the driver at each synchronization (once per device
+// per process).
+int keep_pool_memory(int device) {
+  static std::mutex mu;
+  static bool done[64] = {false};
+  std::lock_guard<std::mutex> lock(mu);
+  if (device < 0 || device >= 64 || done[device]) return 0;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) return 1;
+  uint64_t keep = UINT64_MAX;
+  if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) return 1;
+  done[device] = true;
+  return 0;
 }
 
 // Kerr tortoise coordinate as the source placement uses it
@@ -202,7 +225,7 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
 
   const size_t NM = static_cast<size_t>(p.N) * p.M;
   int st = BHR_OK;
-  if (cudaSetDevice(p.device) != cudaSuccess || prepare_kernels() != cudaSuccess ||
+  if (cudaSetDevice(p.device) != cudaSuccess || prepare_kernels() != cudaSuccess || keep_pool_memory(p.device) ||
       cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
     set_error("cannot set device / create stream");
     delete s;
@@ -230,7 +253,8 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
   if ((e = up(s->coltab, coltab.data(), coltab.size() * 8)) || (e = up(s->rowtab, rowtab.data(), rowtab.size() * 8)) ||
       (e = up(s->rc, g.r_c.data(), g.r_c.size() * 8)) || (e = up(s->th, g.theta.data(), g.theta.size() * 8)) ||
       (e = up(s->wproj, w7.data(), w7.size() * 8)) || (e = up(s->wdedt, we.data(), we.size() * 8)) ||
-      (e = up(s->u0, init.data(), init.size() * 8)) ||
+      (e = cudaMemsetAsync(s->u0, 0, 4 * NM * 8, s->stream)) ||
+      (!init.empty() && (e = up(s->u0, init.data(), init.size() * 8))) ||
       (e = launch_coef_tables(s->coltab, s->rowtab, s->ctab, p.N, p.M, s->stream)) ||
       (e = cudaMemsetAsync(s->u1, 0, 4 * NM * 8, s->stream)) || (e = cudaMemsetAsync(s->u2, 0, 4 * NM * 8, s->stream)) ||
       (e = cudaMemsetAsync(s->integ, 0, 4 * p.M * 8, s->stream)) || (e = cudaMemsetAsync(s->ext, 0, 2 * p.M * 8, s->stream)) ||
@@ -251,6 +275,31 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
         tile_rows = 16;
         s->persist = 1;
       }
+    }
+  }
+  if (p.precision == BHR_MIXED) {
+    s->mixed = true;
+    const size_t nc = static_cast<size_t>(CF_COUNT) * p.N, nr = static_cast<size_t>(RF_COUNT) * p.M;
+    cudaError_t e2 = cudaSuccess;
+    if ((st = dalloc(s, &s->d1f, 4 * NM)) || (st = dalloc(s, &s->e2f, 4 * NM)) || (st = dalloc(s, &s->colf32, nc)) ||
+        (st = dalloc(s, &s->rowf32, nr)) || (st = dalloc(s, &s->bbf, 4 * NM))) {
+      free_all(s);
+      delete s;
+      return st;
+    }
+    if ((e2 = prepare_mixed_kernels()) || (e2 = launch_to_float(s->coltab, s->colf32, nc, s->stream)) ||
+        (e2 = launch_to_float(s->rowtab, s->rowf32, nr, s->stream)) ||
+        (e2 = launch_mixed_coef(s->coltab, s->rowtab, s->ctab, s->bbf, p.N, p.M, 0.016666666666667 / g.dx,
+                                s->stream)) ||
+        (e2 = cudaMemsetAsync(s->d1f, 0, 4 * NM * sizeof(float), s->stream)) ||
+        (e2 = cudaMemsetAsync(s->e2f, 0, 4 * NM * sizeof(float), s->stream)) ||
+        (e2 = encode_mixed_maps(s->d1f, s->bbf, s->colf32, s->rowf32, nullptr, p.N, p.M, &s->mmaps[0])) ||
+        (e2 = encode_mixed_maps(s->e2f, s->bbf, s->colf32, s->rowf32, s->u1, p.N, p.M, &s->mmaps[1])) ||
+        (e2 = cudaStreamSynchronize(s->stream))) {
+      set_error(std::string("mixed-precision set-up: ") + cudaGetErrorString(e2));
+      free_all(s);
+      delete s;
+      return BHR_CUDA_ERROR;
     }
   }
   if (int st = (tile_rows == 8 || tile_rows == 16) ? encode_maps(s, tile_rows) : autotune_rows(s)) {
@@ -399,7 +448,7 @@ int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows) {
     return bad_status.load();
   }
   cudaSetDevice(p.device);
-  if (s->recs) cudaFree(s->recs), s->bytes -= sizeof(StepRec) * static_cast<size_t>(s->nt ? s->nt : 1);
+  if (s->recs) cudaFreeAsync(s->recs, s->stream), s->bytes -= sizeof(StepRec) * static_cast<size_t>(s->nt ? s->nt : 1);
   s->recs = nullptr;
   if (int st = dalloc(s, &s->recs, static_cast<size_t>(s->nt))) return st;
   BHR_CUDA_TRY(cudaMemcpyAsync(s->recs, recs.data(), sizeof(StepRec) * recs.size(), cudaMemcpyHostToDevice, s->stream));
@@ -532,6 +581,21 @@ StageArgs bhr::solver_stage_args(bhr_solver *s) {
   return A;
 }
 
+MixedArgs bhr::solver_mixed_args(bhr_solver *s) {
+  const StageArgs A = solver_stage_args(s);
+  MixedArgs X{};
+  X.err = A.err;
+  X.N = A.N;
+  X.M = A.M;
+  X.even_m = A.even_m;
+  X.dt = static_cast<float>(A.dt);
+  X.cx = static_cast<float>(A.cx);
+  X.cy = static_cast<float>(A.cy);
+  X.cyy = static_cast<float>(A.cyy);
+  X.cko = static_cast<float>(A.cko);
+  return X;
+}
+
 SourceArgs bhr::solver_source_args(bhr_solver *s) {
   const bhr_params &p = s->p;
   SourceArgs S{};
@@ -580,6 +644,23 @@ static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
   if (s->has_source) BHR_CUDA_TRY(launch_source(solver_source_args(s), s->stream));
   BHR_CUDA_TRY(mark(1));
   A.vin = s->u0; A.un = s->u0; A.out = s->u1;
+  if (s->mixed) {
+    // u1 in FP64 and delta1 in FP32, then the FP32 stages 2 and 3.
+    A.dout = s->d1f;
+    BHR_CUDA_TRY(launch_stage(1, s->maps[0], A, s->stream));
+    BHR_CUDA_TRY(mark(2));
+    MixedArgs X = solver_mixed_args(s);
+    X.e_out = s->e2f;
+    BHR_CUDA_TRY(launch_mixed_stage(2, s->mmaps[0], X, s->stream));
+    BHR_CUDA_TRY(mark(3));
+    X.e_out = nullptr;
+    X.u_out = s->u0;
+    BHR_CUDA_TRY(launch_mixed_stage(3, s->mmaps[1], X, s->stream));
+    BHR_CUDA_TRY(mark(4));
+    BHR_CUDA_TRY(launch_extract(solver_extract_args(s), s->stream));
+    BHR_CUDA_TRY(mark(5));
+    return BHR_OK;
+  }
   BHR_CUDA_TRY(launch_stage(1, s->maps[0], A, s->stream));
   BHR_CUDA_TRY(mark(2));
   A.vin = s->u1; A.un = s->u0; A.out = s->u2;

@@ -17,6 +17,10 @@ struct bhr_solver {
   double *u0 = nullptr, *u1 = nullptr, *u2 = nullptr;
   double *coltab = nullptr, *rowtab = nullptr, *ctab = nullptr, *rc = nullptr, *th = nullptr;
   double *src = nullptr, *ext = nullptr, *integ = nullptr, *wproj = nullptr, *wdedt = nullptr, *rows = nullptr;
+  // mixed precision (BHR_MIXED): FP32 delta1 and eps2 planes, FP32 tables
+  bool mixed = false;
+  float *d1f = nullptr, *e2f = nullptr, *colf32 = nullptr, *rowf32 = nullptr, *bbf = nullptr;
+  bhr::MixedMaps mmaps[2];  // stages 2 and 3
   bhr::StepRec *recs = nullptr;
   bhr::RunState *rs = nullptr;
   size_t bytes = 0;
@@ -38,4 +42,5 @@ int solver_create(const bhr_params *p, int tile_rows, bhr_solver **out);
 StageArgs solver_stage_args(bhr_solver *s);
 SourceArgs solver_source_args(bhr_solver *s);
 ExtractArgs solver_extract_args(bhr_solver *s);
+MixedArgs solver_mixed_args(bhr_solver *s);
 }  // namespace bhr

@@ -23,7 +23,7 @@ from typing import List, Optional
 
 import numpy as np
 
-from . import BHR_INIT_GAUSSIAN, Params
+from . import BHR_FP64, BHR_INIT_GAUSSIAN, Params
 from .trajectory import synthetic_plunge
 
 SEED = 20261203
@@ -40,15 +40,16 @@ class Request:
         return self.params.N * self.params.M
 
 
-def _free(rng, N, M, a, m, T, Xmin=-100.0, Xmax=300.0, x_ext=250.0):
+def _free(rng, N, M, a, m, T, Xmin=-100.0, Xmax=300.0, x_ext=250.0, precision=BHR_FP64):
     c, w = rng.uniform(10.0, 40.0), rng.uniform(1.0, 4.0)
     dx = (Xmax - Xmin) / N
     return Params(N=int(N), M=int(M), Xmin=Xmin, Xmax=Xmax, a=float(a), m=float(m), dt=0.0, courant=0.25,
                   out_every=0.5, Fr=0, T=T, out_start=0.0, ext_col=int(round((x_ext - Xmin) / dx)),
-                  init_kind=BHR_INIT_GAUSSIAN, init_center=c, init_width=w, init_ell=float(max(2, abs(m))))
+                  init_kind=BHR_INIT_GAUSSIAN, init_center=c, init_width=w, init_ell=float(max(2, abs(m))),
+                  precision=precision)
 
 
-def batch_requests(n: int = 64, seed: int = SEED, T: float = 500.0) -> List[Request]:
+def batch_requests(n: int = 64, seed: int = SEED, T: float = 500.0, precision: int = BHR_FP64) -> List[Request]:
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(n):
@@ -56,16 +57,17 @@ def batch_requests(n: int = 64, seed: int = SEED, T: float = 500.0) -> List[Requ
         m = int(rng.integers(1, 5))
         N = int(rng.choice([2048, 4096, 8192, 16384]))
         M = int(rng.choice([64, 128, 256]))
-        out.append(Request(_free(rng, N, M, a, m, T), None))
+        out.append(Request(_free(rng, N, M, a, m, T, precision=precision), None))
     return out
 
 
 def plunge_params(a: float, T: float, N: int = 8192, M: int = 128, Xmin: float = -200.0, Xmax: float = 600.0,
-                  x_ext: float = 500.0) -> Params:
+                  x_ext: float = 500.0, precision: int = BHR_FP64) -> Params:
     """Plunge-driven solve; dt = 0.25 min(dx, r_min dtheta) as the waveform
     rows are every Fr = 50 steps."""
     from . import grid
-    prm = Params(N=N, M=M, Xmin=Xmin, Xmax=Xmax, a=a, m=2.0, dt=0.0, courant=0.25, Fr=50, T=T, out_start=0.0)
+    prm = Params(N=N, M=M, Xmin=Xmin, Xmax=Xmax, a=a, m=2.0, dt=0.0, courant=0.25, Fr=50, T=T, out_start=0.0,
+                 precision=precision)
     _, r, _ = grid(prm)
     dx = (Xmax - Xmin) / N
     prm.dt = 0.25 * min(dx, r[0] * np.pi / M)
@@ -74,7 +76,7 @@ def plunge_params(a: float, T: float, N: int = 8192, M: int = 128, Xmin: float =
 
 
 def serve_requests(n: int = 2000, rate_per_s: float = 1.0, seed: int = SEED, time_scale: float = 1.0,
-                   plunge_fraction: float = 0.3) -> List[Request]:
+                   plunge_fraction: float = 0.3, precision: int = BHR_FP64) -> List[Request]:
     """n requests with exponential inter-arrival times of mean 1/rate_per_s."""
     rng = np.random.default_rng(seed)
     t = 0.0
@@ -84,7 +86,7 @@ def serve_requests(n: int = 2000, rate_per_s: float = 1.0, seed: int = SEED, tim
         t += rng.exponential(1.0 / rate_per_s)
         if rng.uniform() < plunge_fraction:
             a = max(1e-8, round(float(rng.uniform(0.0, 0.95)), 2))  # trajectories shared per 0.01 in a
-            prm = plunge_params(a, 1000.0 * time_scale)
+            prm = plunge_params(a, 1000.0 * time_scale, precision=precision)
             key = (a, prm.dt)
             if key not in trajs:
                 trajs[key] = synthetic_plunge(a, prm.dt / 2.0, duration=prm.T)
@@ -94,7 +96,7 @@ def serve_requests(n: int = 2000, rate_per_s: float = 1.0, seed: int = SEED, tim
             m = int(rng.integers(1, 5))
             N = int(rng.choice([2048, 4096]))
             M = int(rng.choice([64, 80, 96, 112, 128]))
-            out.append(Request(_free(rng, N, M, a, m, 500.0 * time_scale), None, t, "free"))
+            out.append(Request(_free(rng, N, M, a, m, 500.0 * time_scale, precision=precision), None, t, "free"))
     return out
 
 

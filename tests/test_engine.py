@@ -82,7 +82,9 @@ def test_request_joining_mid_run_is_bit_identical():
         e.step(40)
         assert e.poll(first)["state"] == bhr.Engine.RUNNING
         late = e.submit(*reqs[2])
-        assert e.poll(late)["state"] == bhr.Engine.QUEUED
+        assert e.poll(late)["state"] in (bhr.Engine.QUEUED, bhr.Engine.RUNNING)
+        while e.poll(late)["state"] != bhr.Engine.RUNNING:  # prepared off the stepping thread
+            e.step(0)
         e.step(10)
         info = e.poll(late)
         assert info["state"] == bhr.Engine.RUNNING and info["steps_done"] == 10
@@ -107,6 +109,32 @@ def test_membership_growing_one_by_one():
         for rid, (t0, h0, d0) in zip(ids, alone):
             t, h, d = e.result(rid)
             assert np.array_equal(t, t0) and np.array_equal(h, h0) and np.array_equal(d, d0)
+
+
+def test_mixed_precision_requests_in_a_mixed_batch():
+    """FP32-corrected (BHR_MIXED) and FP64 requests side by side: each
+    result bit-identical to the same request alone in an engine, and the
+    mixed ones within the FP64 bar of a lone mixed-precision solver."""
+    reqs = requests()
+    for k in (1, 2):
+        reqs[k][0].precision = bhr.BHR_MIXED
+    alone = [run_alone(p, t) for p, t in reqs]
+    with bhr.Engine() as e:
+        ids = [e.submit(p, t) for p, t in reqs]
+        e.run_all()
+        for rid, (t0, h0, d0) in zip(ids, alone):
+            t, h, d = e.result(rid)
+            assert np.array_equal(t, t0) and np.array_equal(h, h0) and np.array_equal(d, d0)
+    for k in (1, 2):
+        prm, traj = reqs[k]
+        with bhr.Solver(prm) as s:
+            if traj is not None:
+                s.set_trajectory(traj)
+            s.run()
+            ts, hs, _ = s.waveform()
+        t, h, _ = alone[k]
+        assert np.array_equal(t, ts)
+        assert np.linalg.norm(h - hs) <= WAVE_TOL * np.linalg.norm(hs)
 
 
 def test_engine_matches_lone_solver():
