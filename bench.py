@@ -30,6 +30,8 @@ import time
 
 import numpy as np
 
+from bh_ringdown_b200 import replicas
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -221,9 +223,7 @@ def run_ours(args, rank, local_rank, world):
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = replicas.max_over_ranks(total_ms, dist, device="cuda")
     clocks = clk.summary()
     solver.close()
 
@@ -400,6 +400,16 @@ def _solve_steps(prm):
     return int(prm.T / dt)
 
 
+def _dist_init(world, local_rank):
+    """Process group for the replica bookkeeping (N > 1), else None."""
+    if world <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
 def run_batch(args):
     """Batched form: 64 seeded source-free solves of mixed size resident on
     one GPU, advanced together by the engine (one launch per RK stage over
@@ -413,11 +423,18 @@ def run_batch(args):
     import torch
     import bh_ringdown_b200 as bhr
     from bh_ringdown_b200.workloads import batch_requests
-    torch.cuda.set_device(0)
-    reqs = batch_requests(64, precision=bhr.BHR_MIXED if PRECISION == "mixed" else bhr.BHR_FP64)
+    rank, local_rank, world = env_rank()
+    torch.cuda.set_device(local_rank)
+    dist = _dist_init(world, local_rank)
+    all_reqs = batch_requests(64, precision=bhr.BHR_MIXED if PRECISION == "mixed" else bhr.BHR_FP64)
+    # replicas: this rank's share of the 64 solves (work-balanced, no collective on the data path)
+    mine = replicas.run_shard(all_reqs, rank, world, lambda r: replicas.request_work(r.params))
+    reqs = [all_reqs[i] for i in mine]
+    for r in reqs:
+        r.params.device = local_rank
     nts = [_solve_steps(r.params) for r in reqs]
     work = [nt * r.points() for nt, r in zip(nts, reqs)]
-    with bhr.Engine(hbm_budget_bytes=150 << 30) as e:
+    with bhr.Engine(device=local_rank, hbm_budget_bytes=150 << 30) as e:
         for r in reqs:
             e.submit(r.params, r.traj)
         while e.stats()["queued"] > 0:  # requests are prepared off the stepping thread
@@ -425,13 +442,15 @@ def run_batch(args):
         e.step(args.warmup)
         st0 = e.stats()
         assert st0["running"] == len(reqs), st0
+        if dist is not None:
+            dist.barrier()
         t0 = time.perf_counter()
-        with ClockSampler(0) as clk:
+        with ClockSampler(local_rank) as clk:
             e.step(args.steps)
-        wall = time.perf_counter() - t0
+        wall = replicas.max_over_ranks(time.perf_counter() - t0, dist, device="cuda")
         st1 = e.stats()
-    dev_ms = st1["device_ms"] - st0["device_ms"]
-    pts = st1["point_updates"] - st0["point_updates"]
+    dev_ms = replicas.max_over_ranks(st1["device_ms"] - st0["device_ms"], dist, device="cuda")
+    pts = sum(replicas.gather_objects(st1["point_updates"] - st0["point_updates"], dist))
     value = pts / (dev_ms / 1e3)
     # one at a time, each solve alone
     plain_ms = []
@@ -439,16 +458,23 @@ def run_batch(args):
         with bhr.Solver(dataclasses.replace(r.params, precision=bhr.BHR_FP64)) as s:
             s.time_steps(args.warmup)
             plain_ms.append(s.time_steps(args.steps) / args.steps)
-    plain_value = sum(work) / (sum(nt * ms for nt, ms in zip(nts, plain_ms)) / 1e3)
-    mean_work = float(np.mean(work))
+    # each GPU runs its share one solve at a time; the job takes the slowest share
+    plain_s = replicas.max_over_ranks(sum(nt * ms for nt, ms in zip(nts, plain_ms)) / 1e3, dist, device="cuda")
+    all_work = [w for ws in replicas.gather_objects(work, dist) for w in ws]
+    plain_value = sum(all_work) / plain_s
+    mean_work = float(np.mean(all_work))
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     out = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if PRECISION == "fp64" else "f64+f32", "data": "synthetic",
         "config": {"workload": f"batch64 ({PRECISION}): 64 seeded source-free solves, a~U[0,0.99], m~U{{1..4}}, "
                                "N_r~{2048,4096,8192,16384}, N_theta~{64,128,256}, x in [-100,300], T=500",
                    "points_per_batch_step": pts / args.steps, "l2": "working set > L2 (GBs)",
-                   "parallelism": "replicas x1"},
+                   "parallelism": f"replicas x{world} (solves sharded by work)"},
         "solves_per_s": value / mean_work, "plain_value": plain_value, "plain_solves_per_s": plain_value / mean_work,
         "speedup_vs_plain": value / plain_value,
         "e2e": {"value": pts / wall, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
@@ -456,6 +482,8 @@ def run_batch(args):
         "gpu_launches": args.steps * 4, "clocks": clk.summary(),
     }
     print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def run_serve(args):
@@ -471,7 +499,9 @@ def run_serve(args):
     import torch
     import bh_ringdown_b200 as bhr
     from bh_ringdown_b200.workloads import serve_requests, with_arrivals
-    torch.cuda.set_device(0)
+    rank, local_rank, world = env_rank()
+    torch.cuda.set_device(local_rank)
+    dist = _dist_init(world, local_rank)
     reqs = serve_requests(args.requests, 1.0, time_scale=args.time_scale,
                           precision=bhr.BHR_MIXED if PRECISION == "mixed" else bhr.BHR_FP64)
     nts = [_solve_steps(r.params) for r in reqs]
@@ -480,7 +510,7 @@ def run_serve(args):
 
     # capacity: a saturated engine on the first requests, device throughput
     ncal = min(len(reqs), 48)
-    with bhr.Engine(hbm_budget_bytes=budget) as e:
+    with bhr.Engine(device=local_rank, hbm_budget_bytes=budget) as e:
         for r in reqs[:ncal]:
             e.submit(r.params, r.traj)
         while e.stats()["queued"] > 0:
@@ -492,13 +522,23 @@ def run_serve(args):
             e.step(50)
         st1 = e.stats()
     cal_rate = (st1["point_updates"] - st0["point_updates"]) / ((st1["device_ms"] - st0["device_ms"]) / 1e3)
-    capacity = cal_rate / float(np.mean(work))
-    rate = args.load * capacity
+    # per-GPU capacity (the slowest GPU's when several serve), the stream's
+    # rate is `load` times all GPUs' capacity
+    capacity = -replicas.max_over_ranks(-cal_rate / float(np.mean(work)), dist, device="cuda")
+    rate = args.load * capacity * world
     with_arrivals(reqs, rate)
+    all_reqs = reqs
+    # replicas: each GPU serves its share of the stream (work-balanced), one engine per GPU
+    reqs = [all_reqs[i] for i in replicas.run_shard(all_reqs, rank, world,
+                                                    lambda r: replicas.request_work(r.params))]
+    for r in reqs:
+        r.params.device = local_rank
 
     # the stream through the engine
-    with bhr.Engine(hbm_budget_bytes=budget) as e:
+    with bhr.Engine(device=local_rank, hbm_budget_bytes=budget) as e:
         ids = [None] * len(reqs)
+        if dist is not None:
+            dist.barrier()
         start = time.perf_counter()
 
         stop = threading.Event()
@@ -515,7 +555,7 @@ def run_serve(args):
         th = threading.Thread(target=submitter)
         th.start()
         try:
-            with ClockSampler(0) as clk:
+            with ClockSampler(local_rank) as clk:
                 while True:
                     running = e.step(args.chunk)
                     if running == 0:
@@ -527,7 +567,7 @@ def run_serve(args):
             # the engine must outlive the submitting thread
             stop.set()
             th.join()
-        makespan = time.perf_counter() - start
+        makespan = replicas.max_over_ranks(time.perf_counter() - start, dist, device="cuda")
         lat, fails = [], 0
         for rid in ids:
             info = e.poll(rid)
@@ -536,10 +576,13 @@ def run_serve(args):
                 continue
             lat.append(info["finish_s"] - info["submit_s"])
         st = e.stats()
-    lat = np.array(lat)
+    lat = np.array([x for part in replicas.gather_objects(lat, dist) for x in part])
+    fails = sum(replicas.gather_objects(fails, dist))
+    dev_pts = sum(replicas.gather_objects(st["point_updates"], dist))
+    dev_ms = replicas.max_over_ranks(st["device_ms"], dist, device="cuda")
 
-    # the plain path: the same requests one at a time through bhr_solver
-    nplain = min(len(reqs), args.plain_requests)
+    # the plain path: the same requests one at a time through bhr_solver (one per GPU)
+    nplain = min(len(reqs), max(1, args.plain_requests // world))
     service = []
     for r in reqs[:nplain]:
         t0 = time.perf_counter()
@@ -557,20 +600,26 @@ def run_serve(args):
     for r, sv in zip(reqs, svc):
         fin = max(fin, r.arrival_s) + sv
         plat.append(fin - r.arrival_s)
-    plat = np.array(plat)
-    plain_capacity = 1.0 / float(np.mean(service))
-    engine_capacity = capacity
+    plat = np.array([x for part in replicas.gather_objects(list(plat), dist) for x in part])
+    service = np.array([x for part in replicas.gather_objects(list(service), dist) for x in part])
+    plain_capacity = world / float(np.mean(service))
+    engine_capacity = capacity * world
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     out = {
-        "metric": METRIC, "value": len(lat) / makespan, "unit": "solves/s", "n_gpus": 1,
+        "metric": METRIC, "value": len(lat) / makespan, "unit": "solves/s", "n_gpus": world,
         "steps": int(st["batch_steps"]), "warmup": 0, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if PRECISION == "fp64" else "f64+f32", "data": "synthetic",
-        "config": {"workload": f"serve ({PRECISION}): {len(reqs)} seeded Poisson arrivals at {args.load:.0%} of measured capacity, "
+        "config": {"workload": f"serve ({PRECISION}): {len(all_reqs)} seeded Poisson arrivals at {args.load:.0%} of measured capacity, "
                                f"70% source-free (N_r 2048/4096, N_theta 64-128), 30% plunge (8192x128); "
                                f"final times x{args.time_scale}", "hbm_budget_gb": budget / 2**30,
-                   "chunk_steps": args.chunk, "arrival_rate_per_s": rate, "parallelism": "replicas x1"},
+                   "chunk_steps": args.chunk, "arrival_rate_per_s": rate,
+                   "parallelism": f"replicas x{world} (requests sharded by work, one engine per GPU)"},
         "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)), "failed": fails,
         "capacity_solves_per_s": engine_capacity,
-        "device_pt_updates_per_s": st["point_updates"] / (st["device_ms"] / 1e3),
+        "device_pt_updates_per_s": dev_pts / (dev_ms / 1e3),
         "plain": {"capacity_solves_per_s": plain_capacity, "p50_s": float(np.percentile(plat, 50)),
                   "p99_s": float(np.percentile(plat, 99)), "measured_requests": nplain,
                   "note": "bhr_solver one request at a time, wall-clock service times, FCFS queue"},
@@ -580,6 +629,8 @@ def run_serve(args):
         "clocks": clk.summary(),
     }
     print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def main():
@@ -606,8 +657,7 @@ def main():
         args.warmup = 3
     rank, local_rank, world = env_rank()
     if args.workload in ("batch64", "serve"):
-        if rank == 0:
-            (run_batch if args.workload == "batch64" else run_serve)(args)
+        (run_batch if args.workload == "batch64" else run_serve)(args)
         return
     global WORKLOAD
     WORKLOAD = WORKLOADS[args.workload]
