@@ -454,6 +454,11 @@ int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows) {
   BHR_CUDA_TRY(cudaMemcpyAsync(s->recs, recs.data(), sizeof(StepRec) * recs.size(), cudaMemcpyHostToDevice, s->stream));
   BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
   s->has_source = true;
+  // The launch arguments now carry the source and the new records: step
+  // graphs captured before (steps taken without a trajectory) are rebuilt.
+  if (s->g1) cudaGraphExecDestroy(s->g1);
+  if (s->gb) cudaGraphExecDestroy(s->gb);
+  s->g1 = s->gb = nullptr;
   return BHR_OK;
 }
 

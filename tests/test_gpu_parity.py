@@ -176,3 +176,22 @@ def test_every_stage_tiling_matches_oracle(tiling, monkeypatch):
     assert np.array_equal(ts, t)
     assert rel_field_err(s.get_state(), o.get_state()) <= FIELD_TOL
     assert np.linalg.norm(hs - h) <= WAVE_TOL * np.linalg.norm(h)
+
+
+@pytest.mark.parametrize("tiling", ["block16", "persistent"])
+def test_trajectory_set_after_stepping(tiling, monkeypatch):
+    """A step taken before the trajectory is set captures the step graph
+    without a source; setting the trajectory must rebuild what was captured.
+    The turn-on window (1 - exp(-t/25))^4 is zero at t = 0, so one step
+    without the source equals the oracle's first sourced step."""
+    monkeypatch.setenv("BHR_STAGE_TILING", tiling)
+    s, o, rows, coef = traj_pair(256, 32, -50.0, 50.0, 0.6, 2.0, ext_col=154)
+    s2 = bhr.Solver(s.params)
+    s2.step(1)
+    s2.set_trajectory(rows)
+    n = 80
+    s2.step(n - 1)
+    o.run(traj=rows, coef_fn=coef, nsteps=n)
+    assert rel_field_err(s2.get_state(), o.get_state()) <= FIELD_TOL
+    s2.close()
+    s.close()
