@@ -69,6 +69,7 @@ struct StageArgs {
   int even_m;
   int rows;             // tile height: 8 or 16 theta rows
   int persist;          // 1: 16-row tiles walked by one persistent block per SM
+  int narrow;           // 1: 8-row tiles on 128-thread blocks (four per SM)
   float *dout;          // mixed precision, stage 1: delta1 = dt L(u^n) in FP32, or nullptr
   double dt, cx, cy, cyy, cko;
 };

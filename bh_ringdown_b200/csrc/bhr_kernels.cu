@@ -382,7 +382,7 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
 }
 
 // One tile per block (grid N/64 x M/ROWS, two blocks per SM).
-template <int STAGE, int ROWS>
+template <int STAGE, int ROWS, int THREADS = STAGE_THREADS>
 __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &A, const int c0, const int b0) {
   extern __shared__ unsigned char smem_raw[];
   StageSmem<ROWS> &S = *reinterpret_cast<StageSmem<ROWS> *>(
@@ -407,15 +407,24 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
     mbar_wait_bounded(&S.bar, 0);
     return;
   }
-  tile_close<ROWS, STAGE_THREADS>(S, A, c0, b0, tid);
+  tile_close<ROWS, THREADS>(S, A, c0, b0, tid);
   __syncthreads();
-  tile_compute<STAGE, ROWS, STAGE_THREADS, false>(S, A, c0, b0, tx, ty);
+  tile_compute<STAGE, ROWS, THREADS, false>(S, A, c0, b0, tx, ty);
 }
 
 template <int STAGE, int ROWS>
 __global__ void __launch_bounds__(STAGE_THREADS, 2)
     stage_kernel(const __grid_constant__ StageMaps T, const StageArgs A) {
   stage_tile<STAGE, ROWS>(T, A, blockIdx.x * TC, blockIdx.y * ROWS);
+}
+
+// 8-row tiles on 128-thread blocks: four blocks (16 warps) per SM, so four
+// tiles' loads and computations interleave instead of two.
+constexpr int kNarrowThreads = 128;
+template <int STAGE>
+__global__ void __launch_bounds__(kNarrowThreads, 4)
+    stage_narrow_kernel(const __grid_constant__ StageMaps T, const StageArgs A) {
+  stage_tile<STAGE, 8, kNarrowThreads>(T, A, blockIdx.x * TC, blockIdx.y * 8);
 }
 
 // Several solves advanced together: block -> (solve, tile) from the work-list.
@@ -953,6 +962,13 @@ static int sm_count() {
 static size_t persist_smem_bytes() { return 2 * sizeof(StageSmem<kPersistRows>) + 128; }
 
 cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st) {
+  if (a.narrow) {
+    const size_t smem = sizeof(StageSmem<8>) + 128;
+    const dim3 grid(a.N / TC, a.M / 8), block(32, kNarrowThreads / 32);
+    if (stage == 1) return launch_pdl(stage_narrow_kernel<1>, grid, block, smem, st, maps, a);
+    if (stage == 2) return launch_pdl(stage_narrow_kernel<2>, grid, block, smem, st, maps, a);
+    return launch_pdl(stage_narrow_kernel<3>, grid, block, smem, st, maps, a);
+  }
   if (a.persist) {
     const int ntiles = (a.N / TC) * (a.M / kPersistRows);
     const dim3 grid(std::min(ntiles, sm_count())), block(32, kPersistThreads / 32);
@@ -980,6 +996,10 @@ cudaError_t prepare_kernels() {
       (e = cudaFuncSetAttribute(stage_batch_kernel<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)) ||
       (e = cudaFuncSetAttribute(stage_batch_kernel<2, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)) ||
       (e = cudaFuncSetAttribute(stage_batch_kernel<3, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)))
+    return e;
+  if ((e = cudaFuncSetAttribute(stage_narrow_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
+      (e = cudaFuncSetAttribute(stage_narrow_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
+      (e = cudaFuncSetAttribute(stage_narrow_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)))
     return e;
   const int sp = static_cast<int>(persist_smem_bytes());
   if ((e = cudaFuncSetAttribute(stage_persistent_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp)) ||

@@ -275,6 +275,10 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
         tile_rows = 16;
         s->persist = 1;
       }
+      if (!std::strcmp(v, "block8n")) {
+        tile_rows = 8;
+        s->narrow = 1;
+      }
     }
   }
   if (p.precision == BHR_MIXED) {
@@ -508,29 +512,31 @@ static int encode_maps(bhr_solver *s, int rows) {
 
 
 // Stage tiling autotuner: per (device, N, M) the stage kernels are timed
-// with 8- and 16-row tiles one per block and with the persistent 16-row
-// kernels, on stages 1 and 2 (which write only the solve's scratch stages
+// with 8- and 16-row tiles one per 256-thread block, 8-row tiles on
+// 128-thread blocks, and the persistent 16-row kernels, on stages 1 and 2 (which write only the solve's scratch stages
 // u1, u2); the fastest is kept for the process.
 static int autotune_rows(bhr_solver *s) {
   static std::mutex mu;
-  static std::vector<std::array<int, 5>> cache;  // device, N, M, rows, persist
+  static std::vector<std::array<int, 6>> cache;  // device, N, M, rows, persist, narrow
   const bhr_params &p = s->p;
   {
     std::lock_guard<std::mutex> lock(mu);
     for (auto &c : cache)
       if (c[0] == p.device && c[1] == p.N && c[2] == p.M) {
         s->persist = c[4];
+        s->narrow = c[5];
         return encode_maps(s, c[3]);
       }
   }
-  static const int cands[3][2] = {{8, 0}, {16, 0}, {16, 1}};
+  static const int cands[4][3] = {{8, 0, 0}, {16, 0, 0}, {16, 1, 0}, {8, 0, 1}};  // rows, persist, narrow
   double best_ms = 1e30;
   int best = 1;
   cudaEvent_t e0, e1;
   BHR_CUDA_TRY(cudaEventCreate(&e0));
   BHR_CUDA_TRY(cudaEventCreate(&e1));
-  for (int c = 0; c < 3; c++) {
+  for (int c = 0; c < 4; c++) {
     s->persist = cands[c][1];
+    s->narrow = cands[c][2];
     if (int st = encode_maps(s, cands[c][0])) return st;
     StageArgs A = solver_stage_args(s);
     A.src = nullptr;
@@ -554,9 +560,10 @@ static int autotune_rows(bhr_solver *s) {
   cudaEventDestroy(e1);
   {
     std::lock_guard<std::mutex> lock(mu);
-    cache.push_back({p.device, p.N, p.M, cands[best][0], cands[best][1]});
+    cache.push_back({p.device, p.N, p.M, cands[best][0], cands[best][1], cands[best][2]});
   }
   s->persist = cands[best][1];
+  s->narrow = cands[best][2];
   return encode_maps(s, cands[best][0]);
 }
 
@@ -578,6 +585,7 @@ StageArgs bhr::solver_stage_args(bhr_solver *s) {
   A.even_m = s->even_m ? 1 : 0;
   A.rows = s->tile_rows;
   A.persist = s->persist;
+  A.narrow = s->narrow;
   A.dt = p.dt;
   A.cx = 0.016666666666667 * odx;
   A.cy = 0.05 * third * odth;

@@ -27,6 +27,7 @@ struct bhr_solver {
   bhr::StageMaps maps[3];  // per stage input state (u^n, u1, u2)
   int tile_rows = 16; // stage tile height chosen for this grid
   int persist = 0;     // 1: persistent stage kernels (16-row tiles, one block per SM)
+  int narrow = 0;      // 1: 8-row tiles on 128-thread blocks (four per SM)
   int steps_done = 0;
   // Captured step graphs: one step, and kGraphBatch steps in one launch.
   cudaGraphExec_t g1 = nullptr, gb = nullptr;

@@ -158,7 +158,7 @@ def test_headline_workload_grid_matches_oracle():
     assert rel_field_err(s.get_state(), o.get_state()) <= FIELD_TOL
 
 
-@pytest.mark.parametrize("tiling", ["block8", "block16", "persistent"])
+@pytest.mark.parametrize("tiling", ["block8", "block16", "persistent", "block8n"])
 def test_every_stage_tiling_matches_oracle(tiling, monkeypatch):
     """Each stage tiling (8- and 16-row tiles one per block, persistent
     blocks walking 16-row tiles through two buffers) on a sourced plunge
@@ -168,7 +168,7 @@ def test_every_stage_tiling_matches_oracle(tiling, monkeypatch):
     s, o, rows, coef = traj_pair(1024, 64, -50.0, 50.0, 0.7, 2.0, ext_col=640)
     info = s.info()
     assert info["persistent"] == (tiling == "persistent")
-    assert info["tile_rows"] == (8 if tiling == "block8" else 16)
+    assert info["tile_rows"] == (8 if tiling in ("block8", "block8n") else 16)
     n = 120
     s.step(n)
     t, h, dedt, steps, _, _ = o.run(traj=rows, coef_fn=coef, nsteps=n)
