@@ -73,7 +73,7 @@ size_t solve_bytes(const bhr_params &p, int traj_rows) {
   size_t b = NM * 8 * (12 + 1);  // u0, u1, u2 (4 planes each), bb
   if (p.precision == BHR_MIXED) b += NM * 4 * (4 + 4 + 4);  // delta1, eps2, FP32 coefficient planes
   b += static_cast<size_t>(CF_COUNT + 2) * p.N * 8 + static_cast<size_t>(RF_COUNT + 12) * p.M * 8;
-  b += static_cast<size_t>(2) * p.PTSX * p.PTSY * 8;
+  b += static_cast<size_t>(4) * p.PTSX * p.PTSY * 8;  // two source patch buffers
   if (traj_rows > 0 && p.dt > 0) b += static_cast<size_t>(p.T / p.dt + 2) * sizeof(StepRec);
   if (p.dt > 0 && p.Fr > 0) b += static_cast<size_t>(p.T / p.dt / p.Fr + 2) * 16 * 8;
   return b + (1 << 20);

@@ -61,7 +61,7 @@ struct StageArgs {
   double *out;          // output planes
   const double *coltab; // [CF_COUNT][N]
   const double *rowtab; // [RF_COUNT][M]
-  const double *src;    // source patch [2][PTSY][PTSX] or nullptr
+  const double *src;    // source patch buffers [2][2][PTSY][PTSX] (step k: buffer k % 2) or nullptr
   const StepRec *recs;  // per-step records or nullptr
   const RunState *rs;
   int *err;
@@ -75,12 +75,14 @@ struct StageArgs {
 };
 
 struct SourceArgs {
-  double *src;          // [2][PTSY][PTSX]
+  double *src;          // two patch buffers [2][2][PTSY][PTSX]: step k's patch in buffer k % 2
   const StepRec *recs;
   const RunState *rs;
   const double *r_c;    // [N]
   const double *theta;  // [M]
   int N, M, PTSX, PTSY;
+  int lookahead;        // the patch built is for step rs->k + lookahead (0 or 1)
+  int nrecs;            // steps with a record; later steps are skipped
   double a, mass, m, wt;
 };
 

@@ -47,6 +47,7 @@ struct __align__(128) StageSmem {
   alignas(128) double rf[RF_COUNT][ROWS];    // TMA box {ROWS, RF_COUNT}: row factors of the tile rows
   uint64_t bar;
   int src_c0, src_r0;           // source patch corner of this step
+  int src_buf;                  // source patch buffer of this step (k % 2)
   int done;                     // persistent kernels: warps done with this buffer's tile
   int issued;                   // persistent kernels: load phases issued into this buffer
   int abort;                    // persistent kernels (buffer 0): a bounded wait gave up
@@ -102,17 +103,17 @@ __device__ __forceinline__ void tile_issue_setup(StageSmem<ROWS> &S, const Stage
   tma_load_2d(&S.rf[0][0], &T.rowf, b0, 0, &S.bar);
 }
 
-// Thread 0, before arming the tile's barrier (so the barrier publishes it):
-// this step's source patch corner.  The step counter is final when any
-// stage kernel starts: its predecessor (the source kernel of a sourced
-// step, or a stage kernel) starts its dependents only after its own grid
-// dependency on the previous step's extraction was satisfied.
+// Thread 0, after the grid dependency (the step counter is written by the
+// previous step's extraction): this step's source patch corner and buffer.
+// A block barrier publishes it to the other warps.
 template <int ROWS>
 __device__ __forceinline__ void tile_note_source(StageSmem<ROWS> &S, const StageArgs &A) {
   if (A.src != nullptr) {
-    const StepRec &rec = A.recs[A.rs->k];
+    const int k = A.rs->k;
+    const StepRec &rec = A.recs[k];
     S.src_c0 = rec.col0;
     S.src_r0 = rec.row0;
+    S.src_buf = k & 1;
   }
 }
 
@@ -198,9 +199,11 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
   const bool lo_cols = (c0 == 0), hi_cols = (c0 + TC + 4 > N - 3);
   int src_c0 = 0, src_r0 = 0;
   bool tile_src = false;
+  const double *srcp = A.src;
   if (A.src != nullptr) {
     src_c0 = S.src_c0;
     src_r0 = S.src_r0;
+    srcp = A.src + static_cast<size_t>(S.src_buf) * 2 * A.PTSX * A.PTSY;
     tile_src = (src_c0 < c0 + TC) && (src_c0 + A.PTSX > c0) && (src_r0 < b0 + ROWS) && (src_r0 + A.PTSY > b0);
   }
 
@@ -282,8 +285,8 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
       if (tile_src) {
         const int sc = a - src_c0, sr = b - src_r0;
         if (sc >= 0 && sc < A.PTSX && sr >= 0 && sr < A.PTSY) {
-          sre = A.src[static_cast<size_t>(sr) * A.PTSX + sc];
-          sim = A.src[static_cast<size_t>(A.PTSY + sr) * A.PTSX + sc];
+          sre = srcp[static_cast<size_t>(sr) * A.PTSX + sc];
+          sim = srcp[static_cast<size_t>(A.PTSY + sr) * A.PTSX + sc];
         }
       }
       res[0][c] = 0.0;
@@ -393,14 +396,14 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
     fence_barrier_init();
   }
   __syncthreads();
-  if (tid == 0) {
-    tile_note_source(S, A);
-    tile_issue_setup<STAGE>(S, T, c0, b0);
-  }
+  if (tid == 0) tile_issue_setup<STAGE>(S, T, c0, b0);
   // Everything below reads what the earlier kernels of the step wrote.
   grid_dependency_wait();
   launch_dependents();
-  if (tid == 0) tile_issue_state<STAGE>(S, T, c0, b0);
+  if (tid == 0) {
+    tile_issue_state<STAGE>(S, T, c0, b0);
+    tile_note_source(S, A);
+  }
   const bool ok = mbar_wait_bounded(&S.bar, 0);
   if (!__syncthreads_and(ok)) {
     if (tid == 0) atomicCAS(A.err, 0, 5 /* BHR_TIMEOUT */);
@@ -508,7 +511,6 @@ __device__ __forceinline__ void stage_persistent(const Work &W, int *err) {
       const int t = first + j * stride;
       if (t < ntiles) {
         W.get(t, tm, ta, c0, b0);
-        tile_note_source(buf[j], *ta);
         tile_issue_setup<STAGE>(buf[j], *tm, c0, b0);
         buf[j].issued = 1;
       }
@@ -522,9 +524,11 @@ __device__ __forceinline__ void stage_persistent(const Work &W, int *err) {
       if (t < ntiles) {
         W.get(t, tm, ta, c0, b0);
         tile_issue_state<STAGE>(buf[j], *tm, c0, b0);
+        tile_note_source(buf[j], *ta);
       }
     }
   }
+  __syncthreads();  // the first tiles' source notes
   int i = 0;
   for (int t = first; t < ntiles; t += stride, i++) {
     StageSmem<ROWS> &S = buf[i & 1];
@@ -682,9 +686,13 @@ constexpr int kSrcRows = 4;
 __device__ __forceinline__ void source_rows(const SourceArgs &A, const int j0, const int k) {
   __shared__ double rowf[kSrcRows][5];  // T0, T1, T2, cos theta, sin theta
   __shared__ int rok[kSrcRows];
+  // The patch of step k goes to buffer k % 2; a lookahead past the last
+  // record builds nothing.
+  const int kstep = A.rs->k + A.lookahead;
+  if (kstep >= A.nrecs) return;  // uniform across the block
   // By value: the stores to the patch below must not force reloads.
-  const StepRec rec = A.recs[A.rs->k];
-  double *__restrict__ src = A.src;
+  const StepRec rec = A.recs[kstep];
+  double *__restrict__ src = A.src + static_cast<size_t>(kstep & 1) * 2 * A.PTSX * A.PTSY;
   const double a = A.a, mass = A.mass;
   if (k < kSrcRows) {
     const int row = j0 + k + rec.row0;

@@ -101,6 +101,14 @@ void free_all(bhr_solver *s) {
     cudaStreamSynchronize(s->stream);
     cudaStreamDestroy(s->stream);
   }
+  if (s->side) {
+    cudaStreamSynchronize(s->side);
+    cudaStreamDestroy(s->side);
+  }
+  if (s->fork) cudaEventDestroy(s->fork);
+  if (s->join) cudaEventDestroy(s->join);
+  s->stream = s->side = nullptr;
+  s->fork = s->join = nullptr;
 }
 
 // The device's default memory pool keeps freed blocks for reuse instead of
@@ -226,7 +234,10 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
   const size_t NM = static_cast<size_t>(p.N) * p.M;
   int st = BHR_OK;
   if (cudaSetDevice(p.device) != cudaSuccess || prepare_kernels() != cudaSuccess || keep_pool_memory(p.device) ||
-      cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming) != cudaSuccess) {
     set_error("cannot set device / create stream");
     delete s;
     return BHR_CUDA_ERROR;
@@ -235,7 +246,7 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
       (st = dalloc(s, &s->coltab, static_cast<size_t>(CF_COUNT) * p.N)) ||
       (st = dalloc(s, &s->rowtab, static_cast<size_t>(RF_COUNT) * p.M)) || (st = dalloc(s, &s->ctab, NM)) ||
       (st = dalloc(s, &s->rc, p.N)) ||
-      (st = dalloc(s, &s->th, p.M)) || (st = dalloc(s, &s->src, 2 * static_cast<size_t>(p.PTSX) * p.PTSY)) ||
+      (st = dalloc(s, &s->th, p.M)) || (st = dalloc(s, &s->src, 4 * static_cast<size_t>(p.PTSX) * p.PTSY)) ||
       (st = dalloc(s, &s->ext, 2 * static_cast<size_t>(p.M))) || (st = dalloc(s, &s->integ, 4 * static_cast<size_t>(p.M))) ||
       (st = dalloc(s, &s->wproj, 7 * static_cast<size_t>(p.M))) || (st = dalloc(s, &s->wdedt, p.M)) ||
       (st = dalloc(s, &s->rows, 16 * static_cast<size_t>(s->max_rows))) || (st = dalloc(s, &s->rs, 1))) {
@@ -258,7 +269,7 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
       (e = launch_coef_tables(s->coltab, s->rowtab, s->ctab, p.N, p.M, s->stream)) ||
       (e = cudaMemsetAsync(s->u1, 0, 4 * NM * 8, s->stream)) || (e = cudaMemsetAsync(s->u2, 0, 4 * NM * 8, s->stream)) ||
       (e = cudaMemsetAsync(s->integ, 0, 4 * p.M * 8, s->stream)) || (e = cudaMemsetAsync(s->ext, 0, 2 * p.M * 8, s->stream)) ||
-      (e = cudaMemsetAsync(s->src, 0, 2 * static_cast<size_t>(p.PTSX) * p.PTSY * 8, s->stream)) ||
+      (e = cudaMemsetAsync(s->src, 0, 4 * static_cast<size_t>(p.PTSX) * p.PTSY * 8, s->stream)) ||
       (e = cudaMemsetAsync(s->rs, 0, sizeof(RunState), s->stream)) || (e = cudaStreamSynchronize(s->stream))) {
     set_error(std::string("upload: ") + cudaGetErrorString(e));
     free_all(s);
@@ -458,6 +469,9 @@ int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows) {
   BHR_CUDA_TRY(cudaMemcpyAsync(s->recs, recs.data(), sizeof(StepRec) * recs.size(), cudaMemcpyHostToDevice, s->stream));
   BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
   s->has_source = true;
+  // The patch of the current step (later patches are built one step ahead).
+  BHR_CUDA_TRY(launch_source(solver_source_args(s), s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
   // The launch arguments now carry the source and the new records: step
   // graphs captured before (steps taken without a trajectory) are rebuilt.
   if (s->g1) cudaGraphExecDestroy(s->g1);
@@ -621,6 +635,8 @@ SourceArgs bhr::solver_source_args(bhr_solver *s) {
   S.M = p.M;
   S.PTSX = p.PTSX;
   S.PTSY = p.PTSY;
+  S.lookahead = 0;
+  S.nrecs = s->nt;
   S.a = p.a;
   S.mass = p.mass;
   S.m = p.m;
@@ -650,11 +666,26 @@ ExtractArgs bhr::solver_extract_args(bhr_solver *s) {
   return E;
 }
 
+// One step.  With a source, the patch of the next step is built on the
+// side stream while this step's stages run (this step's patch was built
+// during the previous step, or when the trajectory was set); the side
+// branch starts after the previous extraction (which advances the step
+// counter it reads) and joins before this step's extraction.  `ev` (8
+// events): 0..5 bracket the main-stream launches, 6..7 the side source.
 static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
   auto mark = [&](int i) { return ev ? cudaEventRecord(ev[i], s->stream) : cudaSuccess; };
   StageArgs A = solver_stage_args(s);
   BHR_CUDA_TRY(mark(0));
-  if (s->has_source) BHR_CUDA_TRY(launch_source(solver_source_args(s), s->stream));
+  if (s->has_source) {
+    SourceArgs S = solver_source_args(s);
+    S.lookahead = 1;
+    BHR_CUDA_TRY(cudaEventRecord(s->fork, s->stream));
+    BHR_CUDA_TRY(cudaStreamWaitEvent(s->side, s->fork, 0));
+    if (ev) BHR_CUDA_TRY(cudaEventRecord(ev[6], s->side));
+    BHR_CUDA_TRY(launch_source(S, s->side));
+    if (ev) BHR_CUDA_TRY(cudaEventRecord(ev[7], s->side));
+    BHR_CUDA_TRY(cudaEventRecord(s->join, s->side));
+  }
   BHR_CUDA_TRY(mark(1));
   A.vin = s->u0; A.un = s->u0; A.out = s->u1;
   if (s->mixed) {
@@ -670,6 +701,7 @@ static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
     X.u_out = s->u0;
     BHR_CUDA_TRY(launch_mixed_stage(3, s->mmaps[1], X, s->stream));
     BHR_CUDA_TRY(mark(4));
+    if (s->has_source) BHR_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->join, 0));
     BHR_CUDA_TRY(launch_extract(solver_extract_args(s), s->stream));
     BHR_CUDA_TRY(mark(5));
     return BHR_OK;
@@ -682,6 +714,7 @@ static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
   A.vin = s->u2; A.un = s->u0; A.out = s->u0;
   BHR_CUDA_TRY(launch_stage(3, s->maps[2], A, s->stream));
   BHR_CUDA_TRY(mark(4));
+  if (s->has_source) BHR_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->join, 0));
   BHR_CUDA_TRY(launch_extract(solver_extract_args(s), s->stream));
   BHR_CUDA_TRY(mark(5));
   return BHR_OK;
@@ -913,7 +946,8 @@ int bhr_solver_get_source(bhr_solver *s, double *tre, double *tim) {
   StepRec rec{};
   std::vector<double> patch(2 * static_cast<size_t>(p.PTSX) * p.PTSY);
   BHR_CUDA_TRY(cudaMemcpyAsync(&rec, s->recs + (rs.k - 1), sizeof(rec), cudaMemcpyDeviceToHost, s->stream));
-  BHR_CUDA_TRY(cudaMemcpyAsync(patch.data(), s->src, patch.size() * 8, cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaMemcpyAsync(patch.data(), s->src + ((rs.k - 1) & 1) * patch.size(), patch.size() * 8,
+                               cudaMemcpyDeviceToHost, s->stream));
   BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
   for (int j = 0; j < p.PTSY; j++) {
     const int row = rec.row0 + j;
@@ -938,7 +972,7 @@ int bhr_solver_profile(bhr_solver *s, int nsteps, double *avg_ms5, double *total
     return BHR_INVALID_ARG;
   }
   // Events bracket each launch of launch_step on the solver stream.
-  std::vector<cudaEvent_t> ev(6 * static_cast<size_t>(nsteps));
+  std::vector<cudaEvent_t> ev(8 * static_cast<size_t>(nsteps));
   for (auto &e : ev) BHR_CUDA_TRY(cudaEventCreate(&e));
   double sums[5] = {0, 0, 0, 0, 0};
   cudaEvent_t t0, t1;
@@ -946,16 +980,18 @@ int bhr_solver_profile(bhr_solver *s, int nsteps, double *avg_ms5, double *total
   BHR_CUDA_TRY(cudaEventCreate(&t1));
   BHR_CUDA_TRY(cudaEventRecord(t0, s->stream));
   for (int i = 0; i < nsteps; i++) {
-    if (int st = launch_step(s, &ev[6 * static_cast<size_t>(i)])) return st;
+    if (int st = launch_step(s, &ev[8 * static_cast<size_t>(i)])) return st;
     s->steps_done++;
   }
   BHR_CUDA_TRY(cudaEventRecord(t1, s->stream));
   BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
   for (int i = 0; i < nsteps; i++) {
-    cudaEvent_t *e = &ev[6 * static_cast<size_t>(i)];
+    cudaEvent_t *e = &ev[8 * static_cast<size_t>(i)];
     for (int j = 0; j < 5; j++) {
       float ms = 0.f;
-      BHR_CUDA_TRY(cudaEventElapsedTime(&ms, e[j], e[j + 1]));
+      // the source runs on the side stream, overlapped with the stages
+      if (j == 0 && s->has_source) BHR_CUDA_TRY(cudaEventElapsedTime(&ms, e[6], e[7]));
+      else BHR_CUDA_TRY(cudaEventElapsedTime(&ms, e[j], e[j + 1]));
       sums[j] += ms;
     }
   }

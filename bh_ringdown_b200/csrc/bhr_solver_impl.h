@@ -13,6 +13,10 @@ struct bhr_solver {
   bool even_m = true;
   bool has_source = false;
   cudaStream_t stream = nullptr;
+  // The particle source of step k+1 is built on `side` while step k's
+  // stages run: forked after step k-1's extraction, joined into step k's.
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   // device memory
   double *u0 = nullptr, *u1 = nullptr, *u2 = nullptr;
   double *coltab = nullptr, *rowtab = nullptr, *ctab = nullptr, *rc = nullptr, *th = nullptr;
