@@ -49,6 +49,11 @@ BYTES_PER_PT = 256.0  # FP64 SSP-RK3 algorithmic bytes per point per step (coeff
 # stage 2 reads delta1 and writes eps2 (FP32), stage 3 reads eps2 and u1 and
 # writes u^{n+1}: 80 + 32 + 80 bytes per point.
 BYTES_PER_PT_MIXED = 192.0
+# Classical RK4 (--integrator rk4): stage 1 reads u^n, writes y1 (64 B);
+# stage 2 reads y1 and u^n, writes y2 and z (128 B); stage 3 reads y2 and
+# u^n, writes y3 (96 B); stage 4 reads y3 and z, writes u^{n+1} (96 B).
+BYTES_PER_PT_RK4 = 384.0
+INTEGRATOR = "ssprk3"
 PRECISION = "fp64"
 
 
@@ -156,7 +161,8 @@ def make_params(device=0, dt=None):
     w = WORKLOAD
     return bhr.Params(N=w["N"], M=w["M"], Xmin=w["Xmin"], Xmax=w["Xmax"], a=w["a"], m=w["m"], T=w["T"],
                       dt=0.0 if dt is None else dt, courant=w["courant"], Fr=50, out_start=0.0, device=device,
-                      init_kind=bhr.BHR_INIT_ZERO, precision=bhr.BHR_MIXED if PRECISION == "mixed" else bhr.BHR_FP64)
+                      init_kind=bhr.BHR_INIT_ZERO, precision=bhr.BHR_MIXED if PRECISION == "mixed" else bhr.BHR_FP64,
+                      integrator=bhr.BHR_RK4 if INTEGRATOR == "rk4" else bhr.BHR_SSPRK3)
 
 
 def workload_inputs(with_source, device=0):
@@ -231,7 +237,8 @@ def run_ours(args, rank, local_rank, world):
     ms_per_step = total_ms / args.steps
     stage_ms = per_kernel[1:4] / args.steps
     peak, peak_kind = measured_peak()
-    bytes_pt = BYTES_PER_PT_MIXED if PRECISION == "mixed" else BYTES_PER_PT
+    bytes_pt = (BYTES_PER_PT_MIXED if PRECISION == "mixed" else
+                BYTES_PER_PT_RK4 if INTEGRATOR == "rk4" else BYTES_PER_PT)
     achieved = bytes_pt * N * M / (float(stage_ms.sum()) / 1e3) / 1e9
     traffic_pp = profile_traffic()
 
@@ -267,17 +274,22 @@ def run_ours(args, rank, local_rank, world):
             "config": {"workload": f"{args.workload}: {'FP64' if PRECISION == 'fp64' else 'mixed FP64/FP32'} "
                                    f"s=-2 m=2 a=0.9, {N}x{M} on [-200,600]"
                                    + (", plunge source" if with_source else ", source-free (Gaussian pulse initial data)"),
-                       "N_r": N, "N_theta": M, "dt": prm.dt, "integrator": "SSP-RK3",
+                       "N_r": N, "N_theta": M, "dt": prm.dt,
+                       "integrator": "classical RK4" if INTEGRATOR == "rk4" else "SSP-RK3",
                        "source": "synthetic prograde equatorial plunge from ISCO" if with_source else "none",
                        "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": None if traffic_pp is None else traffic_pp * N * M,
-                         "kernel": ("stage_kernel<1,2,3> (one SSP-RK3 step, 256 B/pt algorithmic)" if PRECISION == "fp64"
-                                    else "FP64 stage 1 + FP32 mixed_stage_kernel<2,3> (192 B/pt algorithmic)")},
+                         "kernel": ("FP64 stage 1 + FP32 mixed_stage_kernel<2,3> (192 B/pt algorithmic)"
+                                    if PRECISION == "mixed" else
+                                    "stage_kernel<1,4,4,5> (one classical RK4 step, 384 B/pt algorithmic)"
+                                    if INTEGRATOR == "rk4" else
+                                    "stage_kernel<1,2,3> (one SSP-RK3 step, 256 B/pt algorithmic)")},
             "kernel_ms": {"source": per_kernel[0] / args.steps, "stage1": stage_ms[0], "stage2": stage_ms[1],
-                          "stage3": stage_ms[2], "extract": per_kernel[4] / args.steps},
-            "gpu_launches": args.steps * (5 if with_source else 4),
+                          "stage3+4" if INTEGRATOR == "rk4" else "stage3": stage_ms[2],
+                          "extract": per_kernel[4] / args.steps},
+            "gpu_launches": args.steps * ((5 if with_source else 4) + (1 if INTEGRATOR == "rk4" else 0)),
             "e2e": e2e,
             "clocks": clocks,
             "cpu_baseline": cpu,
@@ -292,7 +304,8 @@ def cpu_baseline(prm, rows, seconds):
     workload (steps of the full grid until about `seconds` elapse)."""
     from oracle import pyoracle
     import bh_ringdown_b200 as bhr
-    o = pyoracle.Oracle(prm.N, prm.M, prm.Xmin, prm.Xmax, prm.a, prm.m, prm.dt, T=prm.T, Fr=50, out_start=0.0)
+    o = pyoracle.Oracle(prm.N, prm.M, prm.Xmin, prm.Xmax, prm.a, prm.m, prm.dt, T=prm.T, Fr=50, out_start=0.0,
+                        integrator=prm.integrator)
     coef = None
     if rows is None:
         o.init_gaussian(prm.init_center, prm.init_width, prm.init_ell)
@@ -645,14 +658,19 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch64", "serve"], default="plunge")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="fp64, or mixed: FP64 state and stage 1, FP32 corrections in stages 2 and 3")
+    ap.add_argument("--integrator", choices=["ssprk3", "rk4"], default="ssprk3",
+                    help="single-solve workloads: SSP-RK3 (the reference's) or classical RK4 (FP64 only)")
     ap.add_argument("--requests", type=int, default=200, help="serve: requests in the stream")
     ap.add_argument("--time-scale", type=float, default=0.02, help="serve: factor on every request's final time")
     ap.add_argument("--load", type=float, default=0.8, help="serve: arrival rate / measured capacity")
     ap.add_argument("--chunk", type=int, default=64, help="serve: steps per engine call")
     ap.add_argument("--plain-requests", type=int, default=60, help="serve: requests timed on the plain path")
     args = ap.parse_args()
-    global PRECISION
+    global PRECISION, INTEGRATOR
     PRECISION = args.precision
+    INTEGRATOR = args.integrator
+    if INTEGRATOR == "rk4" and PRECISION == "mixed":
+        ap.error("--integrator rk4 runs in FP64 only")
     if args.warmup < 3:
         args.warmup = 3
     rank, local_rank, world = env_rank()

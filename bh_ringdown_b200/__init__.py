@@ -29,7 +29,7 @@ BHR_OK = 0
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OUT_OF_MEMORY", 3: "CUDA_ERROR", 4: "NAN_DETECTED",
                 5: "TIMEOUT", 6: "IO_ERROR", 7: "NO_DEVICE"}
 
-BHR_SSPRK3 = 0
+BHR_SSPRK3, BHR_RK4 = 0, 1
 BHR_FP64, BHR_MIXED = 0, 1
 BHR_INIT_ZERO, BHR_INIT_GAUSSIAN = 0, 1
 
@@ -378,4 +378,4 @@ class Engine:
 
 
 __all__ = ["Params", "Particle", "Solver", "Engine", "BhrError", "grid", "swsh", "source_coefficients", "load_library",
-           "BHR_INIT_ZERO", "BHR_INIT_GAUSSIAN", "BHR_FP64", "BHR_MIXED", "BHR_SSPRK3"]
+           "BHR_INIT_ZERO", "BHR_INIT_GAUSSIAN", "BHR_FP64", "BHR_MIXED", "BHR_SSPRK3", "BHR_RK4"]

@@ -476,6 +476,7 @@ void bhr_engine_destroy(bhr_engine *e) {
 
 int bhr_engine_submit(bhr_engine *e, const bhr_params *p, const double *traj_rows, int nrows, int64_t *id) {
   if (!e || !p || !id || (traj_rows && nrows < 2)) return set_fail(BHR_INVALID_ARG, "bad submit arguments");
+  if (p->integrator != BHR_SSPRK3) return set_fail(BHR_INVALID_ARG, "the batch engine steps BHR_SSPRK3 solves only");
   Request r;
   r.p = *p;
   if (traj_rows) r.traj.assign(traj_rows, traj_rows + static_cast<size_t>(nrows) * 10);

@@ -71,7 +71,9 @@ struct StageArgs {
   int persist;          // 1: 16-row tiles walked by one persistent block per SM
   int narrow;           // 1: 8-row tiles on 128-thread blocks (four per SM)
   float *dout;          // mixed precision, stage 1: delta1 = dt L(u^n) in FP32, or nullptr
-  double dt, cx, cy, cyy, cko;
+  double *zout;         // RK4 stage 2: z = (y1 + 2 y2 - u^n)/3, or nullptr
+  double dt;            // the stage's step in the combination (RK4: dt/2, dt, dt/6)
+  double cx, cy, cyy, cko;
 };
 
 struct SourceArgs {

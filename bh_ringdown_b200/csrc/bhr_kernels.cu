@@ -3,11 +3,12 @@
 // One time step is five launches on the solver stream:
 //   source_patch  the Gaussian-smeared particle source on its PTSX x PTSY patch
 //                 (HighOrder/kern.cu:755-768 reset + 1185-2683 deposit)
-//   stage<1,2,3>  one SSP-RK3 stage each: TMA stages a (q, p) tile with its
+//   stage<1,2,3>  one SSP-RK3 stage each (classical RK4: stages 1, 4, 4, 5,
+//                 four launches): TMA stages a (q, p) tile with its
 //                 halo into shared memory, the pole and radial-end closures of
 //                 the stage input are rebuilt there, then the 6th-order
 //                 stencils, Kreiss-Oliger dissipation, coefficients, source
-//                 and the Shu-Osher combination are applied and the interior
+//                 and the stage combination are applied and the interior
 //                 of the next stage is written once
 //                 (HighOrder/kern.cu:171-753 as kernel_rhs*/update*/boundary*)
 //   extract       psi at the extraction column, its two time integrals, and
@@ -43,7 +44,7 @@ struct __align__(128) StageSmem {
   alignas(128) double p[2][ROWS][WC];        // TMA box {WC, ROWS, 2}: planes p_re, p_im with column halo
   alignas(128) double bb[ROWS][WC];          // TMA box {WC, ROWS, 1}: bb on the window columns
   alignas(128) double cf[CF_COUNT][TC];      // TMA box {TC, CF_COUNT}: column factors of the tile columns
-  alignas(128) double un[4][ROWS][TC];       // TMA box {TC, ROWS, 4}: u^n (stages 2 and 3)
+  alignas(128) double un[4][ROWS][TC];       // TMA box {TC, ROWS, 4}: u^n (RK4 stage 5: z), stages > 1
   alignas(128) double rf[RF_COUNT][ROWS];    // TMA box {ROWS, RF_COUNT}: row factors of the tile rows
   uint64_t bar;
   int src_c0, src_r0;           // source patch corner of this step
@@ -83,7 +84,8 @@ __global__ void coef_table_kernel(const double *coltab, const double *rowtab, do
   ctab[id] = bb;
 }
 
-// One tile (columns c0..c0+63, rows b0..b0+ROWS-1) of one SSP-RK3 stage.
+// One tile (columns c0..c0+63, rows b0..b0+ROWS-1) of one Runge-Kutta stage
+// (STAGE 1-3: SSP-RK3; classical RK4 runs stages 1, 4, 4, 5).
 // A stage tile is processed in four steps, shared by the one-tile-per-block
 // kernels and the persistent ones: thread 0 arms the tile's mbarrier and
 // requests the set-up data, then (after the grid dependency) the stage
@@ -337,9 +339,19 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
       }
     }
 
-    // Shu-Osher stage combination (HighOrder/kern.cu:301-318, 582-620).
+    // Stage combination: SSP-RK3 in Shu-Osher form (stages 1-3,
+    // HighOrder/kern.cu:301-318, 582-620), or classical RK4 (stage 1 with
+    // dt/2, then stages 4, 4 and 5).
     const size_t base = static_cast<size_t>(b) * N + a0;
     const bool both = inner || ((a0 >= 3) && (a0 + 1 < N - 3));
+    auto store2 = [&](double *dst, const double v0, const double v1) {
+      if (both) {
+        *reinterpret_cast<double2 *>(dst) = make_double2(v0, v1);
+      } else {
+        if (a0 >= 3 && a0 < N - 3) dst[0] = v0;
+        if (a0 + 1 >= 3 && a0 + 1 < N - 3) dst[1] = v1;
+      }
+    };
 #pragma unroll
     for (int pl = 0; pl < 4; pl++) {
       double o[2];
@@ -361,22 +373,30 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
         if (STAGE == 2) {
           o[0] = 0.25 * (3.0 * u.x + fc[pl][0] + dt * res[pl][0]);
           o[1] = 0.25 * (3.0 * u.y + fc[pl][1] + dt * res[pl][1]);
-        } else {
+        } else if (STAGE == 3) {
           o[0] = kThird * (u.x + 2.0 * fc[pl][0] + 2.0 * dt * res[pl][0]);
           o[1] = kThird * (u.y + 2.0 * fc[pl][1] + 2.0 * dt * res[pl][1]);
+        } else if (STAGE == 4) {
+          // RK4 stages 2 and 3: y = u^n + h L(y'), h = dt/2 or dt.  Stage 2
+          // also folds y1 (its input) and y2 into z = (y1 + 2 y2 - u^n)/3,
+          // so the last stage needs z and y3 only.
+          o[0] = u.x + dt * res[pl][0];
+          o[1] = u.y + dt * res[pl][1];
+          if (A.zout != nullptr)
+            store2(A.zout + pl * NM + base, (fc[pl][0] + 2.0 * o[0] - u.x) * kThird,
+                   (fc[pl][1] + 2.0 * o[1] - u.y) * kThird);
+        } else {
+          // RK4 stage 4 (u^n slot = z, h = dt/6):
+          // u^{n+1} = z + y3/3 + dt/6 L(y3) = u^n + dt/6 (k1 + 2 k2 + 2 k3 + k4).
+          o[0] = u.x + kThird * fc[pl][0] + dt * res[pl][0];
+          o[1] = u.y + kThird * fc[pl][1] + dt * res[pl][1];
         }
       }
       if (TO_SMEM) {
         *reinterpret_cast<double2 *>(&S.un[pl][r][2 * tx]) = make_double2(o[0], o[1]);
         continue;
       }
-      double *dst = A.out + pl * NM + base;
-      if (both) {
-        *reinterpret_cast<double2 *>(dst) = make_double2(o[0], o[1]);
-      } else {
-        if (a0 >= 3 && a0 < N - 3) dst[0] = o[0];
-        if (a0 + 1 >= 3 && a0 + 1 < N - 3) dst[1] = o[1];
-      }
+      store2(A.out + pl * NM + base, o[0], o[1]);
     }
   }
   };
@@ -945,15 +965,6 @@ cudaError_t encode_state_maps(void *planes, int N, int M, int rows, CUtensorMap 
 }
 
 
-template <int ROWS>
-static cudaError_t launch_rows(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st) {
-  const size_t smem = sizeof(StageSmem<ROWS>) + 128;
-  const dim3 grid(a.N / TC, a.M / ROWS), block(32, STAGE_THREADS / 32);
-  if (stage == 1) return launch_pdl(stage_kernel<1, ROWS>, grid, block, smem, st, maps, a);
-  if (stage == 2) return launch_pdl(stage_kernel<2, ROWS>, grid, block, smem, st, maps, a);
-  return launch_pdl(stage_kernel<3, ROWS>, grid, block, smem, st, maps, a);
-}
-
 // Multiprocessors of the current device (cached per device).
 static int sm_count() {
   static int counts[64] = {0};
@@ -969,54 +980,63 @@ static int sm_count() {
 
 static size_t persist_smem_bytes() { return 2 * sizeof(StageSmem<kPersistRows>) + 128; }
 
+// Runtime stage number -> kernel template argument.
+template <class F>
+static cudaError_t by_stage(const int stage, F &&f) {
+  switch (stage) {
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 2: return f(std::integral_constant<int, 2>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    case 4: return f(std::integral_constant<int, 4>{});
+    case 5: return f(std::integral_constant<int, 5>{});
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st) {
-  if (a.narrow) {
-    const size_t smem = sizeof(StageSmem<8>) + 128;
-    const dim3 grid(a.N / TC, a.M / 8), block(32, kNarrowThreads / 32);
-    if (stage == 1) return launch_pdl(stage_narrow_kernel<1>, grid, block, smem, st, maps, a);
-    if (stage == 2) return launch_pdl(stage_narrow_kernel<2>, grid, block, smem, st, maps, a);
-    return launch_pdl(stage_narrow_kernel<3>, grid, block, smem, st, maps, a);
-  }
-  if (a.persist) {
-    const int ntiles = (a.N / TC) * (a.M / kPersistRows);
-    const dim3 grid(std::min(ntiles, sm_count())), block(32, kPersistThreads / 32);
-    const size_t smem = persist_smem_bytes();
-    if (stage == 1) return launch_pdl(stage_persistent_kernel<1>, grid, block, smem, st, maps, a);
-    if (stage == 2) return launch_pdl(stage_persistent_kernel<2>, grid, block, smem, st, maps, a);
-    return launch_pdl(stage_persistent_kernel<3>, grid, block, smem, st, maps, a);
-  }
-  return a.rows == 8 ? launch_rows<8>(stage, maps, a, st) : launch_rows<16>(stage, maps, a, st);
+  return by_stage(stage, [&](auto sc) {
+    constexpr int S = decltype(sc)::value;
+    if (a.narrow) {
+      const size_t smem = sizeof(StageSmem<8>) + 128;
+      return launch_pdl(stage_narrow_kernel<S>, dim3(a.N / TC, a.M / 8), dim3(32, kNarrowThreads / 32), smem, st,
+                        maps, a);
+    }
+    if (a.persist) {
+      const int ntiles = (a.N / TC) * (a.M / kPersistRows);
+      return launch_pdl(stage_persistent_kernel<S>, dim3(std::min(ntiles, sm_count())),
+                        dim3(32, kPersistThreads / 32), persist_smem_bytes(), st, maps, a);
+    }
+    const dim3 block(32, STAGE_THREADS / 32);
+    if (a.rows == 8)
+      return launch_pdl(stage_kernel<S, 8>, dim3(a.N / TC, a.M / 8), block, sizeof(StageSmem<8>) + 128, st, maps, a);
+    return launch_pdl(stage_kernel<S, 16>, dim3(a.N / TC, a.M / 16), block, sizeof(StageSmem<16>) + 128, st, maps, a);
+  });
 }
 
 // Once per device (the attribute is per device context).
 cudaError_t prepare_kernels() {
   const int s8 = static_cast<int>(sizeof(StageSmem<8>) + 128), s16 = static_cast<int>(sizeof(StageSmem<16>) + 128);
-  cudaError_t e;
-  if ((e = cudaFuncSetAttribute(stage_kernel<1, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
-      (e = cudaFuncSetAttribute(stage_kernel<2, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
-      (e = cudaFuncSetAttribute(stage_kernel<3, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
-      (e = cudaFuncSetAttribute(stage_kernel<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)) ||
-      (e = cudaFuncSetAttribute(stage_kernel<2, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)) ||
-      (e = cudaFuncSetAttribute(stage_kernel<3, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)) ||
-      (e = cudaFuncSetAttribute(stage_batch_kernel<1, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
-      (e = cudaFuncSetAttribute(stage_batch_kernel<2, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
-      (e = cudaFuncSetAttribute(stage_batch_kernel<3, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
-      (e = cudaFuncSetAttribute(stage_batch_kernel<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)) ||
-      (e = cudaFuncSetAttribute(stage_batch_kernel<2, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)) ||
-      (e = cudaFuncSetAttribute(stage_batch_kernel<3, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, s16)))
-    return e;
-  if ((e = cudaFuncSetAttribute(stage_narrow_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
-      (e = cudaFuncSetAttribute(stage_narrow_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)) ||
-      (e = cudaFuncSetAttribute(stage_narrow_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, s8)))
-    return e;
   const int sp = static_cast<int>(persist_smem_bytes());
-  if ((e = cudaFuncSetAttribute(stage_persistent_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp)) ||
-      (e = cudaFuncSetAttribute(stage_persistent_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp)) ||
-      (e = cudaFuncSetAttribute(stage_persistent_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp)) ||
-      (e = cudaFuncSetAttribute(stage_persistent_batch_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp)) ||
-      (e = cudaFuncSetAttribute(stage_persistent_batch_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp)) ||
-      (e = cudaFuncSetAttribute(stage_persistent_batch_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp)))
-    return e;
+  constexpr auto kSmem = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  for (int stage = 1; stage <= 5; stage++) {
+    const cudaError_t e = by_stage(stage, [&](auto sc) {
+      constexpr int S = decltype(sc)::value;
+      cudaError_t r;
+      if ((r = cudaFuncSetAttribute(stage_kernel<S, 8>, kSmem, s8)) ||
+          (r = cudaFuncSetAttribute(stage_kernel<S, 16>, kSmem, s16)) ||
+          (r = cudaFuncSetAttribute(stage_narrow_kernel<S>, kSmem, s8)) ||
+          (r = cudaFuncSetAttribute(stage_persistent_kernel<S>, kSmem, sp)))
+        return r;
+      if constexpr (S <= 3) {  // the batch engine steps SSP-RK3 only
+        if ((r = cudaFuncSetAttribute(stage_batch_kernel<S, 8>, kSmem, s8)) ||
+            (r = cudaFuncSetAttribute(stage_batch_kernel<S, 16>, kSmem, s16)) ||
+            (r = cudaFuncSetAttribute(stage_persistent_batch_kernel<S>, kSmem, sp)))
+          return r;
+      }
+      return cudaSuccess;
+    });
+    if (e != cudaSuccess) return e;
+  }
   return cudaSuccess;
 }
 

@@ -66,8 +66,12 @@ int validate(const bhr_params &p) {
     set_error("PTSX in [1,1024], PTSY >= 1");
     return BHR_INVALID_ARG;
   }
-  if ((p.precision != BHR_FP64 && p.precision != BHR_MIXED) || p.integrator != BHR_SSPRK3) {
-    set_error("precision must be BHR_FP64 or BHR_MIXED and the integrator BHR_SSPRK3");
+  if ((p.precision != BHR_FP64 && p.precision != BHR_MIXED) || (p.integrator != BHR_SSPRK3 && p.integrator != BHR_RK4)) {
+    set_error("precision must be BHR_FP64 or BHR_MIXED and the integrator BHR_SSPRK3 or BHR_RK4");
+    return BHR_INVALID_ARG;
+  }
+  if (p.integrator == BHR_RK4 && p.precision != BHR_FP64) {
+    set_error("BHR_RK4 runs in BHR_FP64 only");
     return BHR_INVALID_ARG;
   }
   return BHR_OK;
@@ -89,7 +93,7 @@ int dalloc(bhr_solver *s, T **ptr, size_t count) {
 }
 
 void free_all(bhr_solver *s) {
-  void *ptrs[] = {s->u0,    s->u1,   s->u2,     s->coltab, s->rowtab, s->ctab,   s->rc,     s->th,
+  void *ptrs[] = {s->u0,    s->u1,   s->u2,     s->u3,     s->coltab, s->rowtab, s->ctab,   s->rc,     s->th,
                   s->src,   s->ext,  s->integ,  s->wproj,  s->wdedt,  s->rows,   s->recs,   s->rs,
                   s->d1f,   s->e2f,  s->colf32, s->rowf32, s->bbf};
   for (void *q : ptrs)
@@ -290,6 +294,20 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
         tile_rows = 8;
         s->narrow = 1;
       }
+    }
+  }
+  if (p.integrator == BHR_RK4) {
+    s->rk4 = true;
+    if ((st = dalloc(s, &s->u3, 4 * NM))) {
+      free_all(s);
+      delete s;
+      return st;
+    }
+    if ((e = cudaMemsetAsync(s->u3, 0, 4 * NM * 8, s->stream)) || (e = cudaStreamSynchronize(s->stream))) {
+      set_error(std::string("upload: ") + cudaGetErrorString(e));
+      free_all(s);
+      delete s;
+      return BHR_CUDA_ERROR;
     }
   }
   if (p.precision == BHR_MIXED) {
@@ -508,13 +526,15 @@ int bhr_solver_load_trajectory(bhr_solver *s, const char *path) {
 
 static int encode_maps(bhr_solver *s, int rows) {
   const bhr_params &p = s->p;
-  double *bufs[3] = {s->u0, s->u1, s->u2};
-  for (int i = 0; i < 3; i++) {
+  // {stage input, u^n slot, output}: SSP-RK3 stages 0..2, RK4 extras 3, 4
+  double *const plan[5][3] = {{s->u0, s->u0, s->u1}, {s->u1, s->u0, s->u2}, {s->u2, s->u0, s->u0},
+                              {s->u2, s->u0, s->u1}, {s->u1, s->u3, s->u0}};
+  for (int i = 0; i < (s->rk4 ? 5 : 3); i++) {
     StageMaps &m = s->maps[i];
     CUtensorMap unused_q, unused_p;
-    if (encode_state_maps(s->u0, p.N, p.M, rows, &unused_q, &unused_p, &m.u) != cudaSuccess ||
-        encode_state_maps(bufs[(i + 1) % 3], p.N, p.M, rows, &unused_q, &unused_p, &m.o) != cudaSuccess ||
-        encode_state_maps(bufs[i], p.N, p.M, rows, &m.q, &m.p, nullptr) != cudaSuccess ||
+    if (encode_state_maps(plan[i][1], p.N, p.M, rows, &unused_q, &unused_p, &m.u) != cudaSuccess ||
+        encode_state_maps(plan[i][2], p.N, p.M, rows, &unused_q, &unused_p, &m.o) != cudaSuccess ||
+        encode_state_maps(plan[i][0], p.N, p.M, rows, &m.q, &m.p, nullptr) != cudaSuccess ||
         encode_coef_maps(s->ctab, s->coltab, s->rowtab, p.N, p.M, rows, &m) != cudaSuccess) {
       set_error("cuTensorMapEncodeTiled failed");
       return BHR_CUDA_ERROR;
@@ -706,14 +726,32 @@ static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
     BHR_CUDA_TRY(mark(5));
     return BHR_OK;
   }
-  BHR_CUDA_TRY(launch_stage(1, s->maps[0], A, s->stream));
-  BHR_CUDA_TRY(mark(2));
-  A.vin = s->u1; A.un = s->u0; A.out = s->u2;
-  BHR_CUDA_TRY(launch_stage(2, s->maps[1], A, s->stream));
-  BHR_CUDA_TRY(mark(3));
-  A.vin = s->u2; A.un = s->u0; A.out = s->u0;
-  BHR_CUDA_TRY(launch_stage(3, s->maps[2], A, s->stream));
-  BHR_CUDA_TRY(mark(4));
+  if (s->rk4) {
+    // Classical RK4, the step's source held fixed in all four stages:
+    // y1 = u + dt/2 L(u); y2 = u + dt/2 L(y1), z = (y1 + 2 y2 - u)/3;
+    // y3 = u + dt L(y2); u <- z + y3/3 + dt/6 L(y3).
+    const double dt = A.dt;
+    A.dt = 0.5 * dt;
+    BHR_CUDA_TRY(launch_stage(1, s->maps[0], A, s->stream));
+    BHR_CUDA_TRY(mark(2));
+    A.vin = s->u1; A.un = s->u0; A.out = s->u2; A.zout = s->u3;
+    BHR_CUDA_TRY(launch_stage(4, s->maps[1], A, s->stream));
+    BHR_CUDA_TRY(mark(3));
+    A.vin = s->u2; A.un = s->u0; A.out = s->u1; A.zout = nullptr; A.dt = dt;
+    BHR_CUDA_TRY(launch_stage(4, s->maps[3], A, s->stream));
+    A.vin = s->u1; A.un = s->u3; A.out = s->u0; A.dt = dt / 6.0;
+    BHR_CUDA_TRY(launch_stage(5, s->maps[4], A, s->stream));
+    BHR_CUDA_TRY(mark(4));
+  } else {
+    BHR_CUDA_TRY(launch_stage(1, s->maps[0], A, s->stream));
+    BHR_CUDA_TRY(mark(2));
+    A.vin = s->u1; A.un = s->u0; A.out = s->u2;
+    BHR_CUDA_TRY(launch_stage(2, s->maps[1], A, s->stream));
+    BHR_CUDA_TRY(mark(3));
+    A.vin = s->u2; A.un = s->u0; A.out = s->u0;
+    BHR_CUDA_TRY(launch_stage(3, s->maps[2], A, s->stream));
+    BHR_CUDA_TRY(mark(4));
+  }
   if (s->has_source) BHR_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->join, 0));
   BHR_CUDA_TRY(launch_extract(solver_extract_args(s), s->stream));
   BHR_CUDA_TRY(mark(5));

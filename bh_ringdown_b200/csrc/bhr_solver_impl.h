@@ -19,6 +19,9 @@ struct bhr_solver {
   cudaEvent_t fork = nullptr, join = nullptr;
   // device memory
   double *u0 = nullptr, *u1 = nullptr, *u2 = nullptr;
+  // classical RK4 (BHR_RK4): u1 holds y1 then y3, u2 y2, u3 z = (y1 + 2 y2 - u^n)/3
+  bool rk4 = false;
+  double *u3 = nullptr;
   double *coltab = nullptr, *rowtab = nullptr, *ctab = nullptr, *rc = nullptr, *th = nullptr;
   double *src = nullptr, *ext = nullptr, *integ = nullptr, *wproj = nullptr, *wdedt = nullptr, *rows = nullptr;
   // mixed precision (BHR_MIXED): FP32 delta1 and eps2 planes, FP32 tables
@@ -28,7 +31,10 @@ struct bhr_solver {
   bhr::StepRec *recs = nullptr;
   bhr::RunState *rs = nullptr;
   size_t bytes = 0;
-  bhr::StageMaps maps[3];  // per stage input state (u^n, u1, u2)
+  // Per stage: input state, u^n slot and TMA store target.  SSP-RK3 uses
+  // 0..2 (u^n -> u1, u1 -> u2, u2 -> u^n); RK4 uses 0, 1, 3 (u2 -> u1) and
+  // 4 (u1 with z -> u^n).
+  bhr::StageMaps maps[5];
   int tile_rows = 16; // stage tile height chosen for this grid
   int persist = 0;     // 1: persistent stage kernels (16-row tiles, one block per SM)
   int narrow = 0;      // 1: 8-row tiles on 128-thread blocks (four per SM)

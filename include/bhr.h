@@ -42,7 +42,12 @@ typedef enum bhr_status {
   BHR_NO_DEVICE = 7      /* no CUDA device available                       */
 } bhr_status;
 
-typedef enum bhr_integrator { BHR_SSPRK3 = 0 } bhr_integrator;
+/* BHR_SSPRK3: the reference's integrator (HighOrder/kern.cu:301-318,
+ * 582-620).  BHR_RK4: classical four-stage Runge-Kutta, FP64 only, for runs
+ * specified with RK4; the step's particle source is held fixed in all four
+ * stages as in the reference's step.  bhr_step_noalloc and the batch engine
+ * step SSP-RK3 only. */
+typedef enum bhr_integrator { BHR_SSPRK3 = 0, BHR_RK4 = 1 } bhr_integrator;
 typedef enum bhr_precision { BHR_FP64 = 0, BHR_MIXED = 1 } bhr_precision;
 typedef enum bhr_init_kind { BHR_INIT_ZERO = 0, BHR_INIT_GAUSSIAN = 1 } bhr_init_kind;
 
@@ -165,7 +170,8 @@ int bhr_solver_time_steps(bhr_solver *s, int nsteps, double *ms);
 /* Device stream the solver launches on (a cudaStream_t). */
 void *bhr_solver_stream(bhr_solver *s);
 /* Times nsteps steps on the solver stream with CUDA events; per-kernel
- * average durations in ms for: source, stage1, stage2, stage3, extract. */
+ * average durations in ms for: source, stage1, stage2, stage3, extract
+ * (BHR_RK4: the stage3 slot holds stages 3 and 4 together). */
 int bhr_solver_profile(bhr_solver *s, int nsteps, double *avg_ms5, double *total_ms);
 
 /* The particle-only bilinear coefficients of the point-particle source:

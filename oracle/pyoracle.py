@@ -56,6 +56,8 @@ def lib():
             "orc_get_source": (None, [vp, dp, dp]),
             "orc_deposit_source": (None, [vp, C.POINTER(OrcParticle), dp, dp, D, D]),
             "orc_step": (None, [vp]),
+            "orc_set_integrator": (None, [vp, I]),
+            "orc_eval_rhs": (None, [vp, dp, dp]),
             "orc_get_ext": (None, [vp, dp, dp]),
             "orc_swsh": (D, [D, D, D]),
             "orc_project": (D, [dp, I, D, D]),
@@ -81,7 +83,8 @@ class Oracle:
     """FP64 CPU restatement of the reference HighOrder step (see teuk_oracle.h)."""
 
     def __init__(self, N, M, Xmin, Xmax, a, m, dt, mass=1.0, T=100.0, Fr=1, PTSX=128, PTSY=128, wr_fac=2.0,
-                 wt_fac=6.0, out_start=0.0, ext_col=-1):
+                 wt_fac=6.0, out_start=0.0, ext_col=-1, integrator=0):
+        """integrator: 0 SSP-RK3 (the reference's), 1 classical RK4."""
         self.L = lib()
         self.N, self.M = N, M
         self.params = OrcParams(N, M, Xmin, Xmax, mass, a, m, dt, T, Fr, PTSX, PTSY, wr_fac, wt_fac, out_start,
@@ -90,6 +93,7 @@ class Oracle:
         if not self.h:
             raise ValueError("orc_create rejected the parameters")
         self.h = C.c_void_p(self.h)
+        self.L.orc_set_integrator(self.h, integrator)
 
     def close(self):
         if self.h:
@@ -141,6 +145,13 @@ class Oracle:
         cr = np.ascontiguousarray(coef6.real, dtype=np.float64)
         ci = np.ascontiguousarray(coef6.imag, dtype=np.float64)
         self.L.orc_deposit_source(self.h, C.byref(pt), _p(cr), _p(ci), timer, start)
+
+    def eval_rhs(self, planes):
+        """kernel_rhs of the closure of `planes` (4 x M x N), interior points."""
+        x = np.ascontiguousarray(np.stack([np.asarray(p, dtype=np.float64) for p in planes]))
+        out = np.zeros_like(x)
+        self.L.orc_eval_rhs(self.h, _p(x.reshape(-1)), _p(out.reshape(-1)))
+        return out
 
     def step(self, n=1):
         for _ in range(n):

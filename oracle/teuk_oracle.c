@@ -42,6 +42,8 @@ struct orc_solver {
   double *coef[9];           /* bb cc ee a_re a_im d_re d_im v_re v_im */
   double *u[4];              /* qre qim pre pim       (reference q*, p*)     */
   double *uc[4];             /* stage arrays          (reference *_c)        */
+  int integrator;            /* 0 SSP-RK3 (reference), 1 classical RK4        */
+  double *acc[4];            /* RK4 accumulator, allocated on first use       */
   double *rhs[4];
   double *tred, *timd;
   double *ext_re, *ext_im;   /* d_qre_buff / d_qim_buff                      */
@@ -346,7 +348,7 @@ void orc_destroy(orc_solver *s) {
   if (!s) return;
   free(s->x_c); free(s->r_c); free(s->theta);
   for (int k = 0; k < 9; k++) free(s->coef[k]);
-  for (int f = 0; f < 4; f++) { free(s->u[f]); free(s->uc[f]); free(s->rhs[f]); }
+  for (int f = 0; f < 4; f++) { free(s->u[f]); free(s->uc[f]); free(s->rhs[f]); free(s->acc[f]); }
   free(s->tred); free(s->timd); free(s->ext_re); free(s->ext_im);
   free(s);
 }
@@ -470,8 +472,62 @@ void orc_deposit_source(orc_solver *s, const orc_particle *pt, const double *c_r
   }
 }
 
+/* Classical RK4 -- an option, not the reference's integrator: the textbook
+ * form u + dt/6 (k1 + 2 k2 + 2 k3 + k4) with an accumulator, interior points
+ * only, the closure applied to every stage state and to the result as the
+ * reference does after each SSP-RK3 stage, the step's source held fixed. */
+static void orc_step_rk4(orc_solver *s) {
+  const int N = s->N, M = s->M;
+  const double dt = s->p.dt;
+  const double wk[4] = {dt / 6.0, dt / 3.0, dt / 3.0, dt / 6.0};  /* weights of k1..k4 */
+  const double hk[3] = {0.5 * dt, 0.5 * dt, dt};                  /* y_{i+1} = u + h_i k_i */
+  for (int f = 0; f < 4; f++)
+    if (!s->acc[f]) s->acc[f] = zalloc((size_t)N * M);
+  for (int st = 0; st < 4; st++) {
+    orc_rhs(s, st == 0 ? s->u : s->uc);
+#pragma omp parallel for schedule(static)
+    for (int b = 3; b < M - 3; b++)
+      for (int a = 3; a < N - 3; a++) {
+        const size_t id = (size_t)N * b + a;
+        for (int f = 0; f < 4; f++) {
+          const double k = s->rhs[f][id];
+          if (st == 0) s->acc[f][id] = s->u[f][id] + wk[0] * k;
+          else if (st < 3) s->acc[f][id] += wk[st] * k;
+          if (st < 3) s->uc[f][id] = s->u[f][id] + hk[st] * k;
+          else s->u[f][id] = s->acc[f][id] + wk[3] * k;
+        }
+      }
+    double *const *v = st < 3 ? s->uc : s->u;
+    orc_bnd_poles(s, v);
+    orc_bnd_ends(s, v);
+  }
+  orc_copy_ext(s);
+}
+
+void orc_set_integrator(orc_solver *s, int integrator) { s->integrator = integrator; }
+
+/* kernel_rhs on a given state (four M x N planes, contiguous): the closure
+ * is applied to a copy, the right-hand side (current source included) is
+ * written for the interior points and zero elsewhere.  Uses the stage
+ * arrays as scratch, so only between steps. */
+void orc_eval_rhs(orc_solver *s, const double *in4, double *out4) {
+  const size_t NM = (size_t)s->N * s->M;
+  for (int f = 0; f < 4; f++) {
+    memcpy(s->uc[f], in4 + f * NM, NM * sizeof(double));
+    memset(s->rhs[f], 0, NM * sizeof(double));
+  }
+  orc_bnd_poles(s, s->uc);
+  orc_bnd_ends(s, s->uc);
+  orc_rhs(s, s->uc);
+  for (int f = 0; f < 4; f++) memcpy(out4 + f * NM, s->rhs[f], NM * sizeof(double));
+}
+
 /* One full step as HighOrder/body.cu:131-165 sequences the kernels. */
 void orc_step(orc_solver *s) {
+  if (s->integrator == 1) {
+    orc_step_rk4(s);
+    return;
+  }
   orc_rhs(s, s->u);
   orc_update(s, 1);
   orc_bnd_poles(s, s->uc);

@@ -89,8 +89,14 @@ void orc_deposit_source(orc_solver *s, const orc_particle *pt,
                         const double *c_re6, const double *c_im6,
                         double timer, double start);
 
-/* One SSP-RK3 step (body.cu:131-165), current source held fixed. */
+/* One step (body.cu:131-165), current source held fixed: SSP-RK3 as the
+ * reference, or classical RK4 after orc_set_integrator(s, 1) (an option the
+ * reference does not have; 0 restores SSP-RK3). */
 void orc_step(orc_solver *s);
+void orc_set_integrator(orc_solver *s, int integrator);
+/* kernel_rhs (HighOrder/kern.cu:171-299) of the closure of in4 (four M x N
+ * planes) into out4, interior points; between steps only. */
+void orc_eval_rhs(orc_solver *s, const double *in4, double *out4);
 /* Column ext_col of psi after the last step (kernel_boundary2b copy). */
 void orc_get_ext(const orc_solver *s, double *re, double *im);
 
