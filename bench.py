@@ -288,8 +288,12 @@ def run_ours(args, rank, local_rank, world):
                                     "stage_kernel<1,2,3> (one SSP-RK3 step, 256 B/pt algorithmic)")},
             "kernel_ms": {"source": per_kernel[0] / args.steps, "stage1": stage_ms[0], "stage2": stage_ms[1],
                           "stage3+4" if INTEGRATOR == "rk4" else "stage3": stage_ms[2],
-                          "extract": per_kernel[4] / args.steps},
-            "gpu_launches": args.steps * ((5 if with_source else 4) + (1 if INTEGRATOR == "rk4" else 0)),
+                          "extract": per_kernel[4] / args.steps,
+                          "note": "source and extract run on a side stream beside stages 1 and 2; their "
+                                  "times run from the side stream's fork to the kernel's end"},
+            # per step: the stages, the step-clock kernel, the extraction (of the
+            # previous step, beside stage 2) and the source when there is one
+            "gpu_launches": args.steps * ((6 if with_source else 5) + (1 if INTEGRATOR == "rk4" else 0)),
             "e2e": e2e,
             "clocks": clocks,
             "cpu_baseline": cpu,

@@ -217,6 +217,7 @@ int rebuild(bhr_engine *e) {
     for (int b0 = 0; b0 < s->p.M; b0 += e->rows)
       for (int c0 = 0; c0 < s->p.N; c0 += TC) dst.push_back({i, c0, b0, mix_index});
     ext[i] = solver_extract_args(s);
+    ext[i].set_ks = 1;  // stages and extraction run in sequence here
     if (s->has_source) {
       src.push_back(solver_source_args(s));
       e->max_ptsx = std::max(e->max_ptsx, s->p.PTSX);

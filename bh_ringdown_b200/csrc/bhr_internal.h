@@ -45,13 +45,19 @@ struct StepRec {
   int col0, row0;           // patch origin: ip - PTSX/2, it - PTSY/2
 };
 
-// Device-side run counters, advanced by the extraction kernel at the end of
-// each step so a captured step graph can be replayed.
+// Device-side run counters, advanced on the device so a captured step graph
+// can be replayed.  Two step clocks: `ks` (steps whose stages are done; it
+// selects the step's source record and patch buffer) is advanced by a
+// one-thread kernel after a solver step's final stage, or by the extraction
+// where stages and extraction run in sequence (batch engine); `k` (steps
+// extracted; the waveform's clock) by the extraction kernel.  A solver runs
+// the extraction of step n beside stage 2 of step n+1, so until it has run
+// k == ks - 1.
 struct RunState {
-  int k;          // steps done
+  int k;          // steps extracted
   int nrow;       // waveform rows written
   int err;        // bhr_status of the first device-detected failure
-  int pad;
+  int ks;         // steps whose stages are done
   double timer;   // accumulated as timer += dt (HighOrder/body.cu:214)
 };
 
@@ -70,6 +76,7 @@ struct StageArgs {
   int rows;             // tile height: 8 or 16 theta rows
   int persist;          // 1: 16-row tiles walked by one persistent block per SM
   int narrow;           // 1: 8-row tiles on 128-thread blocks (four per SM)
+  int ring;             // 1: 8-row tiles walked by two 256-thread blocks per SM, two buffers each
   float *dout;          // mixed precision, stage 1: delta1 = dt L(u^n) in FP32, or nullptr
   double *zout;         // RK4 stage 2: z = (y1 + 2 y2 - u^n)/3, or nullptr
   double dt;            // the stage's step in the combination (RK4: dt/2, dt, dt/6)
@@ -83,7 +90,7 @@ struct SourceArgs {
   const double *r_c;    // [N]
   const double *theta;  // [M]
   int N, M, PTSX, PTSY;
-  int lookahead;        // the patch built is for step rs->k + lookahead (0 or 1)
+  int lookahead;        // the patch built is for step rs->ks + lookahead (0 or 1)
   int nrecs;            // steps with a record; later steps are skipped
   double a, mass, m, wt;
 };
@@ -97,6 +104,7 @@ struct ExtractArgs {
   double *rows;         // [max_rows][16]: t, h+/hx x 7, dedt
   RunState *rs;
   int N, M, ext_col, Fr, max_rows, even_m;
+  int set_ks;           // 1: also advance rs->ks (stages and extraction in sequence)
   double dt, out_start, Xmax;
 };
 
@@ -162,6 +170,7 @@ struct BatchTile {
 cudaError_t encode_state_maps(void *planes, int N, int M, int rows, CUtensorMap *tm_q, CUtensorMap *tm_p,
                               CUtensorMap *tm_u);
 cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st);
+cudaError_t launch_step_clock(RunState *rs, cudaStream_t st);
 // Per-point coefficient planes [bb | 1/bir | ee] (3 x M x N) from the tables,
 // and the tensor maps over them and over the column table.
 cudaError_t launch_coef_tables(const double *coltab, const double *rowtab, double *ctab, int N, int M,

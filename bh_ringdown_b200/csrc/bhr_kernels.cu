@@ -65,6 +65,7 @@ BHR_TMA_ALIGNED(StageSmem<16>, cf);
 BHR_TMA_ALIGNED(StageSmem<16>, un);
 BHR_TMA_ALIGNED(StageSmem<16>, rf);
 static_assert(sizeof(StageSmem<16>) % 128 == 0, "persistent buffers must stay 128-byte aligned");
+static_assert(sizeof(StageSmem<8>) % 128 == 0, "ring buffers must stay 128-byte aligned");
 
 // The time-independent per-point coefficient bb (HighOrder/kern.cu:141-147),
 // which the stage kernels need on a stencil window, for the interior rows,
@@ -105,13 +106,14 @@ __device__ __forceinline__ void tile_issue_setup(StageSmem<ROWS> &S, const Stage
   tma_load_2d(&S.rf[0][0], &T.rowf, b0, 0, &S.bar);
 }
 
-// Thread 0, after the grid dependency (the step counter is written by the
-// previous step's extraction): this step's source patch corner and buffer.
+// Thread 0, after the grid dependency (the stage step clock is advanced
+// after the previous step's final stage, or by its extraction): this step's
+// source patch corner and buffer.
 // A block barrier publishes it to the other warps.
 template <int ROWS>
 __device__ __forceinline__ void tile_note_source(StageSmem<ROWS> &S, const StageArgs &A) {
   if (A.src != nullptr) {
-    const int k = A.rs->k;
+    const int k = A.rs->ks;
     const StepRec &rec = A.recs[k];
     S.src_c0 = rec.col0;
     S.src_r0 = rec.row0;
@@ -212,6 +214,35 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
   const int a0 = c0 + 2 * tx;  // this thread's columns a0, a0+1
   const int w0 = 2 * tx + 4;   // their window column
   const double dt = A.dt;
+
+  // Theta derivatives of q on all of this thread's rows
+  // (HighOrder/kern.cu:206-226), from one pass over the RPT + 6 window rows
+  // they reach: each row is read from shared memory once, not once per
+  // output row (the shared-memory load pipe is the stage kernels' busiest
+  // unit).
+  double lla[RPT][2][2];
+#pragma unroll
+  for (int pl = 0; pl < 2; pl++) {
+    double f[RPT + 6][2];
+#pragma unroll
+    for (int j = 0; j < RPT + 6; j++) {
+      const double2 t = *reinterpret_cast<const double2 *>(&S.q[pl][RPT * ty + j][w0]);
+      f[j][0] = t.x;
+      f[j][1] = t.y;
+    }
+#pragma unroll
+    for (int rr = 0; rr < RPT; rr++) {
+      const double ctan_cy = S.rf[RF_CTAN][RPT * ty + rr] * A.cy;
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const double *g = &f[rr][0] + c;  // g[2 j] = row rr + j of column c
+        const double y1 = (g[12] - g[0]) - 9.0 * (g[10] - g[2]) + 45.0 * (g[8] - g[4]);
+        const double y2 = 2.0 * (g[12] + g[0]) - 27.0 * (g[10] + g[2]) + 270.0 * (g[8] + g[4]) - 490.0 * g[6];
+        lla[rr][pl][c] = y2 * A.cyy + ctan_cy * y1;
+      }
+    }
+  }
+
   // The row work, instantiated once for interior tiles (no per-column end
   // checks) and once for tiles at a radial end.
   auto rows = [&](auto inner_tag) {
@@ -222,27 +253,15 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
     const int b = b0 + r;
     if (b < 3 || b >= M - 3) continue;
     if (!inner && (a0 + 1 < 3 || a0 >= N - 3)) continue;
-
-    // Theta derivatives of q (HighOrder/kern.cu:206-226).
-    const double ctan_cy = S.rf[RF_CTAN][r] * A.cy;
     double ll[2][2];
 #pragma unroll
-    for (int pl = 0; pl < 2; pl++) {
-      double f[7][2];
-#pragma unroll
-      for (int j = 0; j < 7; j++) {
-        const double2 t = *reinterpret_cast<const double2 *>(&S.q[pl][r + j][w0]);
-        f[j][0] = t.x;
-        f[j][1] = t.y;
+    for (int q = 0; q < RPT; q++)
+      if (q == rr) {
+        ll[0][0] = lla[q][0][0];
+        ll[0][1] = lla[q][0][1];
+        ll[1][0] = lla[q][1][0];
+        ll[1][1] = lla[q][1][1];
       }
-#pragma unroll
-      for (int c = 0; c < 2; c++) {
-        const double y1 = (f[6][c] - f[0][c]) - 9.0 * (f[5][c] - f[1][c]) + 45.0 * (f[4][c] - f[2][c]);
-        const double y2 = 2.0 * (f[6][c] + f[0][c]) - 27.0 * (f[5][c] + f[1][c]) +
-                          270.0 * (f[4][c] + f[2][c]) - 490.0 * f[3][c];
-        ll[pl][c] = y2 * A.cyy + ctan_cy * y1;
-      }
-    }
 
     // Coefficients at the two points (HighOrder/kern.cu:132-158, 192-197).
     const double cs = S.rf[RF_COS][r];
@@ -460,26 +479,36 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
 }
 
 // ---- persistent stage kernels -------------------------------------------
-// One block of kPersistThreads per SM walks the tiles blockIdx.x,
-// blockIdx.x + gridDim.x, ... through two shared-memory tile buffers: the
-// loads of tile i+2 are issued as soon as tile i is computed, so they run
-// under the computation of tile i+1 and the SM's share of HBM bandwidth is
+// One block per SM walks the tiles blockIdx.x, blockIdx.x + gridDim.x, ...
+// through a ring of NBUF shared-memory tile buffers: the loads of tile
+// i+NBUF are issued as soon as tile i is computed, so they run under the
+// computation of the tiles between and the SM's share of HBM bandwidth is
 // kept busy.  Tile work is the same code as the one-tile-per-block kernels.
+// Two shapes:
+//   persistent  16-row tiles, 512 threads, 2 buffers, interior tiles stored
+//               by TMA from shared memory (also the batch engine's)
+//   ring        8-row tiles, 256 threads, 2 buffers, two blocks per SM
+//               (16 warps, four tiles resident), outputs stored from
+//               registers
 constexpr int kPersistThreads = 512;
 constexpr int kPersistRows = 16;
+constexpr int kRingThreads = 256;
+constexpr int kRingRows = 8;
+constexpr int kRingBufs = 2;
+constexpr int kRingBlocksPerSM = 2;
 
 // Work item i of this block: the solve's maps and arguments and the tile
-// corner.  Single solve: tiles in row-major order over the N/64 x M/16 grid.
+// corner.  Single solve: tiles in row-major order over the N/64 x M/rows grid.
 struct SingleWork {
   const StageMaps *T;
   const StageArgs *A;
-  int ntiles, tiles_x;
+  int ntiles, tiles_x, rows;
   __device__ __forceinline__ int count() const { return ntiles; }
   __device__ __forceinline__ void get(int t, const StageMaps *&tm, const StageArgs *&ta, int &c0, int &b0) const {
     tm = T;
     ta = A;
     c0 = (t % tiles_x) * TC;
-    b0 = (t / tiles_x) * kPersistRows;
+    b0 = (t / tiles_x) * rows;
   }
 };
 template <int STAGE>
@@ -504,9 +533,9 @@ struct BatchWork {
 // barrier all warps reach in the same order.  After a bounded wait gives up
 // the block records BHR_TIMEOUT, issues nothing more and lets the loads in
 // flight land before it exits.
-template <int STAGE, class Work>
+template <int STAGE, int ROWS, int THREADS, int NBUF, bool TMA_STORE, class Work>
 __device__ __forceinline__ void stage_persistent(const Work &W, int *err) {
-  constexpr int ROWS = kPersistRows, NWARPS = kPersistThreads / 32;
+  constexpr int NWARPS = THREADS / 32;
   extern __shared__ unsigned char smem_raw[];
   StageSmem<ROWS> *buf = reinterpret_cast<StageSmem<ROWS> *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
@@ -514,7 +543,7 @@ __device__ __forceinline__ void stage_persistent(const Work &W, int *err) {
   const int ntiles = W.count(), stride = gridDim.x, first = blockIdx.x;
   volatile int *abort_flag = &buf[0].abort;
   if (tid == 0) {
-    for (int j = 0; j < 2; j++) {
+    for (int j = 0; j < NBUF; j++) {
       mbar_init(&buf[j].bar, 1);
       buf[j].done = 0;
       buf[j].issued = 0;
@@ -527,7 +556,7 @@ __device__ __forceinline__ void stage_persistent(const Work &W, int *err) {
   const StageArgs *ta;
   int c0, b0;
   if (tid == 0) {
-    for (int j = 0; j < 2; j++) {
+    for (int j = 0; j < NBUF; j++) {
       const int t = first + j * stride;
       if (t < ntiles) {
         W.get(t, tm, ta, c0, b0);
@@ -539,7 +568,7 @@ __device__ __forceinline__ void stage_persistent(const Work &W, int *err) {
   grid_dependency_wait();
   launch_dependents();
   if (tid == 0) {
-    for (int j = 0; j < 2; j++) {
+    for (int j = 0; j < NBUF; j++) {
       const int t = first + j * stride;
       if (t < ntiles) {
         W.get(t, tm, ta, c0, b0);
@@ -551,9 +580,9 @@ __device__ __forceinline__ void stage_persistent(const Work &W, int *err) {
   __syncthreads();  // the first tiles' source notes
   int i = 0;
   for (int t = first; t < ntiles; t += stride, i++) {
-    StageSmem<ROWS> &S = buf[i & 1];
+    StageSmem<ROWS> &S = buf[i % NBUF];
     bool stop = *abort_flag != 0;
-    if (!stop && !mbar_wait_bounded(&S.bar, (i >> 1) & 1)) {
+    if (!stop && !mbar_wait_bounded(&S.bar, (i / NBUF) & 1)) {
       if (tx == 0) {
         atomicExch(&buf[0].abort, 1);
         atomicCAS(err, 0, 5 /* BHR_TIMEOUT */);
@@ -566,15 +595,15 @@ __device__ __forceinline__ void stage_persistent(const Work &W, int *err) {
     const bool edge = (b0 == 0) || (b0 + ROWS + 3 > M - 3) || (c0 == 0) || (c0 + TC + 4 > N - 3);
     const bool full = (b0 >= 3) && (b0 + ROWS <= M - 3) && (c0 >= 3) && (c0 + TC <= N - 3);
     if (edge) {
-      if (!stop) tile_close<ROWS, kPersistThreads>(S, *ta, c0, b0, tid);
-      named_barrier_sync(1, kPersistThreads);
+      if (!stop) tile_close<ROWS, THREADS>(S, *ta, c0, b0, tid);
+      named_barrier_sync(1, THREADS);
     }
     if (!stop) {
-      if (full) {
-        tile_compute<STAGE, ROWS, kPersistThreads, true>(S, *ta, c0, b0, tx, ty);
+      if (TMA_STORE && full) {
+        tile_compute<STAGE, ROWS, THREADS, true>(S, *ta, c0, b0, tx, ty);
         fence_proxy_async();  // this thread's outputs, for the TMA store
       } else {
-        tile_compute<STAGE, ROWS, kPersistThreads, false>(S, *ta, c0, b0, tx, ty);
+        tile_compute<STAGE, ROWS, THREADS, false>(S, *ta, c0, b0, tx, ty);
       }
     }
     __syncwarp();
@@ -584,12 +613,12 @@ __device__ __forceinline__ void stage_persistent(const Work &W, int *err) {
         __threadfence_block();
         S.done = 0;
         const bool ab = *abort_flag != 0;
-        if (full && !ab) {
+        if (TMA_STORE && full && !ab) {
           tma_store_3d(&tm->o, &S.un[0][0][0], c0, b0, 0);
           bulk_commit();
           bulk_wait_read();
         }
-        const int tn = t + 2 * stride;
+        const int tn = t + NBUF * stride;
         if (tn < ntiles && !ab) {
           fence_proxy_async();
           const StageMaps *tm2;
@@ -609,22 +638,29 @@ __device__ __forceinline__ void stage_persistent(const Work &W, int *err) {
   if (tx == 0) bulk_wait_all();
   __syncthreads();
   if (tid == 0 && *abort_flag != 0)
-    for (int j = 0; j < 2; j++)
+    for (int j = 0; j < NBUF; j++)
       if (buf[j].issued > 0) mbar_wait_bounded(&buf[j].bar, (buf[j].issued - 1) & 1);
 }
 
 template <int STAGE>
 __global__ void __launch_bounds__(kPersistThreads, 1)
     stage_persistent_kernel(const __grid_constant__ StageMaps T, const __grid_constant__ StageArgs A) {
-  SingleWork W{&T, &A, (A.N / TC) * (A.M / kPersistRows), A.N / TC};
-  stage_persistent<STAGE>(W, A.err);
+  SingleWork W{&T, &A, (A.N / TC) * (A.M / kPersistRows), A.N / TC, kPersistRows};
+  stage_persistent<STAGE, kPersistRows, kPersistThreads, 2, true>(W, A.err);
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(kRingThreads, kRingBlocksPerSM)
+    stage_ring_kernel(const __grid_constant__ StageMaps T, const __grid_constant__ StageArgs A) {
+  SingleWork W{&T, &A, (A.N / TC) * (A.M / kRingRows), A.N / TC, kRingRows};
+  stage_persistent<STAGE, kRingRows, kRingThreads, kRingBufs, false>(W, A.err);
 }
 
 template <int STAGE>
 __global__ void __launch_bounds__(kPersistThreads, 1)
     stage_persistent_batch_kernel(const BatchSolve *solves, const BatchTile *tiles, int ntiles, int *err) {
   BatchWork<STAGE> W{solves, tiles, ntiles};
-  stage_persistent<STAGE>(W, err);
+  stage_persistent<STAGE, kPersistRows, kPersistThreads, 2, true>(W, err);
 }
 
 // ---- closure of stored planes (HighOrder/kern.cu:622-753) ------------------
@@ -708,7 +744,7 @@ __device__ __forceinline__ void source_rows(const SourceArgs &A, const int j0, c
   __shared__ int rok[kSrcRows];
   // The patch of step k goes to buffer k % 2; a lookahead past the last
   // record builds nothing.
-  const int kstep = A.rs->k + A.lookahead;
+  const int kstep = A.rs->ks + A.lookahead;
   if (kstep >= A.nrecs) return;  // uniform across the block
   // By value: the stores to the patch below must not force reloads.
   const StepRec rec = A.recs[kstep];
@@ -799,11 +835,13 @@ __global__ void source_batch_kernel(const SourceArgs *args) {
 constexpr int kExtractThreads = 256;
 constexpr int kSums = 15;
 
-// Every kernel of a step calls griddepcontrol.wait before it lets its
-// dependents start, so when this kernel starts, the previous step's
-// extraction (the only writer of integ, rows and the RunState) has
-// completed: those, and the weights written at set-up, are read before the
-// wait; only psi at the extraction column waits for stage 3.
+// Every kernel calls griddepcontrol.wait before it lets its dependents
+// start, and a solver's extraction is ordered after the previous one
+// through the step's stage 3 (which waits for it), so when this kernel
+// starts, the previous step's extraction (the only writer of integ, rows,
+// k, nrow and timer) has completed: those, and the weights written at
+// set-up, are read before the wait; only psi at the extraction column waits
+// for stage 3.
 __device__ __forceinline__ void extract_body(const ExtractArgs &A) {
   __shared__ double red[kExtractThreads / 32][kSums];
   const int tid = threadIdx.x;
@@ -878,10 +916,19 @@ __device__ __forceinline__ void extract_body(const ExtractArgs &A) {
     }
     A.rs->timer = timer + A.dt;
     A.rs->k = k + 1;
+    if (A.set_ks) A.rs->ks = k + 1;
   }
 }
 
 __global__ void __launch_bounds__(kExtractThreads) extract_kernel(const ExtractArgs A) { extract_body(A); }
+
+// After a solver step's final stage: advance the stage step clock.  Its own
+// launch, because every block of the final stage reads the clock.
+__global__ void step_clock_kernel(RunState *rs) {
+  grid_dependency_wait();
+  launch_dependents();
+  if (threadIdx.x == 0) rs->ks += 1;
+}
 
 // One block per solve of a batch.
 __global__ void __launch_bounds__(kExtractThreads) extract_batch_kernel(const ExtractArgs *args) {
@@ -979,6 +1026,7 @@ static int sm_count() {
 }
 
 static size_t persist_smem_bytes() { return 2 * sizeof(StageSmem<kPersistRows>) + 128; }
+static size_t ring_smem_bytes() { return kRingBufs * sizeof(StageSmem<kRingRows>) + 128; }
 
 // Runtime stage number -> kernel template argument.
 template <class F>
@@ -1001,6 +1049,12 @@ cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, c
       return launch_pdl(stage_narrow_kernel<S>, dim3(a.N / TC, a.M / 8), dim3(32, kNarrowThreads / 32), smem, st,
                         maps, a);
     }
+    if (a.ring) {
+      const int ntiles = (a.N / TC) * (a.M / kRingRows);
+      return launch_pdl(stage_ring_kernel<S>, dim3(std::min(ntiles, kRingBlocksPerSM * sm_count())),
+                        dim3(32, kRingThreads / 32),
+                        ring_smem_bytes(), st, maps, a);
+    }
     if (a.persist) {
       const int ntiles = (a.N / TC) * (a.M / kPersistRows);
       return launch_pdl(stage_persistent_kernel<S>, dim3(std::min(ntiles, sm_count())),
@@ -1016,7 +1070,7 @@ cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, c
 // Once per device (the attribute is per device context).
 cudaError_t prepare_kernels() {
   const int s8 = static_cast<int>(sizeof(StageSmem<8>) + 128), s16 = static_cast<int>(sizeof(StageSmem<16>) + 128);
-  const int sp = static_cast<int>(persist_smem_bytes());
+  const int sp = static_cast<int>(persist_smem_bytes()), sr = static_cast<int>(ring_smem_bytes());
   constexpr auto kSmem = cudaFuncAttributeMaxDynamicSharedMemorySize;
   for (int stage = 1; stage <= 5; stage++) {
     const cudaError_t e = by_stage(stage, [&](auto sc) {
@@ -1025,7 +1079,8 @@ cudaError_t prepare_kernels() {
       if ((r = cudaFuncSetAttribute(stage_kernel<S, 8>, kSmem, s8)) ||
           (r = cudaFuncSetAttribute(stage_kernel<S, 16>, kSmem, s16)) ||
           (r = cudaFuncSetAttribute(stage_narrow_kernel<S>, kSmem, s8)) ||
-          (r = cudaFuncSetAttribute(stage_persistent_kernel<S>, kSmem, sp)))
+          (r = cudaFuncSetAttribute(stage_persistent_kernel<S>, kSmem, sp)) ||
+          (r = cudaFuncSetAttribute(stage_ring_kernel<S>, kSmem, sr)))
         return r;
       if constexpr (S <= 3) {  // the batch engine steps SSP-RK3 only
         if ((r = cudaFuncSetAttribute(stage_batch_kernel<S, 8>, kSmem, s8)) ||
@@ -1078,6 +1133,8 @@ cudaError_t launch_source(const SourceArgs &a, cudaStream_t st) {
   return launch_pdl(source_patch_kernel, dim3((a.PTSY + kSrcRows - 1) / kSrcRows), dim3(std::max(a.PTSX, kSrcRows)), 0,
                     st, a);
 }
+
+cudaError_t launch_step_clock(RunState *rs, cudaStream_t st) { return launch_pdl(step_clock_kernel, dim3(1), dim3(32), 0, st, rs); }
 
 cudaError_t launch_extract(const ExtractArgs &a, cudaStream_t st) {
   return launch_pdl(extract_kernel, dim3(1), dim3(kExtractThreads), 0, st, a);

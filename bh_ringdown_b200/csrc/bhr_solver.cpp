@@ -111,8 +111,9 @@ void free_all(bhr_solver *s) {
   }
   if (s->fork) cudaEventDestroy(s->fork);
   if (s->join) cudaEventDestroy(s->join);
+  if (s->fork2) cudaEventDestroy(s->fork2);
   s->stream = s->side = nullptr;
-  s->fork = s->join = nullptr;
+  s->fork = s->join = s->fork2 = nullptr;
 }
 
 // The device's default memory pool keeps freed blocks for reuse instead of
@@ -141,6 +142,7 @@ double tortoise(double r, double a, double rpl, double rmn) {
 }  // namespace
 
 static int autotune_rows(bhr_solver *s);
+static int flush_extract(bhr_solver *s);
 
 extern "C" {
 
@@ -237,11 +239,17 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
 
   const size_t NM = static_cast<size_t>(p.N) * p.M;
   int st = BHR_OK;
+  // The side stream (source, extraction: a few blocks beside the stages)
+  // gets the device's highest priority, so its blocks take the first SM
+  // slots that free up.
+  int hi_prio = 0;
   if (cudaSetDevice(p.device) != cudaSuccess || prepare_kernels() != cudaSuccess || keep_pool_memory(p.device) ||
       cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaDeviceGetStreamPriorityRange(nullptr, &hi_prio) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, hi_prio) != cudaSuccess ||
       cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->fork2, cudaEventDisableTiming) != cudaSuccess) {
     set_error("cannot set device / create stream");
     delete s;
     return BHR_CUDA_ERROR;
@@ -280,8 +288,8 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
     delete s;
     return BHR_CUDA_ERROR;
   }
-  // BHR_STAGE_TILING=block8|block16|persistent fixes the stage tiling of
-  // solves whose tiling is not fixed by the caller.
+  // BHR_STAGE_TILING=block8|block16|persistent|block8n|ring fixes the stage
+  // tiling of solves whose tiling is not fixed by the caller.
   if (tile_rows == 0) {
     if (const char *v = std::getenv("BHR_STAGE_TILING")) {
       if (!std::strcmp(v, "block8")) tile_rows = 8;
@@ -293,6 +301,10 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
       if (!std::strcmp(v, "block8n")) {
         tile_rows = 8;
         s->narrow = 1;
+      }
+      if (!std::strcmp(v, "ring")) {
+        tile_rows = 8;
+        s->ring = 1;
       }
     }
   }
@@ -364,14 +376,17 @@ int bhr_solver_info(const bhr_solver *s, bhr_info *info) {
   info->nt = s->nt;
   info->Fr = s->Fr;
   info->steps_done = s->steps_done;
+  // Reading the row count completes the last step's extraction first.
+  if (int st = flush_extract(const_cast<bhr_solver *>(s))) return st;
   RunState rs{};
-  cudaMemcpy(&rs, s->rs, sizeof(rs), cudaMemcpyDeviceToHost);
+  BHR_CUDA_TRY(cudaMemcpyAsync(&rs, s->rs, sizeof(rs), cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
   info->rows_done = rs.nrow;
   info->has_source = s->has_source ? 1 : 0;
   info->r_plus = s->g.r_plus;
   info->device_bytes = s->bytes;
   info->tile_rows = s->tile_rows;
-  info->persistent = s->persist;
+  info->persistent = s->persist || s->ring;
   return BHR_OK;
 }
 
@@ -385,6 +400,8 @@ int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows) {
     set_error("trajectory needs at least two rows");
     return BHR_INVALID_ARG;
   }
+  cudaSetDevice(s->p.device);
+  if (int st = flush_extract(s)) return st;
   const bhr_params &p = s->p;
   const double a = p.a, mass = p.mass;
   const double rpl = mass + std::sqrt(mass * mass - a * a), rmn = mass - std::sqrt(mass * mass - a * a);
@@ -547,11 +564,12 @@ static int encode_maps(bhr_solver *s, int rows) {
 
 // Stage tiling autotuner: per (device, N, M) the stage kernels are timed
 // with 8- and 16-row tiles one per 256-thread block, 8-row tiles on
-// 128-thread blocks, and the persistent 16-row kernels, on stages 1 and 2 (which write only the solve's scratch stages
-// u1, u2); the fastest is kept for the process.
+// 128-thread blocks, the persistent 16-row kernels and the 8-row ring, on
+// stages 1 and 2 (which write only the solve's scratch stages u1, u2); the
+// fastest is kept for the process.
 static int autotune_rows(bhr_solver *s) {
   static std::mutex mu;
-  static std::vector<std::array<int, 6>> cache;  // device, N, M, rows, persist, narrow
+  static std::vector<std::array<int, 7>> cache;  // device, N, M, rows, persist, narrow, ring
   const bhr_params &p = s->p;
   {
     std::lock_guard<std::mutex> lock(mu);
@@ -559,18 +577,20 @@ static int autotune_rows(bhr_solver *s) {
       if (c[0] == p.device && c[1] == p.N && c[2] == p.M) {
         s->persist = c[4];
         s->narrow = c[5];
+        s->ring = c[6];
         return encode_maps(s, c[3]);
       }
   }
-  static const int cands[4][3] = {{8, 0, 0}, {16, 0, 0}, {16, 1, 0}, {8, 0, 1}};  // rows, persist, narrow
+  static const int cands[5][4] = {{8, 0, 0, 0}, {16, 0, 0, 0}, {16, 1, 0, 0}, {8, 0, 1, 0}, {8, 0, 0, 1}};  // rows, persist, narrow, ring
   double best_ms = 1e30;
   int best = 1;
   cudaEvent_t e0, e1;
   BHR_CUDA_TRY(cudaEventCreate(&e0));
   BHR_CUDA_TRY(cudaEventCreate(&e1));
-  for (int c = 0; c < 4; c++) {
+  for (int c = 0; c < 5; c++) {
     s->persist = cands[c][1];
     s->narrow = cands[c][2];
+    s->ring = cands[c][3];
     if (int st = encode_maps(s, cands[c][0])) return st;
     StageArgs A = solver_stage_args(s);
     A.src = nullptr;
@@ -594,10 +614,11 @@ static int autotune_rows(bhr_solver *s) {
   cudaEventDestroy(e1);
   {
     std::lock_guard<std::mutex> lock(mu);
-    cache.push_back({p.device, p.N, p.M, cands[best][0], cands[best][1], cands[best][2]});
+    cache.push_back({p.device, p.N, p.M, cands[best][0], cands[best][1], cands[best][2], cands[best][3]});
   }
   s->persist = cands[best][1];
   s->narrow = cands[best][2];
+  s->ring = cands[best][3];
   return encode_maps(s, cands[best][0]);
 }
 
@@ -620,6 +641,7 @@ StageArgs bhr::solver_stage_args(bhr_solver *s) {
   A.rows = s->tile_rows;
   A.persist = s->persist;
   A.narrow = s->narrow;
+  A.ring = s->ring;
   A.dt = p.dt;
   A.cx = 0.016666666666667 * odx;
   A.cy = 0.05 * third * odth;
@@ -686,26 +708,43 @@ ExtractArgs bhr::solver_extract_args(bhr_solver *s) {
   return E;
 }
 
-// One step.  With a source, the patch of the next step is built on the
-// side stream while this step's stages run (this step's patch was built
-// during the previous step, or when the trajectory was set); the side
-// branch starts after the previous extraction (which advances the step
-// counter it reads) and joins before this step's extraction.  `ev` (8
-// events): 0..5 bracket the main-stream launches, 6..7 the side source.
+// One step.  On the side stream, beside stage 1, the particle source of the
+// next step is built (into the patch buffer this step does not read; its
+// record is selected by the stage step clock, which the previous step
+// advanced), and beside stage 2 (RK4: stages 2-3) the previous step's
+// extraction runs when it is pending: it reads only u^n, which the stages
+// before the last only read, and its own accumulators.  The side branch
+// joins before the final stage, which overwrites u^n; a one-thread kernel
+// then advances the stage step clock.  This step's extraction is left
+// pending (flush_extract launches it, or the next step).  `ev` (10 events):
+// 0..5 on the main stream (1..4 around the stages, the final stage between
+// 3 and 4), 6..7 around the extraction and 8..9 around the source on the
+// side stream.
 static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
   auto mark = [&](int i) { return ev ? cudaEventRecord(ev[i], s->stream) : cudaSuccess; };
-  StageArgs A = solver_stage_args(s);
+  auto side_mark = [&](int i) { return ev ? cudaEventRecord(ev[i], s->side) : cudaSuccess; };
   BHR_CUDA_TRY(mark(0));
   if (s->has_source) {
-    SourceArgs S = solver_source_args(s);
-    S.lookahead = 1;
     BHR_CUDA_TRY(cudaEventRecord(s->fork, s->stream));
     BHR_CUDA_TRY(cudaStreamWaitEvent(s->side, s->fork, 0));
-    if (ev) BHR_CUDA_TRY(cudaEventRecord(ev[6], s->side));
+    SourceArgs S = solver_source_args(s);
+    S.lookahead = 1;
+    BHR_CUDA_TRY(side_mark(8));
     BHR_CUDA_TRY(launch_source(S, s->side));
-    if (ev) BHR_CUDA_TRY(cudaEventRecord(ev[7], s->side));
-    BHR_CUDA_TRY(cudaEventRecord(s->join, s->side));
+    BHR_CUDA_TRY(side_mark(9));
   }
+  const bool extract = s->pending_extract;
+  const bool side = extract || s->has_source;
+  auto fork_extract = [&]() -> cudaError_t {
+    if (!extract) return side ? cudaEventRecord(s->join, s->side) : cudaSuccess;
+    cudaError_t e;
+    if ((e = cudaEventRecord(s->fork2, s->stream)) || (e = cudaStreamWaitEvent(s->side, s->fork2, 0)) ||
+        (e = side_mark(6)) || (e = launch_extract(solver_extract_args(s), s->side)) || (e = side_mark(7)))
+      return e;
+    return cudaEventRecord(s->join, s->side);
+  };
+  auto join = [&]() { return side ? cudaStreamWaitEvent(s->stream, s->join, 0) : cudaSuccess; };
+  StageArgs A = solver_stage_args(s);
   BHR_CUDA_TRY(mark(1));
   A.vin = s->u0; A.un = s->u0; A.out = s->u1;
   if (s->mixed) {
@@ -713,20 +752,16 @@ static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
     A.dout = s->d1f;
     BHR_CUDA_TRY(launch_stage(1, s->maps[0], A, s->stream));
     BHR_CUDA_TRY(mark(2));
+    BHR_CUDA_TRY(fork_extract());
     MixedArgs X = solver_mixed_args(s);
     X.e_out = s->e2f;
     BHR_CUDA_TRY(launch_mixed_stage(2, s->mmaps[0], X, s->stream));
     BHR_CUDA_TRY(mark(3));
+    BHR_CUDA_TRY(join());
     X.e_out = nullptr;
     X.u_out = s->u0;
     BHR_CUDA_TRY(launch_mixed_stage(3, s->mmaps[1], X, s->stream));
-    BHR_CUDA_TRY(mark(4));
-    if (s->has_source) BHR_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->join, 0));
-    BHR_CUDA_TRY(launch_extract(solver_extract_args(s), s->stream));
-    BHR_CUDA_TRY(mark(5));
-    return BHR_OK;
-  }
-  if (s->rk4) {
+  } else if (s->rk4) {
     // Classical RK4, the step's source held fixed in all four stages:
     // y1 = u + dt/2 L(u); y2 = u + dt/2 L(y1), z = (y1 + 2 y2 - u)/3;
     // y3 = u + dt L(y2); u <- z + y3/3 + dt/6 L(y3).
@@ -734,27 +769,39 @@ static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
     A.dt = 0.5 * dt;
     BHR_CUDA_TRY(launch_stage(1, s->maps[0], A, s->stream));
     BHR_CUDA_TRY(mark(2));
+    BHR_CUDA_TRY(fork_extract());
     A.vin = s->u1; A.un = s->u0; A.out = s->u2; A.zout = s->u3;
     BHR_CUDA_TRY(launch_stage(4, s->maps[1], A, s->stream));
-    BHR_CUDA_TRY(mark(3));
     A.vin = s->u2; A.un = s->u0; A.out = s->u1; A.zout = nullptr; A.dt = dt;
     BHR_CUDA_TRY(launch_stage(4, s->maps[3], A, s->stream));
+    BHR_CUDA_TRY(mark(3));
+    BHR_CUDA_TRY(join());
     A.vin = s->u1; A.un = s->u3; A.out = s->u0; A.dt = dt / 6.0;
     BHR_CUDA_TRY(launch_stage(5, s->maps[4], A, s->stream));
-    BHR_CUDA_TRY(mark(4));
   } else {
     BHR_CUDA_TRY(launch_stage(1, s->maps[0], A, s->stream));
     BHR_CUDA_TRY(mark(2));
+    BHR_CUDA_TRY(fork_extract());
     A.vin = s->u1; A.un = s->u0; A.out = s->u2;
     BHR_CUDA_TRY(launch_stage(2, s->maps[1], A, s->stream));
     BHR_CUDA_TRY(mark(3));
+    BHR_CUDA_TRY(join());
     A.vin = s->u2; A.un = s->u0; A.out = s->u0;
     BHR_CUDA_TRY(launch_stage(3, s->maps[2], A, s->stream));
-    BHR_CUDA_TRY(mark(4));
   }
-  if (s->has_source) BHR_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->join, 0));
-  BHR_CUDA_TRY(launch_extract(solver_extract_args(s), s->stream));
+  BHR_CUDA_TRY(mark(4));
+  BHR_CUDA_TRY(launch_step_clock(s->rs, s->stream));
   BHR_CUDA_TRY(mark(5));
+  s->pending_extract = true;
+  return BHR_OK;
+}
+
+// The last step's extraction, before anything reads the waveform, the
+// extraction buffers or the run counters, or replaces the state.
+static int flush_extract(bhr_solver *s) {
+  if (!s->pending_extract) return BHR_OK;
+  BHR_CUDA_TRY(launch_extract(solver_extract_args(s), s->stream));
+  s->pending_extract = false;
   return BHR_OK;
 }
 
@@ -775,14 +822,19 @@ static int check_run_state(bhr_solver *s) {
 
 // Captures `count` steps of launch_step into an executable graph.  Every
 // launch argument is fixed per solve; what changes from step to step (the
-// step index, the timer, the source record) is read on the device from
-// RunState, so one captured graph replays any step.
+// step clocks, the timer, the source record) is read on the device from
+// RunState, so one captured graph replays any step.  A graph starts and ends
+// with an extraction pending: it extracts the step before it and leaves its
+// own last step's extraction to what follows.
 static int capture_steps(bhr_solver *s, int count, cudaGraphExec_t *out) {
   cudaGraph_t g = nullptr;
+  const bool pending = s->pending_extract;
+  s->pending_extract = true;
   BHR_CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
   int st = BHR_OK;
   for (int i = 0; i < count && st == BHR_OK; i++) st = launch_step(s);
   cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+  s->pending_extract = pending;
   if (st != BHR_OK) {
     if (g) cudaGraphDestroy(g);
     return st;
@@ -801,11 +853,16 @@ static int capture_steps(bhr_solver *s, int count, cudaGraphExec_t *out) {
 }
 
 static int enqueue_steps(bhr_solver *s, int nsteps) {
+  if (nsteps <= 0) return BHR_OK;
   if (!s->g1)
     if (int st = capture_steps(s, 1, &s->g1)) return st;
   if (nsteps >= kGraphBatch && !s->gb)
     if (int st = capture_steps(s, kGraphBatch, &s->gb)) return st;
   int left = nsteps;
+  if (!s->pending_extract) {  // the graphs start with an extraction pending
+    if (int st = launch_step(s)) return st;
+    left--;
+  }
   while (left >= kGraphBatch) {
     BHR_CUDA_TRY(cudaGraphLaunch(s->gb, s->stream));
     left -= kGraphBatch;
@@ -858,6 +915,7 @@ int bhr_solver_time_steps(bhr_solver *s, int nsteps, double *ms) {
 int bhr_solver_waveform(bhr_solver *s, double *t, double *h, double *dedt, int max_rows, int *nrows) {
   if (!s) return BHR_INVALID_ARG;
   BHR_CUDA_TRY(cudaSetDevice(s->p.device));
+  if (int st = flush_extract(s)) return st;
   RunState rs{};
   BHR_CUDA_TRY(cudaMemcpyAsync(&rs, s->rs, sizeof(rs), cudaMemcpyDeviceToHost, s->stream));
   BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -884,9 +942,12 @@ int bhr_solver_run(bhr_solver *s, const char *out_dir, const char *name) {
   for (int done = 0; done < remaining; done += chunk) {
     if (int st = bhr_solver_step(s, std::min(chunk, remaining - done))) return st;
   }
+  if (int st = flush_extract(s)) return st;
+  if (int st = check_run_state(s)) return st;
   if (!out_dir || !name) return BHR_OK;
   RunState rs{};
-  BHR_CUDA_TRY(cudaMemcpy(&rs, s->rs, sizeof(rs), cudaMemcpyDeviceToHost));
+  BHR_CUDA_TRY(cudaMemcpyAsync(&rs, s->rs, sizeof(rs), cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
   std::vector<double> t(rs.nrow), h(static_cast<size_t>(rs.nrow) * 14), e(rs.nrow);
   int n = 0;
   if (int st = bhr_solver_waveform(s, t.data(), h.data(), e.data(), rs.nrow, &n)) return st;
@@ -931,6 +992,7 @@ int bhr_write_waveform(const char *out_dir, const char *name, double m, const do
 int bhr_solver_get_state(bhr_solver *s, double *qre, double *qim, double *pre, double *pim) {
   if (!s) return BHR_INVALID_ARG;
   BHR_CUDA_TRY(cudaSetDevice(s->p.device));
+  if (int st = flush_extract(s)) return st;
   const size_t NM = static_cast<size_t>(s->p.N) * s->p.M;
   BHR_CUDA_TRY(launch_closure(s->u0, s->p.N, s->p.M, s->even_m ? 1 : 0, s->stream));
   double *outs[4] = {qre, qim, pre, pim};
@@ -943,6 +1005,7 @@ int bhr_solver_get_state(bhr_solver *s, double *qre, double *qim, double *pre, d
 int bhr_solver_set_state(bhr_solver *s, const double *qre, const double *qim, const double *pre, const double *pim) {
   if (!s) return BHR_INVALID_ARG;
   BHR_CUDA_TRY(cudaSetDevice(s->p.device));
+  if (int st = flush_extract(s)) return st;
   const size_t NM = static_cast<size_t>(s->p.N) * s->p.M;
   const double *ins[4] = {qre, qim, pre, pim};
   for (int f = 0; f < 4; f++) {
@@ -957,6 +1020,7 @@ int bhr_solver_get_extraction(bhr_solver *s, double *psi_re, double *psi_im, dou
                               double *dint_re, double *dint_im) {
   if (!s) return BHR_INVALID_ARG;
   BHR_CUDA_TRY(cudaSetDevice(s->p.device));
+  if (int st = flush_extract(s)) return st;
   const int M = s->p.M;
   std::vector<double> e(2 * M), in(4 * M);
   BHR_CUDA_TRY(cudaMemcpyAsync(e.data(), s->ext, e.size() * 8, cudaMemcpyDeviceToHost, s->stream));
@@ -980,11 +1044,11 @@ int bhr_solver_get_source(bhr_solver *s, double *tre, double *tim) {
   RunState rs{};
   BHR_CUDA_TRY(cudaMemcpyAsync(&rs, s->rs, sizeof(rs), cudaMemcpyDeviceToHost, s->stream));
   BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
-  if (rs.k <= 0) return BHR_OK;
+  if (rs.ks <= 0) return BHR_OK;
   StepRec rec{};
   std::vector<double> patch(2 * static_cast<size_t>(p.PTSX) * p.PTSY);
-  BHR_CUDA_TRY(cudaMemcpyAsync(&rec, s->recs + (rs.k - 1), sizeof(rec), cudaMemcpyDeviceToHost, s->stream));
-  BHR_CUDA_TRY(cudaMemcpyAsync(patch.data(), s->src + ((rs.k - 1) & 1) * patch.size(), patch.size() * 8,
+  BHR_CUDA_TRY(cudaMemcpyAsync(&rec, s->recs + (rs.ks - 1), sizeof(rec), cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaMemcpyAsync(patch.data(), s->src + ((rs.ks - 1) & 1) * patch.size(), patch.size() * 8,
                                cudaMemcpyDeviceToHost, s->stream));
   BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
   for (int j = 0; j < p.PTSY; j++) {
@@ -1009,28 +1073,40 @@ int bhr_solver_profile(bhr_solver *s, int nsteps, double *avg_ms5, double *total
     set_error("profiling past the end of the trajectory records");
     return BHR_INVALID_ARG;
   }
-  // Events bracket each launch of launch_step on the solver stream.
-  std::vector<cudaEvent_t> ev(8 * static_cast<size_t>(nsteps));
+  // Events bracket each launch of launch_step; the extraction and the
+  // source run on the side stream beside the stages.
+  std::vector<cudaEvent_t> ev(10 * static_cast<size_t>(nsteps));
   for (auto &e : ev) BHR_CUDA_TRY(cudaEventCreate(&e));
+  std::vector<char> had_extract(nsteps);
   double sums[5] = {0, 0, 0, 0, 0};
+  int nextract = 0;
   cudaEvent_t t0, t1;
   BHR_CUDA_TRY(cudaEventCreate(&t0));
   BHR_CUDA_TRY(cudaEventCreate(&t1));
   BHR_CUDA_TRY(cudaEventRecord(t0, s->stream));
   for (int i = 0; i < nsteps; i++) {
-    if (int st = launch_step(s, &ev[8 * static_cast<size_t>(i)])) return st;
+    had_extract[i] = s->pending_extract;
+    if (int st = launch_step(s, &ev[10 * static_cast<size_t>(i)])) return st;
     s->steps_done++;
   }
   BHR_CUDA_TRY(cudaEventRecord(t1, s->stream));
   BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->side));
   for (int i = 0; i < nsteps; i++) {
-    cudaEvent_t *e = &ev[8 * static_cast<size_t>(i)];
-    for (int j = 0; j < 5; j++) {
-      float ms = 0.f;
-      // the source runs on the side stream, overlapped with the stages
-      if (j == 0 && s->has_source) BHR_CUDA_TRY(cudaEventElapsedTime(&ms, e[6], e[7]));
-      else BHR_CUDA_TRY(cudaEventElapsedTime(&ms, e[j], e[j + 1]));
+    cudaEvent_t *e = &ev[10 * static_cast<size_t>(i)];
+    float ms = 0.f;
+    if (s->has_source) {
+      BHR_CUDA_TRY(cudaEventElapsedTime(&ms, e[8], e[9]));
+      sums[0] += ms;
+    }
+    for (int j = 1; j < 4; j++) {
+      BHR_CUDA_TRY(cudaEventElapsedTime(&ms, e[j], e[j + 1]));
       sums[j] += ms;
+    }
+    if (had_extract[i]) {
+      BHR_CUDA_TRY(cudaEventElapsedTime(&ms, e[6], e[7]));
+      sums[4] += ms;
+      nextract++;
     }
   }
   float tot = 0.f;
@@ -1038,8 +1114,10 @@ int bhr_solver_profile(bhr_solver *s, int nsteps, double *avg_ms5, double *total
   for (auto &e : ev) cudaEventDestroy(e);
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
-  if (avg_ms5)
-    for (int j = 0; j < 5; j++) avg_ms5[j] = sums[j] / nsteps;
+  if (avg_ms5) {
+    for (int j = 0; j < 4; j++) avg_ms5[j] = sums[j] / nsteps;
+    avg_ms5[4] = nextract ? sums[4] / nextract : 0.0;
+  }
   if (total_ms) *total_ms = tot;
   return check_run_state(s);
 }

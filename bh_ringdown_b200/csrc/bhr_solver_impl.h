@@ -16,7 +16,7 @@ struct bhr_solver {
   // The particle source of step k+1 is built on `side` while step k's
   // stages run: forked after step k-1's extraction, joined into step k's.
   cudaStream_t side = nullptr;
-  cudaEvent_t fork = nullptr, join = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr, fork2 = nullptr;
   // device memory
   double *u0 = nullptr, *u1 = nullptr, *u2 = nullptr;
   // classical RK4 (BHR_RK4): u1 holds y1 then y3, u2 y2, u3 z = (y1 + 2 y2 - u^n)/3
@@ -38,7 +38,11 @@ struct bhr_solver {
   int tile_rows = 16; // stage tile height chosen for this grid
   int persist = 0;     // 1: persistent stage kernels (16-row tiles, one block per SM)
   int narrow = 0;      // 1: 8-row tiles on 128-thread blocks (four per SM)
+  int ring = 0;        // 1: 8-row tiles through 2-buffer rings, two 256-thread blocks per SM
   int steps_done = 0;
+  // The extraction of the last step launched has not been launched yet: it
+  // runs beside the next step's first stages, or before a host read.
+  bool pending_extract = false;
   // Captured step graphs: one step, and kGraphBatch steps in one launch.
   cudaGraphExec_t g1 = nullptr, gb = nullptr;
 };

@@ -158,17 +158,17 @@ def test_headline_workload_grid_matches_oracle():
     assert rel_field_err(s.get_state(), o.get_state()) <= FIELD_TOL
 
 
-@pytest.mark.parametrize("tiling", ["block8", "block16", "persistent", "block8n"])
+@pytest.mark.parametrize("tiling", ["block8", "block16", "persistent", "block8n", "ring"])
 def test_every_stage_tiling_matches_oracle(tiling, monkeypatch):
     """Each stage tiling (8- and 16-row tiles one per block, persistent
-    blocks walking 16-row tiles through two buffers) on a sourced plunge
-    whose grid has several tiles per persistent block and a patch that
-    crosses tile edges."""
+    blocks walking 16-row tiles, or 8-row tiles two blocks per SM, through
+    two buffers) on a sourced plunge whose grid has several tiles per
+    persistent block and a patch that crosses tile edges."""
     monkeypatch.setenv("BHR_STAGE_TILING", tiling)
     s, o, rows, coef = traj_pair(1024, 64, -50.0, 50.0, 0.7, 2.0, ext_col=640)
     info = s.info()
-    assert info["persistent"] == (tiling == "persistent")
-    assert info["tile_rows"] == (8 if tiling in ("block8", "block8n") else 16)
+    assert info["persistent"] == (tiling in ("persistent", "ring"))
+    assert info["tile_rows"] == (8 if tiling in ("block8", "block8n", "ring") else 16)
     n = 120
     s.step(n)
     t, h, dedt, steps, _, _ = o.run(traj=rows, coef_fn=coef, nsteps=n)
@@ -178,7 +178,7 @@ def test_every_stage_tiling_matches_oracle(tiling, monkeypatch):
     assert np.linalg.norm(hs - h) <= WAVE_TOL * np.linalg.norm(h)
 
 
-@pytest.mark.parametrize("tiling", ["block16", "persistent"])
+@pytest.mark.parametrize("tiling", ["block16", "persistent", "ring"])
 def test_trajectory_set_after_stepping(tiling, monkeypatch):
     """A step taken before the trajectory is set captures the step graph
     without a source; setting the trajectory must rebuild what was captured.

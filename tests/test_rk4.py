@@ -109,14 +109,14 @@ def gpu_pair(N, M, Xmin, Xmax, a, m, dt, center=5.0, Fr=1, T=100.0, ext_col=-1):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("tiling", ["block8", "block16", "persistent", "block8n"])
+@pytest.mark.parametrize("tiling", ["block8", "block16", "persistent", "block8n", "ring"])
 def test_rk4_every_stage_tiling_matches_oracle(tiling, monkeypatch):
     """1024 x 64 (several tiles per persistent block), a=0.6, m=2."""
     monkeypatch.setenv("BHR_STAGE_TILING", tiling)
     N, M, Xmin, Xmax = 1024, 64, -50.0, 50.0
     s, o = gpu_pair(N, M, Xmin, Xmax, 0.6, 2.0, 0.25 * (Xmax - Xmin) / N, Fr=5, ext_col=700)
     info = s.info()
-    assert info["persistent"] == (tiling == "persistent")
+    assert info["persistent"] == (tiling in ("persistent", "ring"))
     for k in (1, 9, 30):
         s.step(k)
         o.step(k)
