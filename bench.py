@@ -199,6 +199,7 @@ def run_ours(args, rank, local_rank, world):
     solver = bhr.Solver(prm)
     if rows is not None:
         solver.set_trajectory(rows)
+    tiling = solver.info()["tiling"]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def flush_l2():
@@ -277,6 +278,7 @@ def run_ours(args, rank, local_rank, world):
                        "N_r": N, "N_theta": M, "dt": prm.dt,
                        "integrator": "classical RK4" if INTEGRATOR == "rk4" else "SSP-RK3",
                        "source": "synthetic prograde equatorial plunge from ISCO" if with_source else "none",
+                       "stage_tiling": tiling,
                        "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,

@@ -56,7 +56,9 @@ class Particle(C.Structure):
 class _Info(C.Structure):
     _fields_ = [("N", I), ("M", I), ("dx", D), ("dtheta", D), ("dt", D), ("nt", I), ("Fr", I),
                 ("steps_done", I), ("rows_done", I), ("has_source", I), ("r_plus", D), ("device_bytes", C.c_size_t),
-                ("tile_rows", I), ("persistent", I)]
+                ("tile_rows", I), ("persistent", I), ("tiling", I)]
+
+TILINGS = ("block8", "block16", "persistent", "block8n", "ring")  # bhr_tiling, by value
 
 
 class _RequestInfo(C.Structure):
@@ -244,7 +246,9 @@ class Solver:
     def info(self) -> dict:
         inf = _Info()
         _check(self.lib.bhr_solver_info(self._h, C.byref(inf)))
-        return {f[0]: getattr(inf, f[0]) for f in _Info._fields_}
+        d = {f[0]: getattr(inf, f[0]) for f in _Info._fields_}
+        d["tiling"] = TILINGS[d["tiling"]]
+        return d
 
     def set_trajectory(self, rows: np.ndarray):
         rows = np.ascontiguousarray(rows, dtype=np.float64)

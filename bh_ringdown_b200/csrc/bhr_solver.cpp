@@ -387,6 +387,10 @@ int bhr_solver_info(const bhr_solver *s, bhr_info *info) {
   info->device_bytes = s->bytes;
   info->tile_rows = s->tile_rows;
   info->persistent = s->persist || s->ring;
+  info->tiling = s->ring ? BHR_TILING_RING
+                 : s->narrow ? BHR_TILING_BLOCK8N
+                 : s->persist ? BHR_TILING_PERSISTENT
+                 : s->tile_rows == 8 ? BHR_TILING_BLOCK8 : BHR_TILING_BLOCK16;
   return BHR_OK;
 }
 

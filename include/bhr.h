@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define BHR_ABI_VERSION 1
+#define BHR_ABI_VERSION 2
 
 typedef enum bhr_status {
   BHR_OK = 0,
@@ -50,6 +50,18 @@ typedef enum bhr_status {
 typedef enum bhr_integrator { BHR_SSPRK3 = 0, BHR_RK4 = 1 } bhr_integrator;
 typedef enum bhr_precision { BHR_FP64 = 0, BHR_MIXED = 1 } bhr_precision;
 typedef enum bhr_init_kind { BHR_INIT_ZERO = 0, BHR_INIT_GAUSSIAN = 1 } bhr_init_kind;
+/* Stage kernel tilings (chosen per device and grid by timing, or fixed by
+ * the environment variable BHR_STAGE_TILING=block8|block16|persistent|
+ * block8n|ring): one 64 x 8 or 64 x 16 tile per 256-thread block; 64 x 16
+ * tiles walked by one 512-thread block per SM; 64 x 8 tiles per 128-thread
+ * block, four per SM; 64 x 8 tiles walked by two 256-thread blocks per SM. */
+typedef enum bhr_tiling {
+  BHR_TILING_BLOCK8 = 0,
+  BHR_TILING_BLOCK16 = 1,
+  BHR_TILING_PERSISTENT = 2,
+  BHR_TILING_BLOCK8N = 3,
+  BHR_TILING_RING = 4
+} bhr_tiling;
 
 /* Run parameters.  Replaces HighOrder/parm.h:1-13 (N, M, Xmax, Xmin, Fr, T,
  * PTSX, PTSY) and the constants of HighOrder/main.c:55-61 (mass, aa, ss,
@@ -107,6 +119,7 @@ typedef struct bhr_info {
   size_t device_bytes;
   int tile_rows;      /* stage tile height the autotuner chose (8 or 16)   */
   int persistent;     /* 1: persistent stage kernels (one block per SM)      */
+  int tiling;         /* bhr_tiling: the stage kernels this solve runs       */
 } bhr_info;
 
 typedef struct bhr_solver bhr_solver;

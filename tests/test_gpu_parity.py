@@ -167,6 +167,7 @@ def test_every_stage_tiling_matches_oracle(tiling, monkeypatch):
     monkeypatch.setenv("BHR_STAGE_TILING", tiling)
     s, o, rows, coef = traj_pair(1024, 64, -50.0, 50.0, 0.7, 2.0, ext_col=640)
     info = s.info()
+    assert info["tiling"] == tiling
     assert info["persistent"] == (tiling in ("persistent", "ring"))
     assert info["tile_rows"] == (8 if tiling in ("block8", "block8n", "ring") else 16)
     n = 120

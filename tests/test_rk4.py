@@ -116,7 +116,7 @@ def test_rk4_every_stage_tiling_matches_oracle(tiling, monkeypatch):
     N, M, Xmin, Xmax = 1024, 64, -50.0, 50.0
     s, o = gpu_pair(N, M, Xmin, Xmax, 0.6, 2.0, 0.25 * (Xmax - Xmin) / N, Fr=5, ext_col=700)
     info = s.info()
-    assert info["persistent"] == (tiling in ("persistent", "ring"))
+    assert info["tiling"] == tiling and info["persistent"] == (tiling in ("persistent", "ring"))
     for k in (1, 9, 30):
         s.step(k)
         o.step(k)
