@@ -72,16 +72,18 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per stage-kernel launch per grid point from the committed
-    ncu summary, if there is one (profiles/stage_kernel_plunge8192x128.txt,
-    line 'dram_bytes_per_point_per_step: X')."""
-    path = os.path.join(ROOT, "profiles", "stage_kernel_plunge8192x128.txt")
+def profile_traffic(workload):
+    """DRAM bytes per grid point of one step's three stage launches, from the
+    committed ncu summary of this workload (line
+    'dram_bytes_per_point_per_step: X'), or None."""
+    name = {"plunge": "stage_kernel_plunge8192x128.txt", "grid16k": "stage_dram_grid16384x256.txt"}.get(workload)
+    if name is None:
+        return None
     try:
-        for line in open(path):
+        for line in open(os.path.join(ROOT, "profiles", name)):
             if line.startswith("dram_bytes_per_point_per_step:"):
                 return float(line.split(":")[1])
-    except Exception:
+    except OSError:
         pass
     return None
 
@@ -241,7 +243,7 @@ def run_ours(args, rank, local_rank, world):
     bytes_pt = (BYTES_PER_PT_MIXED if PRECISION == "mixed" else
                 BYTES_PER_PT_RK4 if INTEGRATOR == "rk4" else BYTES_PER_PT)
     achieved = bytes_pt * N * M / (float(stage_ms.sum()) / 1e3) / 1e9
-    traffic_pp = profile_traffic()
+    traffic_pp = profile_traffic(args.workload) if PRECISION == "fp64" and INTEGRATOR == "ssprk3" else None
 
     # End to end through the public API: host params + host trajectory in,
     # solver set-up (grid, tables, initial data uploaded), n steps, waveform

@@ -84,7 +84,8 @@ size_t solve_bytes(const bhr_params &p, int traj_rows) {
 struct bhr_engine {
   int device = 0;
   size_t budget = 0;
-  int rows = 16;
+  int tiling = kTilingRing;  // stage tiling of the FP64 kernels (bhr_tiling values)
+  int rows = 8;              // its tile height: every solve's tensor maps use it
   cudaStream_t stream = nullptr;
   // Requests and the worker (lock wmu): the queue, solves being prepared,
   // prepared solves waiting to join, finished solves waiting to be
@@ -114,8 +115,10 @@ struct bhr_engine {
   SourceArgs *d_src = nullptr;
   MixedBatch *d_mixed = nullptr;  // mixed-precision solves' stage 2/3 tables
   int cap_solves = 0, cap_tiles = 0, ntiles = 0, nsrc = 0, max_ptsx = 1, max_ptsy = 1;
-  int ntiles64 = 0;  // tiles of FP64 solves, first in the work-list; mixed solves' tiles follow
-  int persist = 1;          // persistent stage kernels over the work-list
+  // The work-list: FP64 solves' tiles (ntiles64), then mixed solves' tiles
+  // of the same height for their FP64 stage 1 (up to ntiles1), then mixed
+  // solves' kMixTileRows-high tiles for the FP32 stages 2 and 3 (nmix).
+  int ntiles64 = 0, ntiles1 = 0, nmix = 0;
   int *d_err = nullptr;     // BHR_TIMEOUT from a bounded wait in a stage kernel
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -158,11 +161,10 @@ int enqueue_batch_step(bhr_engine *e) {
   // tiles through the FP64 kernels and mixed solves' tiles through the
   // FP32 ones.
   for (int stage = 1; stage <= 3; stage++) {
-    const int n64 = stage == 1 ? e->ntiles : e->ntiles64;
-    cudaError_t err =
-        launch_stage_batch(stage, e->rows, e->persist, e->d_solves, e->d_tiles, n64, e->d_err, e->stream);
-    if (err == cudaSuccess && stage > 1 && e->ntiles > e->ntiles64)
-      err = launch_mixed_batch(stage, e->d_mixed, e->d_tiles + e->ntiles64, e->ntiles - e->ntiles64, e->stream);
+    const int n64 = stage == 1 ? e->ntiles1 : e->ntiles64;
+    cudaError_t err = launch_stage_batch(stage, e->tiling, e->d_solves, e->d_tiles, n64, e->d_err, e->stream);
+    if (err == cudaSuccess && stage > 1 && e->nmix > 0)
+      err = launch_mixed_batch(stage, e->d_mixed, e->d_tiles + e->ntiles1, e->nmix, e->stream);
     if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("stage batch: ") + cudaGetErrorString(err));
   }
   cudaError_t err = launch_extract_batch(e->d_ext, n, e->stream);
@@ -180,11 +182,11 @@ int rebuild(bhr_engine *e) {
   }
   e->dirty = false;
   if (n == 0) {
-    e->ntiles = 0;
+    e->ntiles = e->ntiles64 = e->ntiles1 = e->nmix = 0;
     return BHR_OK;
   }
   std::vector<BatchSolve> solves(n);
-  std::vector<BatchTile> tiles, mtiles;
+  std::vector<BatchTile> tiles, m1tiles, mtiles;
   std::vector<ExtractArgs> ext(n);
   std::vector<SourceArgs> src;
   std::vector<MixedBatch> mixed;
@@ -213,9 +215,12 @@ int rebuild(bhr_engine *e) {
       mix_index = static_cast<int>(mixed.size());
       mixed.push_back(X);
     }
-    std::vector<BatchTile> &dst = s->mixed ? mtiles : tiles;
+    std::vector<BatchTile> &dst = s->mixed ? m1tiles : tiles;
     for (int b0 = 0; b0 < s->p.M; b0 += e->rows)
       for (int c0 = 0; c0 < s->p.N; c0 += TC) dst.push_back({i, c0, b0, mix_index});
+    if (s->mixed)
+      for (int b0 = 0; b0 < s->p.M; b0 += kMixTileRows)
+        for (int c0 = 0; c0 < s->p.N; c0 += TC) mtiles.push_back({i, c0, b0, mix_index});
     ext[i] = solver_extract_args(s);
     ext[i].set_ks = 1;  // stages and extraction run in sequence here
     if (s->has_source) {
@@ -227,7 +232,10 @@ int rebuild(bhr_engine *e) {
   // Blocks are ordered solve by solve, row block by row block, FP64 solves
   // first.
   e->ntiles64 = static_cast<int>(tiles.size());
+  tiles.insert(tiles.end(), m1tiles.begin(), m1tiles.end());
+  e->ntiles1 = static_cast<int>(tiles.size());
   tiles.insert(tiles.end(), mtiles.begin(), mtiles.end());
+  e->nmix = static_cast<int>(mtiles.size());
   e->ntiles = static_cast<int>(tiles.size());
   e->nsrc = static_cast<int>(src.size());
   // The per-solve tables share one capacity; the work-list has its own.
@@ -444,8 +452,14 @@ int bhr_engine_create(int device, size_t hbm_budget_bytes, bhr_engine **out) {
     delete e;
     return set_fail(BHR_CUDA_ERROR, "engine set-up failed");
   }
-  // BHR_ENGINE_TILING=block selects the one-tile-per-block stage kernels.
-  if (const char *v = std::getenv("BHR_ENGINE_TILING")) e->persist = std::strcmp(v, "block") != 0;
+  // BHR_ENGINE_TILING=block8|block16|persistent|block8n|ring selects the
+  // FP64 stage kernels over the work-list (default ring).
+  if (const char *v = std::getenv("BHR_ENGINE_TILING")) {
+    static const char *names[] = {"block8", "block16", "persistent", "block8n", "ring"};
+    for (int t = 0; t < 5; t++)
+      if (!std::strcmp(v, names[t])) e->tiling = t;
+  }
+  e->rows = tiling_rows(e->tiling);
   e->worker = std::thread(worker_loop, e);
   *out = e;
   return BHR_OK;

@@ -180,7 +180,14 @@ cudaError_t encode_coef_maps(double *ctab, const double *coltab, const double *r
 cudaError_t launch_source(const SourceArgs &a, cudaStream_t st);
 // persist = 1 walks the work-list with one block per SM (16-row tiles);
 // err receives BHR_TIMEOUT if a bounded wait gives up.
-cudaError_t launch_stage_batch(int stage, int rows, int persist, const BatchSolve *solves, const BatchTile *tiles,
+// Stage tilings (the values of bhr_tiling): kernels and tile heights.
+enum StageTiling { kTilingBlock8 = 0, kTilingBlock16 = 1, kTilingPersistent = 2, kTilingBlock8n = 3, kTilingRing = 4 };
+constexpr int tiling_rows(int tiling) {
+  return (tiling == kTilingBlock8 || tiling == kTilingBlock8n || tiling == kTilingRing) ? 8 : 16;
+}
+// Tile height of the mixed-precision FP32 stage kernels.
+constexpr int kMixTileRows = 16;
+cudaError_t launch_stage_batch(int stage, int tiling, const BatchSolve *solves, const BatchTile *tiles,
                                int ntiles, int *err, cudaStream_t st);
 cudaError_t launch_source_batch(const SourceArgs *args, int nsolves, int max_ptsy, int max_ptsx, cudaStream_t st);
 cudaError_t launch_extract_batch(const ExtractArgs *args, int nsolves, cudaStream_t st);

@@ -663,6 +663,22 @@ __global__ void __launch_bounds__(kPersistThreads, 1)
   stage_persistent<STAGE, kPersistRows, kPersistThreads, 2, true>(W, err);
 }
 
+// The 8-row tilings over a batch work-list (tiles of 8 rows).
+template <int STAGE>
+__global__ void __launch_bounds__(kRingThreads, kRingBlocksPerSM)
+    stage_ring_batch_kernel(const BatchSolve *solves, const BatchTile *tiles, int ntiles, int *err) {
+  BatchWork<STAGE> W{solves, tiles, ntiles};
+  stage_persistent<STAGE, kRingRows, kRingThreads, kRingBufs, false>(W, err);
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(kNarrowThreads, 4)
+    stage_narrow_batch_kernel(const BatchSolve *solves, const BatchTile *tiles) {
+  const BatchTile t = tiles[blockIdx.x];
+  const BatchSolve &B = solves[t.solve];
+  stage_tile<STAGE, 8, kNarrowThreads>(B.maps[STAGE - 1], B.args[STAGE - 1], t.c0, t.b0);
+}
+
 // ---- closure of stored planes (HighOrder/kern.cu:622-753) ------------------
 __device__ __forceinline__ double pole_val(const double *P, int N, int M, int even, int b, int a) {
   if (b >= 3 && b < M - 3) return P[static_cast<size_t>(b) * N + a];
@@ -1085,7 +1101,9 @@ cudaError_t prepare_kernels() {
       if constexpr (S <= 3) {  // the batch engine steps SSP-RK3 only
         if ((r = cudaFuncSetAttribute(stage_batch_kernel<S, 8>, kSmem, s8)) ||
             (r = cudaFuncSetAttribute(stage_batch_kernel<S, 16>, kSmem, s16)) ||
-            (r = cudaFuncSetAttribute(stage_persistent_batch_kernel<S>, kSmem, sp)))
+            (r = cudaFuncSetAttribute(stage_persistent_batch_kernel<S>, kSmem, sp)) ||
+            (r = cudaFuncSetAttribute(stage_narrow_batch_kernel<S>, kSmem, s8)) ||
+            (r = cudaFuncSetAttribute(stage_ring_batch_kernel<S>, kSmem, sr)))
           return r;
       }
       return cudaSuccess;
@@ -1095,27 +1113,30 @@ cudaError_t prepare_kernels() {
   return cudaSuccess;
 }
 
-cudaError_t launch_stage_batch(int stage, int rows, int persist, const BatchSolve *solves, const BatchTile *tiles,
-                               int ntiles, int *err, cudaStream_t st) {
+cudaError_t launch_stage_batch(int stage, int tiling, const BatchSolve *solves, const BatchTile *tiles, int ntiles,
+                               int *err, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
-  if (persist) {
-    const dim3 grid(std::min(ntiles, sm_count())), block(32, kPersistThreads / 32);
-    const size_t smem = persist_smem_bytes();
-    if (stage == 1) return launch_pdl(stage_persistent_batch_kernel<1>, grid, block, smem, st, solves, tiles, ntiles, err);
-    if (stage == 2) return launch_pdl(stage_persistent_batch_kernel<2>, grid, block, smem, st, solves, tiles, ntiles, err);
-    return launch_pdl(stage_persistent_batch_kernel<3>, grid, block, smem, st, solves, tiles, ntiles, err);
-  }
-  const dim3 grid(ntiles), block(32, STAGE_THREADS / 32);
-  if (rows == 8) {
-    const size_t smem = sizeof(StageSmem<8>) + 128;
-    if (stage == 1) return launch_pdl(stage_batch_kernel<1, 8>, grid, block, smem, st, solves, tiles);
-    if (stage == 2) return launch_pdl(stage_batch_kernel<2, 8>, grid, block, smem, st, solves, tiles);
-    return launch_pdl(stage_batch_kernel<3, 8>, grid, block, smem, st, solves, tiles);
-  }
-  const size_t smem = sizeof(StageSmem<16>) + 128;
-  if (stage == 1) return launch_pdl(stage_batch_kernel<1, 16>, grid, block, smem, st, solves, tiles);
-  if (stage == 2) return launch_pdl(stage_batch_kernel<2, 16>, grid, block, smem, st, solves, tiles);
-  return launch_pdl(stage_batch_kernel<3, 16>, grid, block, smem, st, solves, tiles);
+  if (stage < 1 || stage > 3) return cudaErrorInvalidValue;
+  return by_stage(stage, [&](auto sc) {
+    constexpr int S = decltype(sc)::value < 4 ? decltype(sc)::value : 1;
+    switch (tiling) {
+      case kTilingPersistent:
+        return launch_pdl(stage_persistent_batch_kernel<S>, dim3(std::min(ntiles, sm_count())),
+                          dim3(32, kPersistThreads / 32), persist_smem_bytes(), st, solves, tiles, ntiles, err);
+      case kTilingRing:
+        return launch_pdl(stage_ring_batch_kernel<S>, dim3(std::min(ntiles, kRingBlocksPerSM * sm_count())),
+                          dim3(32, kRingThreads / 32), ring_smem_bytes(), st, solves, tiles, ntiles, err);
+      case kTilingBlock8n:
+        return launch_pdl(stage_narrow_batch_kernel<S>, dim3(ntiles), dim3(32, kNarrowThreads / 32),
+                          sizeof(StageSmem<8>) + 128, st, solves, tiles);
+      case kTilingBlock8:
+        return launch_pdl(stage_batch_kernel<S, 8>, dim3(ntiles), dim3(32, STAGE_THREADS / 32),
+                          sizeof(StageSmem<8>) + 128, st, solves, tiles);
+      default:
+        return launch_pdl(stage_batch_kernel<S, 16>, dim3(ntiles), dim3(32, STAGE_THREADS / 32),
+                          sizeof(StageSmem<16>) + 128, st, solves, tiles);
+    }
+  });
 }
 
 cudaError_t launch_source_batch(const SourceArgs *args, int nsolves, int max_ptsy, int max_ptsx, cudaStream_t st) {

@@ -24,7 +24,7 @@
 namespace bhr {
 namespace {
 
-constexpr int kMixRows = 16;
+constexpr int kMixRows = kMixTileRows;
 constexpr int kMixThreads = 256;
 
 // Every TMA destination starts on a 128-byte boundary.

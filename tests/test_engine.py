@@ -137,6 +137,29 @@ def test_mixed_precision_requests_in_a_mixed_batch():
         assert np.linalg.norm(h - hs) <= WAVE_TOL * np.linalg.norm(hs)
 
 
+@pytest.mark.parametrize("tiling", ["block8", "block16", "persistent", "block8n", "ring"])
+def test_every_engine_tiling(tiling, monkeypatch):
+    """Each FP64 stage tiling over the work-list, with FP64 and mixed-precision
+    requests in one batch (mixed solves run their FP64 stage 1 on the
+    tiling's tiles and the FP32 stages on 16-row tiles): every result within
+    the FP64 bar of a lone solver on the same request."""
+    monkeypatch.setenv("BHR_ENGINE_TILING", tiling)
+    reqs = requests()
+    reqs[1][0].precision = bhr.BHR_MIXED
+    with bhr.Engine() as e:
+        ids = [e.submit(p, t) for p, t in reqs]
+        e.run_all()
+        got = [e.result(i) for i in ids]
+    for (prm, traj), (t, h, _) in zip(reqs, got):
+        with bhr.Solver(prm) as s:
+            if traj is not None:
+                s.set_trajectory(traj)
+            s.run()
+            ts, hs, _ = s.waveform()
+        assert np.array_equal(t, ts) and np.max(np.abs(hs)) > 1e-8
+        assert np.linalg.norm(h - hs) <= WAVE_TOL * np.linalg.norm(hs)
+
+
 def test_engine_matches_lone_solver():
     for prm, traj in requests():
         s = bhr.Solver(prm)
