@@ -367,8 +367,11 @@ void worker_loop(bhr_engine *e) {
     r.p.device = e->device;
     bhr_solver *s = nullptr;
     int st = solver_create(&r.p, e->rows, &s);
-    if (st == BHR_OK && !r.traj.empty())
+    if (st == BHR_OK && !r.traj.empty()) {
       st = bhr_solver_set_trajectory(s, r.traj.data(), static_cast<int>(r.traj.size() / 10));
+      // batch steps read every step's record without waiting: all of them first
+      if (st == BHR_OK) st = solver_wait_records(s, s->nt);
+    }
     std::string msg;
     if (st != BHR_OK) {
       msg = bhr_last_error_string();

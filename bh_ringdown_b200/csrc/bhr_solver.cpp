@@ -13,6 +13,7 @@
 #include <array>
 #include <atomic>
 #include <thread>
+#include <memory>
 #include <mutex>
 #include <sstream>
 #include <string>
@@ -93,6 +94,10 @@ int dalloc(bhr_solver *s, T **ptr, size_t count) {
 }
 
 void free_all(bhr_solver *s) {
+  if (s->rec_thread.joinable()) {  // it writes into s->recs
+    s->rec_stop = true;
+    s->rec_thread.join();
+  }
   void *ptrs[] = {s->u0,    s->u1,   s->u2,     s->u3,     s->coltab, s->rowtab, s->ctab,   s->rc,     s->th,
                   s->src,   s->ext,  s->integ,  s->wproj,  s->wdedt,  s->rows,   s->recs,   s->rs,
                   s->d1f,   s->e2f,  s->colf32, s->rowf32, s->bbf};
@@ -394,6 +399,129 @@ int bhr_solver_info(const bhr_solver *s, bhr_info *info) {
   return BHR_OK;
 }
 
+}  // extern "C"
+
+// Steps whose source records set_trajectory builds before it returns; the
+// rest follow in chunks of kRecordChunk on a host thread.
+static constexpr int kFirstRecords = 8192;
+static constexpr int kRecordChunk = 16384;
+
+// What the records of a trajectory are built from.
+struct RecordJob {
+  bhr_params p;
+  double dx, dtheta, rpl, rmn;
+  std::vector<bhr_particle> pts;  // particle state of every step
+  std::vector<double> turn;       // turn-on window of every step
+};
+
+// Records of steps [k0, k1) into out[0 .. k1-k0) on all host threads:
+// source coefficients times the turn-on window, radial width and patch
+// origin.  Returns the first step whose particle is off the grid, inside
+// the horizon or on a pole (its status in *bad_status), or -1.
+static int build_records(const RecordJob &J, int k0, int k1, StepRec *out, int *bad_status) {
+  const bhr_params &p = J.p;
+  std::mutex bad_mu;
+  int first_bad = -1, status = BHR_OK;
+  auto work = [&](int a0, int a1) {
+    for (int k = a0; k < a1; k++) {
+      const bhr_particle &pt = J.pts[k];
+      StepRec &R = out[k - k0];
+      double cr[6], ci[6];
+      const int st = bhr_source_coefficients(&pt, p.a, p.mass, p.m, cr, ci);
+      const double xp = tortoise(pt.rp, p.a, J.rpl, J.rmn);
+      const double ipd = (xp - p.Xmin) / J.dx, itd = pt.tp / J.dtheta;
+      if (st != BHR_OK || !std::isfinite(ipd) || !std::isfinite(itd) || std::fabs(ipd) > 1e9 ||
+          std::fabs(itd) > 1e9) {
+        std::lock_guard<std::mutex> lock(bad_mu);  // keep the earliest bad step
+        if (first_bad < 0 || k < first_bad) {
+          first_bad = k;
+          status = st != BHR_OK ? st : BHR_INVALID_ARG;
+        }
+        return;
+      }
+      for (int i = 0; i < 6; i++) {
+        R.c_re[i] = cr[i] * J.turn[k];
+        R.c_im[i] = ci[i] * J.turn[k];
+      }
+      R.rp = pt.rp;
+      R.tp = pt.tp;
+      R.wr = p.wr_fac * J.dx * (1.0 - J.rpl / pt.rp);
+      R.col0 = static_cast<int>(ipd) - p.PTSX / 2;
+      R.row0 = static_cast<int>(itd) - p.PTSY / 2;
+    }
+  };
+  const int n = k1 - k0;
+  const int nth = std::max(1, std::min(64, static_cast<int>(std::thread::hardware_concurrency())));
+  if (n < 2048 || nth == 1) {
+    work(k0, k1);
+  } else {
+    std::vector<std::thread> pool;
+    const int chunk = (n + nth - 1) / nth;
+    for (int t = 0; t < nth; t++) {
+      const int a0 = k0 + t * chunk, a1 = std::min(k1, a0 + chunk);
+      if (a0 < a1) pool.emplace_back(work, a0, a1);
+    }
+    for (auto &th : pool) th.join();
+  }
+  *bad_status = status;
+  return first_bad;
+}
+
+// Host thread: records of steps [k_from, nt) chunk by chunk, each uploaded
+// (on its own stream, waited for) before it is published to stepping.
+static void record_worker(bhr_solver *s, std::shared_ptr<RecordJob> job, int k_from) {
+  cudaSetDevice(job->p.device);
+  cudaStream_t up = nullptr;
+  const bool ok_stream = cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking) == cudaSuccess;
+  std::vector<StepRec> buf(kRecordChunk);
+  for (int k0 = k_from; k0 < s->nt && !s->rec_stop.load(); k0 += kRecordChunk) {
+    const int k1 = std::min(s->nt, k0 + kRecordChunk);
+    int status = BHR_OK;
+    int bad = build_records(*job, k0, k1, buf.data(), &status);
+    if (bad < 0 && (!ok_stream ||
+                    cudaMemcpyAsync(s->recs + k0, buf.data(), sizeof(StepRec) * (k1 - k0), cudaMemcpyHostToDevice,
+                                    up) != cudaSuccess ||
+                    cudaStreamSynchronize(up) != cudaSuccess)) {
+      bad = k0;
+      status = BHR_CUDA_ERROR;
+    }
+    std::lock_guard<std::mutex> lock(s->rec_mu);
+    if (bad >= 0) {
+      s->rec_bad = bad;
+      s->rec_status = status;
+      s->rec_cv.notify_all();
+      break;
+    }
+    s->rec_ready = k1;
+    s->rec_cv.notify_all();
+  }
+  if (up) cudaStreamDestroy(up);
+}
+
+// Stops and joins a record thread (before its records are freed or replaced).
+static void stop_records(bhr_solver *s) {
+  if (!s->rec_thread.joinable()) return;
+  s->rec_stop = true;
+  s->rec_thread.join();
+  s->rec_stop = false;
+}
+
+int bhr::solver_wait_records(bhr_solver *s, int upto) {
+  if (!s->has_source) return BHR_OK;
+  upto = std::min(upto, s->nt);
+  std::unique_lock<std::mutex> lock(s->rec_mu);
+  s->rec_cv.wait(lock, [&] { return s->rec_ready >= upto || (s->rec_bad >= 0 && s->rec_bad < upto); });
+  if (s->rec_bad >= 0 && s->rec_bad < upto) {
+    set_error("trajectory step " + std::to_string(s->rec_bad) +
+              (s->rec_status == BHR_CUDA_ERROR ? ": record upload failed"
+                                               : ": particle off the grid, inside the horizon or on a pole"));
+    return s->rec_status;
+  }
+  return BHR_OK;
+}
+
+extern "C" {
+
 // HighOrder/body.cu:97-124: the pre-loop reads one line and then lines
 // until ptime >= timer; each step reads two lines and uses the second; a
 // read past the end leaves the particle variables unchanged; rp gets
@@ -406,10 +534,10 @@ int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows) {
   }
   cudaSetDevice(s->p.device);
   if (int st = flush_extract(s)) return st;
+  stop_records(s);
   const bhr_params &p = s->p;
   const double a = p.a, mass = p.mass;
   const double rpl = mass + std::sqrt(mass * mass - a * a), rmn = mass - std::sqrt(mass * mass - a * a);
-  std::vector<StepRec> recs(s->nt);
   double row[10] = {0};
   int cursor = 0;
   auto rd = [&]() {
@@ -456,57 +584,38 @@ int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows) {
     timer += p.dt;
   }
   // Independent per step: source coefficients, width and patch origin,
-  // evaluated on all host threads.
-  std::atomic<int> first_bad{-1};
-  std::atomic<int> bad_status{BHR_OK};
-  auto work = [&](int k0, int k1) {
-    for (int k = k0; k < k1; k++) {
-      const bhr_particle &pt = pts[k];
-      StepRec &R = recs[k];
-      double cr[6], ci[6];
-      const int st = bhr_source_coefficients(&pt, a, mass, p.m, cr, ci);
-      const double xp = tortoise(pt.rp, a, rpl, rmn);
-      const double ipd = (xp - p.Xmin) / s->g.dx, itd = pt.tp / s->g.dtheta;
-      if (st != BHR_OK || !std::isfinite(ipd) || !std::isfinite(itd) || std::fabs(ipd) > 1e9 ||
-          std::fabs(itd) > 1e9) {
-        int expect = -1;
-        if (first_bad.compare_exchange_strong(expect, k)) bad_status = st != BHR_OK ? st : BHR_INVALID_ARG;
-        return;
-      }
-      for (int i = 0; i < 6; i++) {
-        R.c_re[i] = cr[i] * turn[k];
-        R.c_im[i] = ci[i] * turn[k];
-      }
-      R.rp = pt.rp;
-      R.tp = pt.tp;
-      R.wr = p.wr_fac * s->g.dx * (1.0 - rpl / pt.rp);
-      R.col0 = static_cast<int>(ipd) - p.PTSX / 2;
-      R.row0 = static_cast<int>(itd) - p.PTSY / 2;
-    }
-  };
-  const int nth = std::max(1, std::min(64, static_cast<int>(std::thread::hardware_concurrency())));
-  if (s->nt < 4096 || nth == 1) {
-    work(0, s->nt);
-  } else {
-    std::vector<std::thread> pool;
-    const int chunk = (s->nt + nth - 1) / nth;
-    for (int t = 0; t < nth; t++) {
-      const int k0 = t * chunk, k1 = std::min(s->nt, k0 + chunk);
-      if (k0 < k1) pool.emplace_back(work, k0, k1);
-    }
-    for (auto &th : pool) th.join();
-  }
-  if (first_bad.load() >= 0) {
-    set_error("trajectory step " + std::to_string(first_bad.load()) +
-              ": particle off the grid, inside the horizon or on a pole");
-    return bad_status.load();
+  // evaluated on all host threads.  The first chunk of steps is built here;
+  // the rest on a host thread while the device steps (solver_wait_records
+  // holds stepping back until the records it reaches are uploaded).
+  auto job = std::make_shared<RecordJob>();
+  job->p = p;
+  job->dx = s->g.dx;
+  job->dtheta = s->g.dtheta;
+  job->rpl = rpl;
+  job->rmn = rmn;
+  job->pts = std::move(pts);
+  job->turn = std::move(turn);
+  const int k_first = std::min(s->nt, kFirstRecords);
+  std::vector<StepRec> recs(static_cast<size_t>(std::max(1, k_first)));
+  int bad_status = BHR_OK;
+  const int bad = build_records(*job, 0, k_first, recs.data(), &bad_status);
+  if (bad >= 0) {
+    set_error("trajectory step " + std::to_string(bad) + ": particle off the grid, inside the horizon or on a pole");
+    return bad_status;
   }
   cudaSetDevice(p.device);
   if (s->recs) cudaFreeAsync(s->recs, s->stream), s->bytes -= sizeof(StepRec) * static_cast<size_t>(s->nt ? s->nt : 1);
   s->recs = nullptr;
   if (int st = dalloc(s, &s->recs, static_cast<size_t>(s->nt))) return st;
-  BHR_CUDA_TRY(cudaMemcpyAsync(s->recs, recs.data(), sizeof(StepRec) * recs.size(), cudaMemcpyHostToDevice, s->stream));
+  BHR_CUDA_TRY(cudaMemcpyAsync(s->recs, recs.data(), sizeof(StepRec) * k_first, cudaMemcpyHostToDevice, s->stream));
   BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  {
+    std::lock_guard<std::mutex> lock(s->rec_mu);
+    s->rec_ready = k_first;
+    s->rec_bad = -1;
+    s->rec_status = BHR_OK;
+  }
+  if (k_first < s->nt) s->rec_thread = std::thread(record_worker, s, job, k_first);
   s->has_source = true;
   // The patch of the current step (later patches are built one step ahead).
   BHR_CUDA_TRY(launch_source(solver_source_args(s), s->stream));
@@ -885,6 +994,7 @@ int bhr_solver_step(bhr_solver *s, int nsteps) {
     set_error("stepping past the end of the trajectory records");
     return BHR_INVALID_ARG;
   }
+  if (int st = solver_wait_records(s, s->steps_done + nsteps + 1)) return st;
   if (int st = enqueue_steps(s, nsteps)) return st;
   return check_run_state(s);
 }
@@ -896,6 +1006,7 @@ int bhr_solver_time_steps(bhr_solver *s, int nsteps, double *ms) {
     set_error("stepping past the end of the trajectory records");
     return BHR_INVALID_ARG;
   }
+  if (int st = solver_wait_records(s, s->steps_done + nsteps + 1)) return st;
   if (!s->g1)
     if (int st = capture_steps(s, 1, &s->g1)) return st;
   if (nsteps >= kGraphBatch && !s->gb)
@@ -1077,6 +1188,7 @@ int bhr_solver_profile(bhr_solver *s, int nsteps, double *avg_ms5, double *total
     set_error("profiling past the end of the trajectory records");
     return BHR_INVALID_ARG;
   }
+  if (int st = solver_wait_records(s, s->steps_done + nsteps + 1)) return st;
   // Events bracket each launch of launch_step; the extraction and the
   // source run on the side stream beside the stages.
   std::vector<cudaEvent_t> ev(10 * static_cast<size_t>(nsteps));

@@ -2,6 +2,11 @@
 // and the batch engine (bhr_engine.cpp).  Not part of the public ABI.
 #pragma once
 
+#include <atomic>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
+
 #include "bhr.h"
 #include "bhr_host.h"
 #include "bhr_internal.h"
@@ -45,6 +50,16 @@ struct bhr_solver {
   bool pending_extract = false;
   // Captured step graphs: one step, and kGraphBatch steps in one launch.
   cudaGraphExec_t g1 = nullptr, gb = nullptr;
+  // Per-step source records past the first chunk are built and uploaded by
+  // a host thread after set_trajectory returns; stepping waits for the
+  // steps it reaches (lock rec_mu).
+  std::thread rec_thread;
+  std::mutex rec_mu;
+  std::condition_variable rec_cv;
+  std::atomic<bool> rec_stop{false};
+  int rec_ready = 0;                // records on the device: steps [0, rec_ready)
+  int rec_bad = -1;                 // first step whose record failed, or -1
+  int rec_status = 0;               // its status
 };
 
 
@@ -58,4 +73,7 @@ StageArgs solver_stage_args(bhr_solver *s);
 SourceArgs solver_source_args(bhr_solver *s);
 ExtractArgs solver_extract_args(bhr_solver *s);
 MixedArgs solver_mixed_args(bhr_solver *s);
+// Waits until the source records of steps [0, upto) are on the device
+// (returns the status of a record that failed before upto).
+int solver_wait_records(bhr_solver *s, int upto);
 }  // namespace bhr

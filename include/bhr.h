@@ -136,7 +136,12 @@ int bhr_solver_info(const bhr_solver *s, bhr_info *info);
 
 /* Trajectory input: rows of the 10 .traj columns t r theta dr/dt dtheta/dt
  * dphi/dt phi E Lz Q (row-major, nrows x 10).  The data are copied in.
- * Replaces the fopen/fscanf consumption of HighOrder/body.cu:77,97-120. */
+ * Replaces the fopen/fscanf consumption of HighOrder/body.cu:77,97-120.
+ * The per-step source records of the first 8192 steps are built before
+ * this returns (a particle off the grid there is reported here); the rest
+ * are built on a host thread while the solver steps, and a step call that
+ * reaches a step whose particle is off the grid, inside the horizon or on a
+ * pole returns that error (BHR_INVALID_ARG) without launching. */
 int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows);
 int bhr_solver_load_trajectory(bhr_solver *s, const char *path);
 

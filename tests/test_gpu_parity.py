@@ -196,3 +196,28 @@ def test_trajectory_set_after_stepping(tiling, monkeypatch):
     assert rel_field_err(s2.get_state(), o.get_state()) <= FIELD_TOL
     s2.close()
     s.close()
+
+
+def test_long_trajectory_records_built_while_stepping():
+    """A trajectory longer than the source records built up front (8192
+    steps): the rest are built on a host thread while the solver steps.  The
+    waveform over 12000 steps, past the first chunk boundary, matches the
+    oracle, which forms every step's source itself."""
+    from bh_ringdown_b200.trajectory import synthetic_plunge
+    from tests.test_source import product_coef_fn
+    N, M, Xmin, Xmax, a = 256, 32, -50.0, 50.0, 0.6
+    dt = 0.25 * (Xmax - Xmin) / N
+    prm = bhr.Params(N=N, M=M, Xmin=Xmin, Xmax=Xmax, a=a, m=2.0, dt=dt, Fr=50, T=1500.0, out_start=0.0,
+                     ext_col=154)
+    rows = synthetic_plunge(a, dt / 2.0, duration=200.0)
+    n = 12000
+    with bhr.Solver(prm) as s:
+        s.set_trajectory(rows)
+        s.step(n)                            # races the record thread
+        ts, hs, _ = s.waveform()
+        gs = s.get_state()
+    o = pyoracle.Oracle(N, M, Xmin, Xmax, a, 2.0, dt, T=1500.0, Fr=50, out_start=0.0, ext_col=154)
+    t, h, _, _, _, _ = o.run(traj=rows, coef_fn=product_coef_fn(), nsteps=n)
+    assert len(ts) == n // 50 and np.array_equal(ts, t) and np.max(np.abs(h)) > 0
+    assert np.linalg.norm(hs - h) <= WAVE_TOL * np.linalg.norm(h)
+    assert rel_field_err(gs, o.get_state()) <= 1e-9  # 12000 steps of rounding
