@@ -310,8 +310,6 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
           sim = srcp[static_cast<size_t>(A.PTSY + sr) * A.PTSX + sc];
         }
       }
-      res[0][c] = 0.0;
-      res[1][c] = 0.0;
       res[2][c] = fma(cc, ll[0][c], sre);
       res[3][c] = fma(cc, ll[1][c], sim);
     }
@@ -337,23 +335,24 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
         const double fx = d1c(v, 4 + c) * A.cx;
         const double fk = (inner || (a >= 4 && a < N - 4)) ? ko8c(v, 4 + c) * A.cko : 0.0;
         fc[pl][c] = f0;
-        // each plane's contribution is formed on its own, then added once
+        // each term folded into its accumulator by one FMA (res[0] and
+        // res[1] start with the q planes' terms)
         if (pl == 0) {         // q_re
-          res[0][c] += fma(-kbb[c], fx, -fk);
-          res[2][c] += fma(kdre[c], fx, -kvre[c] * f0);
-          res[3][c] += fma(kdim[c], fx, -kvim[c] * f0);
+          res[0][c] = fma(-kbb[c], fx, -fk);
+          res[2][c] = fma(kdre[c], fx, fma(-kvre[c], f0, res[2][c]));
+          res[3][c] = fma(kdim[c], fx, fma(-kvim[c], f0, res[3][c]));
         } else if (pl == 1) {  // q_im
-          res[1][c] += fma(-kbb[c], fx, -fk);
-          res[2][c] += fma(-kdim[c], fx, kvim[c] * f0);
-          res[3][c] += fma(kdre[c], fx, -kvre[c] * f0);
+          res[1][c] = fma(-kbb[c], fx, -fk);
+          res[2][c] = fma(-kdim[c], fx, fma(kvim[c], f0, res[2][c]));
+          res[3][c] = fma(kdre[c], fx, fma(-kvre[c], f0, res[3][c]));
         } else if (pl == 2) {  // p_re
           res[0][c] += f0;
-          res[2][c] += fma(kee[c], fx, fma(-kare[c], f0, -fk));
-          res[3][c] += -kaim[c] * f0;
+          res[2][c] = fma(kee[c], fx, fma(-kare[c], f0, res[2][c] - fk));
+          res[3][c] = fma(-kaim[c], f0, res[3][c]);
         } else {               // p_im
           res[1][c] += f0;
-          res[2][c] += kaim[c] * f0;
-          res[3][c] += fma(kee[c], fx, fma(-kare[c], f0, -fk));
+          res[2][c] = fma(kaim[c], f0, res[2][c]);
+          res[3][c] = fma(kee[c], fx, fma(-kare[c], f0, res[3][c] - fk));
         }
       }
     }
