@@ -126,6 +126,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     dp = P(D)
     sigs = {
         "bhr_abi_version": (I, []),
+        "bhr_selftest_bounded_wait": (I, [I, C.POINTER(I)]),
         "bhr_last_error_string": (C.c_char_p, []),
         "bhr_params_default": (I, [P(_Params)]),
         "bhr_grid": (I, [P(_Params), dp, dp, dp]),
@@ -174,6 +175,14 @@ def _ptr(a: Optional[np.ndarray]):
 def _check(st: int):
     if st != BHR_OK:
         raise BhrError(st, load_library().bhr_last_error_string().decode(errors="replace"))
+
+
+def selftest_bounded_wait(device: int = 0) -> int:
+    """Runs the device self-check of the bounded waits; returns the status
+    the kernel reported (BHR_TIMEOUT when the wait gave up as designed)."""
+    st = I(0)
+    _check(load_library().bhr_selftest_bounded_wait(device, C.byref(st)))
+    return st.value
 
 
 def grid(params: Params):

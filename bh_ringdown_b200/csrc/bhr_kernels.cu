@@ -1160,6 +1160,26 @@ cudaError_t launch_extract(const ExtractArgs &a, cudaStream_t st) {
   return launch_pdl(extract_kernel, dim3(1), dim3(kExtractThreads), 0, st, a);
 }
 
+// Self-check of the bounded barrier wait every stage kernel uses: one block
+// waits on an mbarrier that nothing completes; the wait gives up after its
+// iteration limit and the kernel returns BHR_TIMEOUT (5) in *status instead
+// of spinning forever.
+__global__ void wait_selftest_kernel(int *status) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const bool ok = mbar_wait_bounded(&bar, 0);
+  if (threadIdx.x == 0) *status = ok ? 0 : 5;
+}
+
+cudaError_t launch_wait_selftest(int *status, cudaStream_t st) {
+  wait_selftest_kernel<<<1, 32, 0, st>>>(status);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_closure(double *planes, int N, int M, int even_m, cudaStream_t st) {
   closure_poles_kernel<<<dim3((N + 127) / 128, 4), 128, 0, st>>>(planes, N, M, even_m);
   closure_ends_kernel<<<dim3((M + 127) / 128, 4), 128, 0, st>>>(planes, N, M);

@@ -152,6 +152,33 @@ static int flush_extract(bhr_solver *s);
 extern "C" {
 
 int bhr_abi_version(void) { return BHR_ABI_VERSION; }
+
+int bhr_selftest_bounded_wait(int device, int *device_status) {
+  if (!device_status) return BHR_INVALID_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    set_error("no CUDA device");
+    return BHR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) return BHR_INVALID_ARG;
+  BHR_CUDA_TRY(cudaSetDevice(device));
+  cudaStream_t st = nullptr;
+  int *d = nullptr;
+  BHR_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&d), sizeof(int), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = launch_wait_selftest(d, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(device_status, d, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (d) cudaFreeAsync(d, st);
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  if (e != cudaSuccess) {
+    set_error(std::string("wait self-check: ") + cudaGetErrorString(e));
+    return BHR_CUDA_ERROR;
+  }
+  return BHR_OK;
+}
 const char *bhr_last_error_string(void) { return g_err.c_str(); }
 double bhr_swsh(double ell, double m, double theta) { return swsh(ell, m, theta); }
 

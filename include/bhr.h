@@ -264,6 +264,12 @@ int bhr_engine_result(bhr_engine *e, int64_t id, double *t, double *h, double *d
 int bhr_engine_stats(bhr_engine *e, bhr_engine_counters *st);
 
 const char *bhr_last_error_string(void);
+/* Device self-check of the bounded waits (no counterpart in the reference):
+ * one block waits on a shared-memory barrier that nothing completes; the
+ * wait gives up after its iteration limit (about a second) and the kernel
+ * returns normally with *device_status = BHR_TIMEOUT, the same path a stage
+ * kernel takes when its tile data never arrive.  The device stays usable. */
+int bhr_selftest_bounded_wait(int device, int *device_status);
 int bhr_abi_version(void);
 
 #ifdef __cplusplus
