@@ -142,6 +142,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "bhr_solver_set_state": (I, [vp, dp, dp, dp, dp]),
         "bhr_solver_get_extraction": (I, [vp, dp, dp, dp, dp, dp, dp]),
         "bhr_solver_get_source": (I, [vp, dp, dp]),
+        "bhr_solver_checkpoint_size": (C.c_size_t, [vp]),
+        "bhr_solver_checkpoint": (I, [vp, vp, C.c_size_t]),
+        "bhr_solver_restore": (I, [vp, vp, C.c_size_t]),
         "bhr_solver_stream": (vp, [vp]),
         "bhr_solver_profile": (I, [vp, I, dp, dp]),
         "bhr_solver_time_steps": (I, [vp, I, dp]),
@@ -301,6 +304,22 @@ class Solver:
         tre, tim = np.zeros(self.N * self.M), np.zeros(self.N * self.M)
         _check(self.lib.bhr_solver_get_source(self._h, _ptr(tre), _ptr(tim)))
         return tre.reshape(self.M, self.N), tim.reshape(self.M, self.N)
+
+    def checkpoint(self) -> bytes:
+        """The solve's resumable state (fields, extraction integrals, counters,
+        waveform rows so far) as bytes; see restore()."""
+        n = self.lib.bhr_solver_checkpoint_size(self._h)
+        if n == 0:
+            raise BhrError(3, "checkpoint size unavailable: " + self.lib.bhr_last_error_string().decode(errors="replace"))
+        buf = C.create_string_buffer(n)
+        _check(self.lib.bhr_solver_checkpoint(self._h, buf, n))
+        return buf.raw
+
+    def restore(self, data: bytes):
+        """Continues from a checkpoint of a solve with the same parameters
+        (and the same trajectory, when sourced)."""
+        buf = C.create_string_buffer(bytes(data), len(data))
+        _check(self.lib.bhr_solver_restore(self._h, buf, len(data)))
 
     def stream(self) -> int:
         return int(self.lib.bhr_solver_stream(self._h) or 0)

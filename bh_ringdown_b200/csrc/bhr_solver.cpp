@@ -1175,6 +1175,104 @@ int bhr_solver_get_extraction(bhr_solver *s, double *psi_re, double *psi_im, dou
   return BHR_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// Layout of a checkpoint: this header, then the four state planes (4 N M),
+// ext (2 M), integ (4 M) and nrow waveform rows (16 doubles each).
+struct CheckpointHeader {
+  char magic[8];  // "BHRCKPT1"
+  int N, M, nt, max_rows, steps_done, has_source;
+  RunState rs;
+  double dt, a, m;
+};
+constexpr char kCkptMagic[8] = {'B', 'H', 'R', 'C', 'K', 'P', 'T', '1'};
+
+size_t checkpoint_bytes(const bhr_solver *s, int nrow) {
+  const size_t NM = static_cast<size_t>(s->p.N) * s->p.M;
+  return sizeof(CheckpointHeader) + 8 * (4 * NM + 6 * static_cast<size_t>(s->p.M) + 16 * static_cast<size_t>(nrow));
+}
+}  // namespace
+
+extern "C" {
+
+size_t bhr_solver_checkpoint_size(bhr_solver *s) {
+  if (!s) return 0;
+  cudaSetDevice(s->p.device);
+  if (flush_extract(s)) return 0;
+  RunState rs{};
+  if (cudaMemcpyAsync(&rs, s->rs, sizeof(rs), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+      cudaStreamSynchronize(s->stream) != cudaSuccess)
+    return 0;
+  return checkpoint_bytes(s, rs.nrow);
+}
+
+int bhr_solver_checkpoint(bhr_solver *s, void *buf, size_t size) {
+  if (!s || !buf) return BHR_INVALID_ARG;
+  BHR_CUDA_TRY(cudaSetDevice(s->p.device));
+  if (int st = flush_extract(s)) return st;
+  CheckpointHeader h{};
+  std::memcpy(h.magic, kCkptMagic, sizeof(h.magic));
+  BHR_CUDA_TRY(cudaMemcpyAsync(&h.rs, s->rs, sizeof(RunState), cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  if (size < checkpoint_bytes(s, h.rs.nrow)) {
+    set_error("checkpoint buffer too small (bhr_solver_checkpoint_size gives the size)");
+    return BHR_INVALID_ARG;
+  }
+  h.N = s->p.N;
+  h.M = s->p.M;
+  h.nt = s->nt;
+  h.max_rows = s->max_rows;
+  h.steps_done = s->steps_done;
+  h.has_source = s->has_source ? 1 : 0;
+  h.dt = s->p.dt;
+  h.a = s->p.a;
+  h.m = s->p.m;
+  const size_t NM = static_cast<size_t>(s->p.N) * s->p.M, M = s->p.M;
+  char *out = static_cast<char *>(buf);
+  std::memcpy(out, &h, sizeof(h));
+  double *d = reinterpret_cast<double *>(out + sizeof(h));
+  BHR_CUDA_TRY(cudaMemcpyAsync(d, s->u0, 4 * NM * 8, cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaMemcpyAsync(d + 4 * NM, s->ext, 2 * M * 8, cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaMemcpyAsync(d + 4 * NM + 2 * M, s->integ, 4 * M * 8, cudaMemcpyDeviceToHost, s->stream));
+  if (h.rs.nrow > 0)
+    BHR_CUDA_TRY(cudaMemcpyAsync(d + 4 * NM + 6 * M, s->rows, 16 * static_cast<size_t>(h.rs.nrow) * 8,
+                                 cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return BHR_OK;
+}
+
+int bhr_solver_restore(bhr_solver *s, const void *buf, size_t size) {
+  if (!s || !buf || size < sizeof(CheckpointHeader)) return BHR_INVALID_ARG;
+  BHR_CUDA_TRY(cudaSetDevice(s->p.device));
+  CheckpointHeader h;
+  std::memcpy(&h, buf, sizeof(h));
+  if (std::memcmp(h.magic, kCkptMagic, sizeof(h.magic)) != 0 || h.N != s->p.N || h.M != s->p.M || h.nt != s->nt ||
+      h.max_rows != s->max_rows || h.dt != s->p.dt || h.a != s->p.a || h.m != s->p.m ||
+      h.has_source != (s->has_source ? 1 : 0) || h.rs.nrow < 0 || h.rs.nrow > s->max_rows ||
+      size < checkpoint_bytes(s, h.rs.nrow)) {
+    set_error("checkpoint does not match this solve (grid, spin, m, dt, length or trajectory)");
+    return BHR_INVALID_ARG;
+  }
+  if (int st = flush_extract(s)) return st;
+  if (s->has_source)
+    if (int st = solver_wait_records(s, h.rs.ks + 1)) return st;
+  const size_t NM = static_cast<size_t>(s->p.N) * s->p.M, M = s->p.M;
+  const double *d = reinterpret_cast<const double *>(static_cast<const char *>(buf) + sizeof(h));
+  BHR_CUDA_TRY(cudaMemcpyAsync(s->u0, d, 4 * NM * 8, cudaMemcpyHostToDevice, s->stream));
+  BHR_CUDA_TRY(cudaMemcpyAsync(s->ext, d + 4 * NM, 2 * M * 8, cudaMemcpyHostToDevice, s->stream));
+  BHR_CUDA_TRY(cudaMemcpyAsync(s->integ, d + 4 * NM + 2 * M, 4 * M * 8, cudaMemcpyHostToDevice, s->stream));
+  if (h.rs.nrow > 0)
+    BHR_CUDA_TRY(cudaMemcpyAsync(s->rows, d + 4 * NM + 6 * M, 16 * static_cast<size_t>(h.rs.nrow) * 8,
+                                 cudaMemcpyHostToDevice, s->stream));
+  BHR_CUDA_TRY(cudaMemcpyAsync(s->rs, &h.rs, sizeof(RunState), cudaMemcpyHostToDevice, s->stream));
+  // The patch of the step the solve resumes at (later ones are built ahead).
+  if (s->has_source) BHR_CUDA_TRY(launch_source(solver_source_args(s), s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  s->steps_done = h.steps_done;
+  return BHR_OK;
+}
+
 int bhr_solver_get_source(bhr_solver *s, double *tre, double *tim) {
   if (!s || !tre || !tim) return BHR_INVALID_ARG;
   BHR_CUDA_TRY(cudaSetDevice(s->p.device));

@@ -181,6 +181,19 @@ int bhr_solver_get_extraction(bhr_solver *s, double *psi_re, double *psi_im, dou
  * as the device built them (zero off the patch). */
 int bhr_solver_get_source(bhr_solver *s, double *tre, double *tim);
 
+/* Checkpoint and resume (no counterpart in the reference, which rebuilds
+ * each solve from scratch): the bytes a checkpoint of this solve needs now
+ * (they grow with the waveform rows written), a copy of its resumable
+ * state -- the four field planes, the extraction column and its two time
+ * integrals, the step and row counters, the timer and the waveform rows so
+ * far -- into a caller buffer, and the restore of such a copy into a solve
+ * created with the same parameters (and, for a sourced solve, given the
+ * same trajectory).  A restored solve continues bit-identically to the one
+ * that was checkpointed. */
+size_t bhr_solver_checkpoint_size(bhr_solver *s);
+int bhr_solver_checkpoint(bhr_solver *s, void *buf, size_t size);
+int bhr_solver_restore(bhr_solver *s, const void *buf, size_t size);
+
 /* Advances nsteps steps like bhr_solver_step and reports the device time
  * between CUDA events recorded on the solver stream around them. */
 int bhr_solver_time_steps(bhr_solver *s, int nsteps, double *ms);
