@@ -1,6 +1,8 @@
 // bhr_kernels.cu -- sm_100a kernels of the FP64 Teukolsky step.
 //
-// One time step is five launches on the solver stream:
+// The kernels of one time step (the solver runs the source of the next step
+// and the extraction of the previous one on a side stream beside stages 1
+// and 2, and advances the stage step clock after the final stage):
 //   source_patch  the Gaussian-smeared particle source on its PTSX x PTSY patch
 //                 (HighOrder/kern.cu:755-768 reset + 1185-2683 deposit)
 //   stage<1,2,3>  one SSP-RK3 stage each (classical RK4: stages 1, 4, 4, 5,
@@ -14,6 +16,7 @@
 //   extract       psi at the extraction column, its two time integrals, and
 //                 on output steps the swsh projection and dE/dt
 //                 (HighOrder/body.cu:168-212, HighOrder/proj.c:37-75)
+//   step_clock    one thread: the stage step clock of the next step
 //
 // Storage: each state is four planes (q_re, q_im, p_re, p_im) of M x N
 // doubles, idx(b,a) = N*b + a.  Only interior points 3 <= b < M-3,

@@ -64,9 +64,9 @@ struct bhr_solver {
 
 
 namespace bhr {
-// Creates a solve; tile_rows 0 lets the autotuner pick the stage tiling
-// (8- or 16-row tiles one per block, or persistent), 8 or 16 fixes
-// one-tile-per-block kernels of that height.
+// Creates a solve; tile_rows 0 lets the autotuner (or BHR_STAGE_TILING) pick
+// the stage tiling, 8 or 16 fixes one-tile-per-block kernels of that height
+// (the batch engine's choice, whose own kernels read the solve's maps).
 int solver_create(const bhr_params *p, int tile_rows, bhr_solver **out);
 // Launch arguments of the solve's kernels (stage pointers vin/un/out unset).
 StageArgs solver_stage_args(bhr_solver *s);
