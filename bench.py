@@ -76,7 +76,9 @@ def profile_traffic(workload):
     """DRAM bytes per grid point of one step's three stage launches, from the
     committed ncu summary of this workload (line
     'dram_bytes_per_point_per_step: X'), or None."""
-    name = {"plunge": "stage_kernel_plunge8192x128.txt", "grid16k": "stage_dram_grid16384x256.txt"}.get(workload)
+    name = {("plunge", "ssprk3"): "stage_kernel_plunge8192x128.txt",
+            ("grid16k", "ssprk3"): "stage_dram_grid16384x256.txt",
+            ("grid16k", "rk4"): "stage_dram_rk4_grid16384x256.txt"}.get((workload, INTEGRATOR))
     if name is None:
         return None
     try:
@@ -243,7 +245,7 @@ def run_ours(args, rank, local_rank, world):
     bytes_pt = (BYTES_PER_PT_MIXED if PRECISION == "mixed" else
                 BYTES_PER_PT_RK4 if INTEGRATOR == "rk4" else BYTES_PER_PT)
     achieved = bytes_pt * N * M / (float(stage_ms.sum()) / 1e3) / 1e9
-    traffic_pp = profile_traffic(args.workload) if PRECISION == "fp64" and INTEGRATOR == "ssprk3" else None
+    traffic_pp = profile_traffic(args.workload) if PRECISION == "fp64" else None
 
     # End to end through the public API: host params + host trajectory in,
     # solver set-up (grid, tables, initial data uploaded), n steps, waveform
