@@ -248,19 +248,17 @@ void apply_closure_host(double *planes, int N, int M, bool even_m, int nplanes) 
 // Initial data: zero (HighOrder/kern.cu:164-167) or the Gaussian pulse
 // psi = exp(-(x-c)^2/(2w^2)) swsh(l, m, theta), Pi = 0, closed by the
 // boundary extrapolation so every stored state satisfies the closure.
-void make_initial_data(const bhr_params &p, const Grid &g, std::vector<double> &qre) {
-  const size_t NM = static_cast<size_t>(p.N) * p.M;
-  qre.clear();
+void make_initial_factors(const bhr_params &p, const Grid &g, std::vector<double> &fa, std::vector<double> &gb) {
+  fa.clear();
+  gb.clear();
   if (p.init_kind != BHR_INIT_GAUSSIAN) return;
-  qre.assign(NM, 0.0);
-  for (int b = 0; b < p.M; b++) {
-    const double y = swsh(p.init_ell, p.m, g.theta[b]);
-    for (int a = 0; a < p.N; a++) {
-      const double x = g.x_c[a] - p.init_center;
-      qre[static_cast<size_t>(b) * p.N + a] = std::exp(-x * x / (2.0 * p.init_width * p.init_width)) * y;
-    }
+  fa.resize(p.N);
+  gb.resize(p.M);
+  for (int a = 0; a < p.N; a++) {
+    const double x = g.x_c[a] - p.init_center;
+    fa[a] = std::exp(-x * x / (2.0 * p.init_width * p.init_width));
   }
-  apply_closure_host(qre.data(), p.N, p.M, (static_cast<int>(p.m) % 2) == 0, 1);
+  for (int b = 0; b < p.M; b++) gb[b] = swsh(p.init_ell, p.m, g.theta[b]);
 }
 
 }  // namespace bhr

@@ -35,9 +35,11 @@ double swsh(double ell, double ml, double the);
 void make_projection_weights(const bhr_params &p, const Grid &g, std::vector<double> &w7);
 // Weights of dE/dt = sum_b |int psi|^2 * E[b] (HighOrder/body.cu:174-184).
 void make_dedt_weights(const bhr_params &p, const Grid &g, std::vector<double> &e);
-// Closed initial q_re plane for init_kind (empty for zero data; q_im, p_re
-// and p_im start at zero in both cases).
-void make_initial_data(const bhr_params &p, const Grid &g, std::vector<double> &qre);
+// Gaussian initial data psi = exp(-(x-c)^2/(2 w^2)) swsh(l, m, theta) is
+// separable: the radial factors fa[N] and angular factors gb[M] (both empty
+// for zero data); the device forms the interior products (q_im, p_re and
+// p_im start at zero; the closure is rebuilt by every reader).
+void make_initial_factors(const bhr_params &p, const Grid &g, std::vector<double> &fa, std::vector<double> &gb);
 // Reference closure (kernel_boundary2a then 2b) applied on nplanes host planes.
 void apply_closure_host(double *planes, int N, int M, bool even_m, int nplanes = 4);
 

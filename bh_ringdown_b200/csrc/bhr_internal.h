@@ -194,6 +194,7 @@ cudaError_t launch_extract_batch(const ExtractArgs *args, int nsolves, cudaStrea
 cudaError_t launch_extract(const ExtractArgs &a, cudaStream_t st);
 cudaError_t launch_closure(double *planes, int N, int M, int even_m, cudaStream_t st);
 cudaError_t launch_wait_selftest(int *status, cudaStream_t st);
+cudaError_t launch_init_product(double *q, const double *fa, const double *gb, int N, int M, cudaStream_t st);
 size_t stage_smem_bytes();
 cudaError_t prepare_kernels();
 

@@ -1163,6 +1163,18 @@ cudaError_t launch_extract(const ExtractArgs &a, cudaStream_t st) {
   return launch_pdl(extract_kernel, dim3(1), dim3(kExtractThreads), 0, st, a);
 }
 
+// Gaussian initial data on the interior: q_re = fa[a] * gb[b] (the product
+// the host would form; the closure is rebuilt by every reader).
+__global__ void init_product_kernel(double *q, const double *fa, const double *gb, int N, int M) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y;
+  if (a >= 3 && a < N - 3 && b >= 3 && b < M - 3) q[static_cast<size_t>(b) * N + a] = fa[a] * gb[b];
+}
+
+cudaError_t launch_init_product(double *q, const double *fa, const double *gb, int N, int M, cudaStream_t st) {
+  init_product_kernel<<<dim3((N + 255) / 256, M), 256, 0, st>>>(q, fa, gb, N, M);
+  return cudaGetLastError();
+}
+
 // Self-check of the bounded barrier wait every stage kernel uses: one block
 // waits on an mbarrier that nothing completes; the wait gives up after its
 // iteration limit and the kernel returns BHR_TIMEOUT (5) in *status instead

@@ -298,27 +298,48 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
     delete s;
     return st;
   }
-  std::vector<double> coltab, rowtab, w7, we, init;
+  std::vector<double> coltab, rowtab, w7, we, fa, gb;
   make_tables(p, g, coltab, rowtab);
   make_projection_weights(p, g, w7);
   make_dedt_weights(p, g, we);
-  make_initial_data(p, g, init);
+  make_initial_factors(p, g, fa, gb);
+  double *dfac = nullptr;  // fa then gb, freed once the product is formed
+  if (!fa.empty() && cudaMallocAsync(reinterpret_cast<void **>(&dfac), (fa.size() + gb.size()) * 8, s->stream) !=
+                         cudaSuccess) {
+    set_error("cudaMallocAsync failed (initial data factors)");
+    free_all(s);
+    delete s;
+    return BHR_OUT_OF_MEMORY;
+  }
   auto up = [&](void *dst, const void *srcp, size_t n) { return cudaMemcpyAsync(dst, srcp, n, cudaMemcpyHostToDevice, s->stream); };
   cudaError_t e = cudaSuccess;
   if ((e = up(s->coltab, coltab.data(), coltab.size() * 8)) || (e = up(s->rowtab, rowtab.data(), rowtab.size() * 8)) ||
       (e = up(s->rc, g.r_c.data(), g.r_c.size() * 8)) || (e = up(s->th, g.theta.data(), g.theta.size() * 8)) ||
       (e = up(s->wproj, w7.data(), w7.size() * 8)) || (e = up(s->wdedt, we.data(), we.size() * 8)) ||
       (e = cudaMemsetAsync(s->u0, 0, 4 * NM * 8, s->stream)) ||
-      (!init.empty() && (e = up(s->u0, init.data(), init.size() * 8))) ||
       (e = launch_coef_tables(s->coltab, s->rowtab, s->ctab, p.N, p.M, s->stream)) ||
       (e = cudaMemsetAsync(s->u1, 0, 4 * NM * 8, s->stream)) || (e = cudaMemsetAsync(s->u2, 0, 4 * NM * 8, s->stream)) ||
       (e = cudaMemsetAsync(s->integ, 0, 4 * p.M * 8, s->stream)) || (e = cudaMemsetAsync(s->ext, 0, 2 * p.M * 8, s->stream)) ||
       (e = cudaMemsetAsync(s->src, 0, 4 * static_cast<size_t>(p.PTSX) * p.PTSY * 8, s->stream)) ||
       (e = cudaMemsetAsync(s->rs, 0, sizeof(RunState), s->stream)) || (e = cudaStreamSynchronize(s->stream))) {
     set_error(std::string("upload: ") + cudaGetErrorString(e));
+    if (dfac) cudaFreeAsync(dfac, s->stream);
     free_all(s);
     delete s;
     return BHR_CUDA_ERROR;
+  }
+  if (dfac) {  // Gaussian initial data: the products formed on the device
+    if ((e = up(dfac, fa.data(), fa.size() * 8)) == cudaSuccess &&
+        (e = up(dfac + fa.size(), gb.data(), gb.size() * 8)) == cudaSuccess)
+      e = launch_init_product(s->u0, dfac, dfac + fa.size(), p.N, p.M, s->stream);
+    cudaFreeAsync(dfac, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) {
+      set_error(std::string("initial data: ") + cudaGetErrorString(e));
+      free_all(s);
+      delete s;
+      return BHR_CUDA_ERROR;
+    }
   }
   // BHR_STAGE_TILING=block8|block16|persistent|block8n|ring fixes the stage
   // tiling of solves whose tiling is not fixed by the caller.
