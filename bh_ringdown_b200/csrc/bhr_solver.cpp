@@ -454,25 +454,80 @@ int bhr_solver_info(const bhr_solver *s, bhr_info *info) {
 static constexpr int kFirstRecords = 8192;
 static constexpr int kRecordChunk = 16384;
 
-// What the records of a trajectory are built from.
+// HighOrder/body.cu:97-124 as a resumable cursor over a copy of the
+// trajectory rows: the pre-loop reads one line and then lines until
+// ptime >= timer; each step reads two lines and uses the second; a read
+// past the end leaves the particle variables unchanged; rp gets +1e-6 every
+// step; the second time derivatives are backward differences of the first
+// over dt (zero history at step 0); third derivatives are 0.  fill() must be
+// called for consecutive step ranges.
 struct RecordJob {
   bhr_params p;
   double dx, dtheta, rpl, rmn;
-  std::vector<bhr_particle> pts;  // particle state of every step
-  std::vector<double> turn;       // turn-on window of every step
+  std::vector<double> rows;
+  int nrows = 0, cursor = 0;
+  double row[10] = {0};
+  double rp = 0, tmp11 = 0, tmp22 = 0, tmp33 = 0, timer = 0, start = 0;
+
+  void read() {
+    if (cursor < nrows) {
+      std::memcpy(row, rows.data() + static_cast<size_t>(10) * cursor, sizeof(row));
+      cursor++;
+    }
+  }
+  void begin() {
+    timer = 0.0;
+    start = timer;
+    read();
+    do {
+      read();
+    } while (row[0] < timer && cursor < nrows);
+    rp = row[1];
+  }
+  // Particle state and turn-on factor of the next n steps.
+  void fill(int n, bhr_particle *pts, double *turn) {
+    for (int i = 0; i < n; i++) {
+      const int c0 = cursor;
+      read();
+      read();
+      if (cursor != c0) rp = row[1];
+      rp = rp + 1e-6;
+      bhr_particle &pt = pts[i];
+      pt = bhr_particle{};
+      pt.rp = rp;
+      pt.tp = row[2];
+      pt.phip = row[6];
+      pt.E = row[7];
+      pt.lz = row[8];
+      pt.Q = row[9];
+      pt.drdt = row[3];
+      pt.d2rdt2 = (row[3] - tmp11) / p.dt;
+      pt.dthdt = row[4];
+      pt.d2thdt2 = (row[4] - tmp22) / p.dt;
+      pt.dphidt = row[5];
+      pt.d2phidt2 = (row[5] - tmp33) / p.dt;
+      tmp11 = row[3];
+      tmp22 = row[4];
+      tmp33 = row[5];
+      turn[i] = std::pow(1.0 - std::exp(-(timer - start) / 25.0), 4);
+      timer += p.dt;
+    }
+  }
 };
 
-// Records of steps [k0, k1) into out[0 .. k1-k0) on all host threads:
-// source coefficients times the turn-on window, radial width and patch
+// Records of steps [k0, k1) into out[0 .. k1-k0) on all host threads, from
+// those steps' particle states and turn-on factors (pts, turn, indexed from
+// k0): source coefficients times the turn-on window, radial width and patch
 // origin.  Returns the first step whose particle is off the grid, inside
 // the horizon or on a pole (its status in *bad_status), or -1.
-static int build_records(const RecordJob &J, int k0, int k1, StepRec *out, int *bad_status) {
+static int build_records(const RecordJob &J, int k0, int k1, const bhr_particle *pts, const double *turn,
+                         StepRec *out, int *bad_status) {
   const bhr_params &p = J.p;
   std::mutex bad_mu;
   int first_bad = -1, status = BHR_OK;
   auto work = [&](int a0, int a1) {
     for (int k = a0; k < a1; k++) {
-      const bhr_particle &pt = J.pts[k];
+      const bhr_particle &pt = pts[k - k0];
       StepRec &R = out[k - k0];
       double cr[6], ci[6];
       const int st = bhr_source_coefficients(&pt, p.a, p.mass, p.m, cr, ci);
@@ -488,8 +543,8 @@ static int build_records(const RecordJob &J, int k0, int k1, StepRec *out, int *
         return;
       }
       for (int i = 0; i < 6; i++) {
-        R.c_re[i] = cr[i] * J.turn[k];
-        R.c_im[i] = ci[i] * J.turn[k];
+        R.c_re[i] = cr[i] * turn[k - k0];
+        R.c_im[i] = ci[i] * turn[k - k0];
       }
       R.rp = pt.rp;
       R.tp = pt.tp;
@@ -522,10 +577,13 @@ static void record_worker(bhr_solver *s, std::shared_ptr<RecordJob> job, int k_f
   cudaStream_t up = nullptr;
   const bool ok_stream = cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking) == cudaSuccess;
   std::vector<StepRec> buf(kRecordChunk);
+  std::vector<bhr_particle> pts(kRecordChunk);
+  std::vector<double> turn(kRecordChunk);
   for (int k0 = k_from; k0 < s->nt && !s->rec_stop.load(); k0 += kRecordChunk) {
     const int k1 = std::min(s->nt, k0 + kRecordChunk);
+    job->fill(k1 - k0, pts.data(), turn.data());
     int status = BHR_OK;
-    int bad = build_records(*job, k0, k1, buf.data(), &status);
+    int bad = build_records(*job, k0, k1, pts.data(), turn.data(), buf.data(), &status);
     if (bad < 0 && (!ok_stream ||
                     cudaMemcpyAsync(s->recs + k0, buf.data(), sizeof(StepRec) * (k1 - k0), cudaMemcpyHostToDevice,
                                     up) != cudaSuccess ||
@@ -570,11 +628,8 @@ int bhr::solver_wait_records(bhr_solver *s, int upto) {
 
 extern "C" {
 
-// HighOrder/body.cu:97-124: the pre-loop reads one line and then lines
-// until ptime >= timer; each step reads two lines and uses the second; a
-// read past the end leaves the particle variables unchanged; rp gets
-// +1e-6 every step; the second time derivatives are backward differences
-// of the first over dt (zero history at step 0); third derivatives are 0.
+// The trajectory cursor of HighOrder/body.cu:97-124 (RecordJob above)
+// feeds the per-step source records.
 int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows) {
   if (!s || !rows || nrows < 2) {
     set_error("trajectory needs at least two rows");
@@ -586,67 +641,27 @@ int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows) {
   const bhr_params &p = s->p;
   const double a = p.a, mass = p.mass;
   const double rpl = mass + std::sqrt(mass * mass - a * a), rmn = mass - std::sqrt(mass * mass - a * a);
-  double row[10] = {0};
-  int cursor = 0;
-  auto rd = [&]() {
-    if (cursor < nrows) {
-      std::memcpy(row, rows + static_cast<size_t>(10) * cursor, sizeof(row));
-      cursor++;
-    }
-  };
-  double timer = 0.0;
-  const double start = timer;
-  rd();
-  do {
-    rd();
-  } while (row[0] < timer && cursor < nrows);
-  double rp = row[1];
-  double tmp11 = 0.0, tmp22 = 0.0, tmp33 = 0.0;
-  // Sequential pass: particle state and turn-on factor of every step.
-  std::vector<bhr_particle> pts(s->nt);
-  std::vector<double> turn(s->nt);
-  for (int k = 0; k < s->nt; k++) {
-    const int c0 = cursor;
-    rd();
-    rd();
-    if (cursor != c0) rp = row[1];
-    rp = rp + 1e-6;
-    bhr_particle &pt = pts[k];
-    pt = bhr_particle{};
-    pt.rp = rp;
-    pt.tp = row[2];
-    pt.phip = row[6];
-    pt.E = row[7];
-    pt.lz = row[8];
-    pt.Q = row[9];
-    pt.drdt = row[3];
-    pt.d2rdt2 = (row[3] - tmp11) / p.dt;
-    pt.dthdt = row[4];
-    pt.d2thdt2 = (row[4] - tmp22) / p.dt;
-    pt.dphidt = row[5];
-    pt.d2phidt2 = (row[5] - tmp33) / p.dt;
-    tmp11 = row[3];
-    tmp22 = row[4];
-    tmp33 = row[5];
-    turn[k] = std::pow(1.0 - std::exp(-(timer - start) / 25.0), 4);
-    timer += p.dt;
-  }
-  // Independent per step: source coefficients, width and patch origin,
-  // evaluated on all host threads.  The first chunk of steps is built here;
-  // the rest on a host thread while the device steps (solver_wait_records
-  // holds stepping back until the records it reaches are uploaded).
+  // Per step: particle state (a sequential cursor), then source
+  // coefficients, width and patch origin (independent, on all host
+  // threads).  The first chunk of steps is built here; the rest on a host
+  // thread while the device steps (solver_wait_records holds stepping back
+  // until the records it reaches are uploaded).
   auto job = std::make_shared<RecordJob>();
   job->p = p;
   job->dx = s->g.dx;
   job->dtheta = s->g.dtheta;
   job->rpl = rpl;
   job->rmn = rmn;
-  job->pts = std::move(pts);
-  job->turn = std::move(turn);
+  job->rows.assign(rows, rows + static_cast<size_t>(10) * nrows);
+  job->nrows = nrows;
+  job->begin();
   const int k_first = std::min(s->nt, kFirstRecords);
   std::vector<StepRec> recs(static_cast<size_t>(std::max(1, k_first)));
+  std::vector<bhr_particle> pts(static_cast<size_t>(std::max(1, k_first)));
+  std::vector<double> turn(static_cast<size_t>(std::max(1, k_first)));
+  job->fill(k_first, pts.data(), turn.data());
   int bad_status = BHR_OK;
-  const int bad = build_records(*job, 0, k_first, recs.data(), &bad_status);
+  const int bad = build_records(*job, 0, k_first, pts.data(), turn.data(), recs.data(), &bad_status);
   if (bad >= 0) {
     set_error("trajectory step " + std::to_string(bad) + ": particle off the grid, inside the horizon or on a pole");
     return bad_status;
