@@ -261,7 +261,15 @@ def run_ours(args, rank, local_rank, world):
     info = s2.info()
     s2.close()
     t_e2e = time.perf_counter() - t0
-    h2d = 4 * N * M * 8 + (13 * N + 4 * M + N + M + 8 * M) * 8 + (0 if rows is None else info["nt"] * 160)
+    # bytes the API copies host -> device: column and row tables, r_c and
+    # theta, projection and dE/dt weights, the separable initial-data factors
+    # (Gaussian data), and one 128-byte source record per step of the run
+    # (sourced; built and uploaded chunk by chunk while the device steps)
+    h2d = ((13 * N + 4 * M) + (N + M) + (7 * M + M)) * 8
+    if prm.init_kind == bhr.BHR_INIT_GAUSSIAN:
+        h2d += (N + M) * 8
+    if rows is not None:
+        h2d += info["nt"] * 128
     d2h = len(tw) * 16 * 8
     e2e = {"value": N * M * n_e2e / t_e2e * world, "unit": UNIT, "h2d_bytes_per_step": int(h2d / n_e2e),
            "d2h_bytes_per_step": int(d2h / n_e2e), "steps": n_e2e,
