@@ -354,6 +354,11 @@ def run_reference(args, rank, world):
     host's cores (oracle/_ref/libref_cfg2.so), on the same workload."""
     if rank != 0:
         return
+    if args.workload != "plunge" or PRECISION != "fp64" or INTEGRATOR != "ssprk3":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's grid is fixed at compile time; "
+                                                               "oracle/_ref is built for the 8192x128 FP64 SSP-RK3 "
+                                                               "plunge workload only"}))
+        return
     import ctypes as C
     lib_path = os.path.join(ROOT, "oracle", "_ref", "libref_cfg2.so")
     if not os.path.exists(lib_path):
