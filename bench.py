@@ -697,6 +697,9 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     rank, local_rank, world = env_rank()
+    if args.impl == "reference" and args.workload in ("batch64", "serve"):
+        run_reference(args, rank, world)
+        return
     if args.workload in ("batch64", "serve"):
         (run_batch if args.workload == "batch64" else run_serve)(args)
         return
