@@ -142,6 +142,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "bhr_solver_set_state": (I, [vp, dp, dp, dp, dp]),
         "bhr_solver_get_extraction": (I, [vp, dp, dp, dp, dp, dp, dp]),
         "bhr_solver_get_source": (I, [vp, dp, dp]),
+        "bhr_solver_psi_samples": (I, [vp, dp, dp, I, C.POINTER(I)]),
         "bhr_solver_checkpoint_size": (C.c_size_t, [vp]),
         "bhr_solver_checkpoint": (I, [vp, vp, C.c_size_t]),
         "bhr_solver_restore": (I, [vp, vp, C.c_size_t]),
@@ -304,6 +305,16 @@ class Solver:
         tre, tim = np.zeros(self.N * self.M), np.zeros(self.N * self.M)
         _check(self.lib.bhr_solver_get_source(self._h, _ptr(tre), _ptr(tim)))
         return tre.reshape(self.M, self.N), tim.reshape(self.M, self.N)
+
+    def psi_samples(self):
+        """psi(theta) at the extraction column on each waveform row's step:
+        (re, im), each rows x M."""
+        n = self.info()["rows_done"]
+        re, im = np.zeros(max(1, n) * self.M), np.zeros(max(1, n) * self.M)
+        got = I(0)
+        _check(self.lib.bhr_solver_psi_samples(self._h, _ptr(re), _ptr(im), n, C.byref(got)))
+        k = got.value
+        return re[:k * self.M].reshape(k, self.M), im[:k * self.M].reshape(k, self.M)
 
     def checkpoint(self) -> bytes:
         """The solve's resumable state (fields, extraction integrals, counters,

@@ -75,7 +75,7 @@ size_t solve_bytes(const bhr_params &p, int traj_rows) {
   b += static_cast<size_t>(CF_COUNT + 2) * p.N * 8 + static_cast<size_t>(RF_COUNT + 12) * p.M * 8;
   b += static_cast<size_t>(4) * p.PTSX * p.PTSY * 8;  // two source patch buffers
   if (traj_rows > 0 && p.dt > 0) b += static_cast<size_t>(p.T / p.dt + 2) * sizeof(StepRec);
-  if (p.dt > 0 && p.Fr > 0) b += static_cast<size_t>(p.T / p.dt / p.Fr + 2) * 16 * 8;
+  if (p.dt > 0 && p.Fr > 0) b += static_cast<size_t>(p.T / p.dt / p.Fr + 2) * (16 + 2 * p.M) * 8;  // rows, psi samples
   return b + (1 << 20);
 }
 

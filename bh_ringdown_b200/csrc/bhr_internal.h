@@ -102,6 +102,7 @@ struct ExtractArgs {
   const double *wproj;  // [7][M] Boole x swsh projection weights
   const double *wdedt;  // [M]
   double *rows;         // [max_rows][16]: t, h+/hx x 7, dedt
+  double *psirows;      // [max_rows][2][M]: psi at the extraction column on each row's step, or nullptr
   RunState *rs;
   int N, M, ext_col, Fr, max_rows, even_m;
   int set_ks;           // 1: also advance rs->ks (stages and extraction in sequence)

@@ -889,6 +889,10 @@ __device__ __forceinline__ void extract_body(const ExtractArgs &A) {
     if (!isfinite(psr) || !isfinite(psi)) bad = 1;
     A.ext[b] = psr;
     A.ext[M + b] = psi;
+    if (out_step && nrow < A.max_rows && A.psirows != nullptr) {
+      A.psirows[(2 * static_cast<size_t>(nrow)) * M + b] = psr;
+      A.psirows[(2 * static_cast<size_t>(nrow) + 1) * M + b] = psi;
+    }
     const double ir = in[0] + psr * A.dt;
     const double ii = in[1] + psi * A.dt;
     const double dr = in[2] + ir * A.dt;

@@ -99,7 +99,7 @@ void free_all(bhr_solver *s) {
     s->rec_thread.join();
   }
   void *ptrs[] = {s->u0,    s->u1,   s->u2,     s->u3,     s->coltab, s->rowtab, s->ctab,   s->rc,     s->th,
-                  s->src,   s->ext,  s->integ,  s->wproj,  s->wdedt,  s->rows,   s->recs,   s->rs,
+                  s->src,   s->ext,  s->integ,  s->wproj,  s->wdedt,  s->rows,   s->recs,   s->rs,  s->psirows,
                   s->d1f,   s->e2f,  s->colf32, s->rowf32, s->bbf};
   for (void *q : ptrs)
     if (q) cudaFreeAsync(q, s->stream);
@@ -293,7 +293,8 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
       (st = dalloc(s, &s->th, p.M)) || (st = dalloc(s, &s->src, 4 * static_cast<size_t>(p.PTSX) * p.PTSY)) ||
       (st = dalloc(s, &s->ext, 2 * static_cast<size_t>(p.M))) || (st = dalloc(s, &s->integ, 4 * static_cast<size_t>(p.M))) ||
       (st = dalloc(s, &s->wproj, 7 * static_cast<size_t>(p.M))) || (st = dalloc(s, &s->wdedt, p.M)) ||
-      (st = dalloc(s, &s->rows, 16 * static_cast<size_t>(s->max_rows))) || (st = dalloc(s, &s->rs, 1))) {
+      (st = dalloc(s, &s->rows, 16 * static_cast<size_t>(s->max_rows))) ||
+      (st = dalloc(s, &s->psirows, 2 * static_cast<size_t>(p.M) * s->max_rows)) || (st = dalloc(s, &s->rs, 1))) {
     free_all(s);
     delete s;
     return st;
@@ -871,6 +872,7 @@ ExtractArgs bhr::solver_extract_args(bhr_solver *s) {
   E.wproj = s->wproj;
   E.wdedt = s->wdedt;
   E.rows = s->rows;
+  E.psirows = s->psirows;
   E.rs = s->rs;
   E.N = p.N;
   E.M = p.M;
@@ -1215,7 +1217,8 @@ int bhr_solver_get_extraction(bhr_solver *s, double *psi_re, double *psi_im, dou
 
 namespace {
 // Layout of a checkpoint: this header, then the four state planes (4 N M),
-// ext (2 M), integ (4 M) and nrow waveform rows (16 doubles each).
+// ext (2 M), integ (4 M), nrow waveform rows (16 doubles each) and their
+// psi samples (2 M each).
 struct CheckpointHeader {
   char magic[8];  // "BHRCKPT1"
   int N, M, nt, max_rows, steps_done, has_source;
@@ -1226,11 +1229,34 @@ constexpr char kCkptMagic[8] = {'B', 'H', 'R', 'C', 'K', 'P', 'T', '1'};
 
 size_t checkpoint_bytes(const bhr_solver *s, int nrow) {
   const size_t NM = static_cast<size_t>(s->p.N) * s->p.M;
-  return sizeof(CheckpointHeader) + 8 * (4 * NM + 6 * static_cast<size_t>(s->p.M) + 16 * static_cast<size_t>(nrow));
+  return sizeof(CheckpointHeader) +
+         8 * (4 * NM + 6 * static_cast<size_t>(s->p.M) + (16 + 2 * static_cast<size_t>(s->p.M)) * nrow);
 }
 }  // namespace
 
 extern "C" {
+
+int bhr_solver_psi_samples(bhr_solver *s, double *psi_re, double *psi_im, int max_rows, int *nrows) {
+  if (!s) return BHR_INVALID_ARG;
+  BHR_CUDA_TRY(cudaSetDevice(s->p.device));
+  if (int st = flush_extract(s)) return st;
+  RunState rs{};
+  BHR_CUDA_TRY(cudaMemcpyAsync(&rs, s->rs, sizeof(rs), cudaMemcpyDeviceToHost, s->stream));
+  BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  const int n = std::min(rs.nrow, std::max(0, max_rows));
+  const size_t M = s->p.M;
+  std::vector<double> buf(2 * M * static_cast<size_t>(n));
+  if (n > 0) {
+    BHR_CUDA_TRY(cudaMemcpyAsync(buf.data(), s->psirows, buf.size() * 8, cudaMemcpyDeviceToHost, s->stream));
+    BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  }
+  for (int r = 0; r < n; r++) {
+    if (psi_re) std::memcpy(psi_re + r * M, buf.data() + 2 * M * r, M * 8);
+    if (psi_im) std::memcpy(psi_im + r * M, buf.data() + 2 * M * r + M, M * 8);
+  }
+  if (nrows) *nrows = n;
+  return BHR_OK;
+}
 
 size_t bhr_solver_checkpoint_size(bhr_solver *s) {
   if (!s) return 0;
@@ -1271,9 +1297,12 @@ int bhr_solver_checkpoint(bhr_solver *s, void *buf, size_t size) {
   BHR_CUDA_TRY(cudaMemcpyAsync(d, s->u0, 4 * NM * 8, cudaMemcpyDeviceToHost, s->stream));
   BHR_CUDA_TRY(cudaMemcpyAsync(d + 4 * NM, s->ext, 2 * M * 8, cudaMemcpyDeviceToHost, s->stream));
   BHR_CUDA_TRY(cudaMemcpyAsync(d + 4 * NM + 2 * M, s->integ, 4 * M * 8, cudaMemcpyDeviceToHost, s->stream));
-  if (h.rs.nrow > 0)
+  if (h.rs.nrow > 0) {
     BHR_CUDA_TRY(cudaMemcpyAsync(d + 4 * NM + 6 * M, s->rows, 16 * static_cast<size_t>(h.rs.nrow) * 8,
                                  cudaMemcpyDeviceToHost, s->stream));
+    BHR_CUDA_TRY(cudaMemcpyAsync(d + 4 * NM + 6 * M + 16 * static_cast<size_t>(h.rs.nrow), s->psirows,
+                                 2 * M * static_cast<size_t>(h.rs.nrow) * 8, cudaMemcpyDeviceToHost, s->stream));
+  }
   BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));
   return BHR_OK;
 }
@@ -1298,9 +1327,12 @@ int bhr_solver_restore(bhr_solver *s, const void *buf, size_t size) {
   BHR_CUDA_TRY(cudaMemcpyAsync(s->u0, d, 4 * NM * 8, cudaMemcpyHostToDevice, s->stream));
   BHR_CUDA_TRY(cudaMemcpyAsync(s->ext, d + 4 * NM, 2 * M * 8, cudaMemcpyHostToDevice, s->stream));
   BHR_CUDA_TRY(cudaMemcpyAsync(s->integ, d + 4 * NM + 2 * M, 4 * M * 8, cudaMemcpyHostToDevice, s->stream));
-  if (h.rs.nrow > 0)
+  if (h.rs.nrow > 0) {
     BHR_CUDA_TRY(cudaMemcpyAsync(s->rows, d + 4 * NM + 6 * M, 16 * static_cast<size_t>(h.rs.nrow) * 8,
                                  cudaMemcpyHostToDevice, s->stream));
+    BHR_CUDA_TRY(cudaMemcpyAsync(s->psirows, d + 4 * NM + 6 * M + 16 * static_cast<size_t>(h.rs.nrow),
+                                 2 * M * static_cast<size_t>(h.rs.nrow) * 8, cudaMemcpyHostToDevice, s->stream));
+  }
   BHR_CUDA_TRY(cudaMemcpyAsync(s->rs, &h.rs, sizeof(RunState), cudaMemcpyHostToDevice, s->stream));
   // The patch of the step the solve resumes at (later ones are built ahead).
   if (s->has_source) BHR_CUDA_TRY(launch_source(solver_source_args(s), s->stream));

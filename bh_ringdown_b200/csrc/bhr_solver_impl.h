@@ -29,6 +29,7 @@ struct bhr_solver {
   double *u3 = nullptr;
   double *coltab = nullptr, *rowtab = nullptr, *ctab = nullptr, *rc = nullptr, *th = nullptr;
   double *src = nullptr, *ext = nullptr, *integ = nullptr, *wproj = nullptr, *wdedt = nullptr, *rows = nullptr;
+  double *psirows = nullptr;  // psi(theta) at the extraction column per waveform row
   // mixed precision (BHR_MIXED): FP32 delta1 and eps2 planes, FP32 tables
   bool mixed = false;
   float *d1f = nullptr, *e2f = nullptr, *colf32 = nullptr, *rowf32 = nullptr, *bbf = nullptr;

@@ -180,6 +180,11 @@ int bhr_solver_get_extraction(bhr_solver *s, double *psi_re, double *psi_im, dou
 /* Source planes (tred/timd of HighOrder/kern.cu:15-16) for the current step
  * as the device built them (zero off the patch). */
 int bhr_solver_get_source(bhr_solver *s, double *tre, double *tim);
+/* The raw samples behind the waveform rows: psi(theta) at the extraction
+ * column (psi_re/psi_im[r*M + b], M values per row) on the step of each of
+ * the first max_rows rows -- the HighOrder/kern.cu:750-751 column copy on
+ * output steps, for projections of the caller's own. */
+int bhr_solver_psi_samples(bhr_solver *s, double *psi_re, double *psi_im, int max_rows, int *nrows);
 
 /* Checkpoint and resume (no counterpart in the reference, which rebuilds
  * each solve from scratch): the bytes a checkpoint of this solve needs now

@@ -58,12 +58,18 @@ def test_waveform_rows_match_oracle(m):
                       Fr=5)
     nsteps = 600
     s.step(nsteps)
-    t, h, dedt, steps, _, _ = o.run(nsteps=nsteps)
+    t, h, dedt, steps, er, ei = o.run(nsteps=nsteps, ext_every=5, max_ext=nsteps // 5)
     ts, hs, es = s.waveform()
     assert len(ts) == len(t) == nsteps // 5
     assert np.array_equal(ts, t)
     assert np.linalg.norm(hs - h) <= WAVE_TOL * np.linalg.norm(h)
     assert np.linalg.norm(es - dedt) <= WAVE_TOL * np.linalg.norm(dedt)
+    # the raw psi(theta) samples behind the rows (kern.cu:750-751 column copy)
+    pr, pi = s.psi_samples()
+    assert pr.shape == er.shape == (nsteps // 5, M)
+    scale = max(np.max(np.abs(er)), np.max(np.abs(ei)))
+    assert scale > 1e-8
+    assert max(np.max(np.abs(pr - er)), np.max(np.abs(pi - ei))) <= FIELD_TOL * scale
 
 
 def test_config1_full_length_waveform():
