@@ -508,6 +508,7 @@ int bhr_engine_submit(bhr_engine *e, const bhr_params *p, const double *traj_row
 }
 
 int bhr_engine_step(bhr_engine *e, int max_steps, int *running) {
+  NvtxRange range("bhr_engine_step");
   if (!e || max_steps < 0) return set_fail(BHR_INVALID_ARG, "bad step arguments");
   std::lock_guard<std::mutex> lock(e->mu);
   if (cudaSetDevice(e->device) != cudaSuccess) return set_fail(BHR_CUDA_ERROR, "cudaSetDevice failed");

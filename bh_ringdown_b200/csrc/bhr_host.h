@@ -5,9 +5,20 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "bhr.h"
 
 namespace bhr {
+
+// An NVTX range around a host API call (visible in Nsight timelines; a
+// no-op when no tool is attached).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 constexpr double kPiParm = 3.14159265358979;  // HighOrder/parm.h:12
 

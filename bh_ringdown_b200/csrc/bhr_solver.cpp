@@ -230,6 +230,7 @@ int bhr_solver_create(const bhr_params *pin, bhr_solver **out) { return bhr::sol
 static int encode_maps(bhr_solver *s, int rows);
 
 int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
+  NvtxRange range("bhr_solver_create");
   if (!pin || !out) {
     set_error("null argument");
     return BHR_INVALID_ARG;
@@ -632,6 +633,7 @@ extern "C" {
 // The trajectory cursor of HighOrder/body.cu:97-124 (RecordJob above)
 // feeds the per-step source records.
 int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows) {
+  NvtxRange range("bhr_solver_set_trajectory");
   if (!s || !rows || nrows < 2) {
     set_error("trajectory needs at least two rows");
     return BHR_INVALID_ARG;
@@ -1053,6 +1055,7 @@ static int enqueue_steps(bhr_solver *s, int nsteps) {
 extern "C" {
 
 int bhr_solver_step(bhr_solver *s, int nsteps) {
+  NvtxRange range("bhr_solver_step");
   if (!s || nsteps < 0) return BHR_INVALID_ARG;
   BHR_CUDA_TRY(cudaSetDevice(s->p.device));
   if (s->steps_done + nsteps > s->nt && s->has_source) {
@@ -1065,6 +1068,7 @@ int bhr_solver_step(bhr_solver *s, int nsteps) {
 }
 
 int bhr_solver_time_steps(bhr_solver *s, int nsteps, double *ms) {
+  NvtxRange range("bhr_solver_time_steps");
   if (!s || nsteps < 0 || !ms) return BHR_INVALID_ARG;
   BHR_CUDA_TRY(cudaSetDevice(s->p.device));
   if (s->steps_done + nsteps > s->nt && s->has_source) {
@@ -1116,6 +1120,7 @@ int bhr_solver_waveform(bhr_solver *s, double *t, double *h, double *dedt, int m
 }
 
 int bhr_solver_run(bhr_solver *s, const char *out_dir, const char *name) {
+  NvtxRange range("bhr_solver_run");
   if (!s) return BHR_INVALID_ARG;
   const int remaining = s->nt - s->steps_done;
   const int chunk = 1000;
@@ -1270,6 +1275,7 @@ size_t bhr_solver_checkpoint_size(bhr_solver *s) {
 }
 
 int bhr_solver_checkpoint(bhr_solver *s, void *buf, size_t size) {
+  NvtxRange range("bhr_solver_checkpoint");
   if (!s || !buf) return BHR_INVALID_ARG;
   BHR_CUDA_TRY(cudaSetDevice(s->p.device));
   if (int st = flush_extract(s)) return st;
@@ -1308,6 +1314,7 @@ int bhr_solver_checkpoint(bhr_solver *s, void *buf, size_t size) {
 }
 
 int bhr_solver_restore(bhr_solver *s, const void *buf, size_t size) {
+  NvtxRange range("bhr_solver_restore");
   if (!s || !buf || size < sizeof(CheckpointHeader)) return BHR_INVALID_ARG;
   BHR_CUDA_TRY(cudaSetDevice(s->p.device));
   CheckpointHeader h;
@@ -1375,6 +1382,7 @@ int bhr_solver_get_source(bhr_solver *s, double *tre, double *tim) {
 void *bhr_solver_stream(bhr_solver *s) { return s ? static_cast<void *>(s->stream) : nullptr; }
 
 int bhr_solver_profile(bhr_solver *s, int nsteps, double *avg_ms5, double *total_ms) {
+  NvtxRange range("bhr_solver_profile");
   if (!s || nsteps <= 0) return BHR_INVALID_ARG;
   BHR_CUDA_TRY(cudaSetDevice(s->p.device));
   if (s->has_source && s->steps_done + nsteps > s->nt) {
