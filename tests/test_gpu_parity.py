@@ -227,3 +227,19 @@ def test_long_trajectory_records_built_while_stepping():
     assert len(ts) == n // 50 and np.array_equal(ts, t) and np.max(np.abs(h)) > 0
     assert np.linalg.norm(hs - h) <= WAVE_TOL * np.linalg.norm(h)
     assert rel_field_err(gs, o.get_state()) <= 1e-9  # 12000 steps of rounding
+
+
+@pytest.mark.parametrize("tiling", ["block8", "block16", "persistent", "block8n", "ring"])
+@pytest.mark.parametrize("N,M", [(64, 16), (128, 16), (192, 32)])
+def test_tiny_grids_every_tiling(tiling, N, M, monkeypatch):
+    """Grids of one to a dozen tiles, every tile at an edge, persistent
+    kernels with more block slots than tiles: each tiling against the
+    oracle."""
+    monkeypatch.setenv("BHR_STAGE_TILING", tiling)
+    Xmin, Xmax = -20.0, 20.0
+    s, o, info = pair(N, M, Xmin, Xmax, 0.7, 2.0, dt=0.2 * (Xmax - Xmin) / N, center=0.0, width=2.0)
+    assert info["tiling"] == tiling
+    s.step(20)
+    o.step(20)
+    assert rel_field_err(s.get_state(), o.get_state()) <= FIELD_TOL
+    s.close()
