@@ -145,6 +145,7 @@ void fill_tables(const bhr_params &p, double dx, const double *r_c, const double
     c[CF_XR * N + j] = -(xr_num / (cL3 * eR));
     c[CF_YR * N + j] = -(yr_num / (cL3 * eR));
     c[CF_CR0 * N + j] = Dt * (2.0 * eR2 + 6.0 * eR * mass * Om - 6.0 * Om2 * a2) / eR2;
+    c[CF_DT * N + j] = Dt;
     c[CF_CR1 * N + j] = Dt;
     c[CF_BI0 * N + j] = 2.0 * spin * em * (-(Om2 * Sg) + cL * (eR2 + 2.0 * eR * mass * Om + Om2 * a2)) / cL;
     c[CF_BI1 * N + j] = -4.0 * spin * Dt;

@@ -21,19 +21,23 @@ constexpr int STAGE_THREADS = 256;
 // B1*sin^2(theta) every coefficient of HighOrder/kern.cu:132-158 is a
 // per-column numerator, a per-row factor and 1/bir.
 enum ColField {
+  // The first CF_TILE factors are the ones every FP64 stage tile loads.
   CF_B0 = 0,   // -(2 cL - Om^2) Sg^2 / cL^2
-  CF_B1,       // a^2 Dt
+  CF_DT,       // Dt; with the solve's a^2 and -4a it also gives B1, CCN,
+               // CR1 and BI1 below, which the FP64 stage kernels form per point
   CF_ATN,      // 2 (cL - Om^2) Sg^2 / cL^2        Ataurho = ATN / bir
-  CF_ARN,      // -Om^2 Sg^2 / cL^2                Arhorho = ARN / bir
-  CF_CCN,      // -Dt                              Ayy     = CCN / bir
   CF_XR,       // BtauReal * bir
   CF_YR,       // BrhoReal * bir
   CF_CR0,      // CReal * bir, theta-free part
-  CF_CR1,      // Dt: multiplies g(theta) = 4cot^2 - 4m cot csc + m^2 csc^2
   CF_BI0,      // BtauImag * bir, theta-free part
-  CF_BI1,      // -4 a Dt: multiplies cos(theta)
   CF_BRI,      // BrhoImag * bir
   CF_CIN,      // CImag * bir
+  CF_TILE,
+  CF_ARN = CF_TILE,  // -Om^2 Sg^2 / cL^2          Arhorho = ARN / bir (the bb table only)
+  CF_B1,       // a^2 Dt
+  CF_CCN,      // -Dt                              Ayy     = CCN / bir
+  CF_CR1,      // Dt: multiplies g(theta) = 4cot^2 - 4m cot csc + m^2 csc^2
+  CF_BI1,      // -4 a Dt: multiplies cos(theta)
   CF_COUNT
 };
 enum RowField { RF_S2 = 0, RF_COS, RF_G, RF_CTAN, RF_COUNT };
@@ -81,6 +85,7 @@ struct StageArgs {
   double *zout;         // RK4 stage 2: z = (y1 + 2 y2 - u^n)/3, or nullptr
   double dt;            // the stage's step in the combination (RK4: dt/2, dt, dt/6)
   double cx, cy, cyy, cko;
+  double a2, m4a;       // a^2 and -4a: B1 = a2 Dt and BI1 = m4a Dt, the products the column table holds
 };
 
 struct SourceArgs {

@@ -46,7 +46,7 @@ struct __align__(128) StageSmem {
   alignas(128) double q[2][ROWS + 6][WC];    // TMA box {WC, ROWS+6, 2}: planes q_re, q_im with halo
   alignas(128) double p[2][ROWS][WC];        // TMA box {WC, ROWS, 2}: planes p_re, p_im with column halo
   alignas(128) double bb[ROWS][WC];          // TMA box {WC, ROWS, 1}: bb on the window columns
-  alignas(128) double cf[CF_COUNT][TC];      // TMA box {TC, CF_COUNT}: column factors of the tile columns
+  alignas(128) double cf[CF_TILE][TC];       // TMA box {TC, CF_TILE}: column factors of the tile columns
   alignas(128) double un[4][ROWS][TC];       // TMA box {TC, ROWS, 4}: u^n (RK4 stage 5: z), stages > 1
   alignas(128) double rf[RF_COUNT][ROWS];    // TMA box {ROWS, RF_COUNT}: row factors of the tile rows
   uint64_t bar;
@@ -281,26 +281,28 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
       bw[2 * j + 1] = t.y;
     }
     auto pair = [&](const double *base) { return *reinterpret_cast<const double2 *>(base + 2 * tx); };
-    const double2 g0 = pair(S.cf[CF_B0]), g1 = pair(S.cf[CF_B1]), g2 = pair(S.cf[CF_ATN]);
-    const double2 f0 = pair(S.cf[CF_CCN]), f1 = pair(S.cf[CF_XR]), f2 = pair(S.cf[CF_YR]), f3 = pair(S.cf[CF_BI0]),
-                  f4 = pair(S.cf[CF_BI1]), f5 = pair(S.cf[CF_BRI]), f6 = pair(S.cf[CF_CR0]), f7 = pair(S.cf[CF_CR1]),
-                  f8 = pair(S.cf[CF_CIN]);
+    const double2 g0 = pair(S.cf[CF_B0]), gd = pair(S.cf[CF_DT]), g2 = pair(S.cf[CF_ATN]);
+    const double2 f1 = pair(S.cf[CF_XR]), f2 = pair(S.cf[CF_YR]), f3 = pair(S.cf[CF_BI0]), f5 = pair(S.cf[CF_BRI]),
+                  f6 = pair(S.cf[CF_CR0]), f8 = pair(S.cf[CF_CIN]);
 #pragma unroll
     for (int c = 0; c < 2; c++) {
       const int a = a0 + c;
       auto pk = [&](double2 v) { return c ? v.y : v.x; };
       const double bb = bw[4 + c];
-      const double ib = inv_bir(pk(g0), pk(g1), s2);
+      // B1, CCN, CR1 and BI1 are Dt times a^2, -1, 1 and -4a: the same
+      // products the column table holds, formed here to load 9 factors, not 12.
+      const double Dt = pk(gd);
+      const double ib = inv_bir(pk(g0), A.a2 * Dt, s2);
       const double ee = pk(g2) * ib + bb;  // Ataurho + bb
       const double dbdx = d1c(bw, 4 + c) * A.cx;
-      const double cc = pk(f0) * ib;
+      const double cc = -Dt * ib;
       const double btr = pk(f1) * ib;
       const double brr = pk(f2) * ib;
-      const double bti = (pk(f3) + pk(f4) * cs) * ib;
+      const double bti = (pk(f3) + (A.m4a * Dt) * cs) * ib;
       kbb[c] = bb;
       kee[c] = ee;
       kdim[c] = pk(f5) * ib - bb * bti;
-      kvre[c] = -(pk(f6) + pk(f7) * gth) * ib;
+      kvre[c] = -(pk(f6) + Dt * gth) * ib;
       kvim[c] = -pk(f8) * ib;
       kare[c] = -btr;
       kaim[c] = -bti;
@@ -985,7 +987,7 @@ cudaError_t encode_coef_maps(double *ctab, const double *coltab, const double *r
   const cuuint32_t box_bb[3] = {WC, TRb, 1};
   const cuuint64_t cdims[2] = {static_cast<cuuint64_t>(N), CF_COUNT};
   const cuuint64_t cstrides[1] = {static_cast<cuuint64_t>(N) * 8};
-  const cuuint32_t box_cf[2] = {TC, CF_COUNT};
+  const cuuint32_t box_cf[2] = {TC, CF_TILE};
   CUresult r1 = encode(&maps->coef_bb, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, ctab, dims, strides, box_bb, estr,
                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);

@@ -124,6 +124,8 @@ extern "C" int bhr_step_noalloc(const bhr_params *p, double *state, int nsteps, 
   A.cy = 0.05 * third * (1.0 / dth);
   A.cyy = 0.05 * third * third * (1.0 / dth) * (1.0 / dth);
   A.cko = 0.1 * 0.0625 * (1.0 / p->dt);
+  A.a2 = p->a * p->a;
+  A.m4a = -4.0 * p->a;
   for (int k = 0; k < nsteps; k++) {
     A.vin = state; A.un = state; A.out = u1;
     if (launch_stage(1, maps[0], A, st) != cudaSuccess) return fail(BHR_CUDA_ERROR, "stage 1 launch failed");

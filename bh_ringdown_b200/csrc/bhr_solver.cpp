@@ -826,6 +826,8 @@ StageArgs bhr::solver_stage_args(bhr_solver *s) {
   A.cy = 0.05 * third * odth;
   A.cyy = 0.05 * third * third * odth * odth;
   A.cko = 0.1 * 0.0625 * odt;
+  A.a2 = p.a * p.a;
+  A.m4a = -4.0 * p.a;
   return A;
 }
 
