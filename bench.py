@@ -372,7 +372,9 @@ def run_reference(args, rank, world):
     N, M = L.ref_N(), L.ref_M()
     w = WORKLOAD
     o = pyoracle.Oracle(N, M, w["Xmin"], w["Xmax"], w["a"], w["m"], 0.01)
-    x, r, th = o.grid()  # the reference's grid() with its NaN radii floored at r+
+    # the reference's grid(), except that the radii it leaves NaN near the horizon are floored at
+    # nextafter(r+), as the library does
+    x, r, th = o.grid()
     o.close()
     dx = (w["Xmax"] - w["Xmin"]) / N
     dt = w["courant"] * min(dx, r[0] * np.pi / M)
