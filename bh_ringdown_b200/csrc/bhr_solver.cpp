@@ -604,6 +604,10 @@ static void record_worker(bhr_solver *s, std::shared_ptr<RecordJob> job, int k_f
     s->rec_cv.notify_all();
   }
   if (up) cudaStreamDestroy(up);
+  // Stepping waits only while a thread may still publish the records it needs.
+  std::lock_guard<std::mutex> lock(s->rec_mu);
+  s->rec_running = false;
+  s->rec_cv.notify_all();
 }
 
 // Stops and joins a record thread (before its records are freed or replaced).
@@ -618,12 +622,22 @@ int bhr::solver_wait_records(bhr_solver *s, int upto) {
   if (!s->has_source) return BHR_OK;
   upto = std::min(upto, s->nt);
   std::unique_lock<std::mutex> lock(s->rec_mu);
-  s->rec_cv.wait(lock, [&] { return s->rec_ready >= upto || (s->rec_bad >= 0 && s->rec_bad < upto); });
+  if (s->rec_unusable) {
+    set_error("the last trajectory set on this solve failed; set one before stepping");
+    return BHR_INVALID_ARG;
+  }
+  s->rec_cv.wait(lock, [&] {
+    return s->rec_ready >= upto || (s->rec_bad >= 0 && s->rec_bad < upto) || !s->rec_running;
+  });
   if (s->rec_bad >= 0 && s->rec_bad < upto) {
     set_error("trajectory step " + std::to_string(s->rec_bad) +
               (s->rec_status == BHR_CUDA_ERROR ? ": record upload failed"
                                                : ": particle off the grid, inside the horizon or on a pole"));
     return s->rec_status;
+  }
+  if (s->rec_ready < upto) {
+    set_error("trajectory records end at step " + std::to_string(s->rec_ready));
+    return BHR_INVALID_ARG;
   }
   return BHR_OK;
 }
@@ -641,6 +655,13 @@ int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows) {
   cudaSetDevice(s->p.device);
   if (int st = flush_extract(s)) return st;
   stop_records(s);
+  {
+    // Until this call succeeds the solve has no usable records: a sourced
+    // solve whose trajectory change fails reports it at its next step.
+    std::lock_guard<std::mutex> lock(s->rec_mu);
+    s->rec_unusable = s->has_source;
+    s->rec_running = false;
+  }
   const bhr_params &p = s->p;
   const double a = p.a, mass = p.mass;
   const double rpl = mass + std::sqrt(mass * mass - a * a), rmn = mass - std::sqrt(mass * mass - a * a);
@@ -680,9 +701,21 @@ int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows) {
     s->rec_ready = k_first;
     s->rec_bad = -1;
     s->rec_status = BHR_OK;
+    s->rec_unusable = false;
+    s->rec_running = k_first < s->nt;
   }
-  if (k_first < s->nt) s->rec_thread = std::thread(record_worker, s, job, k_first);
   s->has_source = true;
+  if (k_first < s->nt) {
+    try {
+      s->rec_thread = std::thread(record_worker, s, job, k_first);
+    } catch (const std::exception &) {
+      std::lock_guard<std::mutex> lock(s->rec_mu);
+      s->rec_running = false;
+      s->rec_unusable = true;
+      set_error("could not start the trajectory record thread");
+      return BHR_OUT_OF_MEMORY;
+    }
+  }
   // The patch of the current step (later patches are built one step ahead).
   BHR_CUDA_TRY(launch_source(solver_source_args(s), s->stream));
   BHR_CUDA_TRY(cudaStreamSynchronize(s->stream));

@@ -61,6 +61,8 @@ struct bhr_solver {
   int rec_ready = 0;                // records on the device: steps [0, rec_ready)
   int rec_bad = -1;                 // first step whose record failed, or -1
   int rec_status = 0;               // its status
+  bool rec_running = false;         // a record thread may still publish records
+  bool rec_unusable = false;        // a trajectory change failed after the old records were dropped
 };
 
 

@@ -124,3 +124,29 @@ def test_bounded_wait_gives_up_and_the_device_stays_usable():
         s.step(5)
         t, h, _ = s.waveform()
         assert len(t) == 5 and np.all(np.isfinite(h))
+
+
+@pytest.mark.gpu
+@pytest.mark.timeout(300)
+def test_failed_trajectory_change_is_reported_at_the_next_step():
+    """A sourced solve whose second trajectory fails after the first one's
+    record thread was stopped: its next step reports that, instead of
+    stepping on the old records or waiting for records no thread publishes;
+    a good trajectory makes it usable again."""
+    from bh_ringdown_b200.trajectory import synthetic_plunge
+    prm = small_params(dt=0.05, T=500.0)  # 10000 steps: past the first 8192 records come from the thread
+    rows = synthetic_plunge(0.5, 0.025, duration=60.0)
+    with bhr.Solver(prm) as s:
+        s.set_trajectory(rows)
+        s.step(5)
+        bad = rows.copy()
+        bad[:, 1] = 1.0  # inside the horizon on every row
+        with pytest.raises(bhr.BhrError) as e:
+            s.set_trajectory(bad)
+        assert e.value.status == 1
+        with pytest.raises(bhr.BhrError) as e:
+            s.step(3)
+        assert e.value.status == 1 and "set one before stepping" in str(e.value)
+        s.set_trajectory(rows)
+        s.step(3)
+        assert s.info()["steps_done"] == 8
