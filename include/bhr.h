@@ -141,7 +141,9 @@ int bhr_solver_info(const bhr_solver *s, bhr_info *info);
  * this returns (a particle off the grid there is reported here); the rest
  * are built on a host thread while the solver steps, and a step call that
  * reaches a step whose particle is off the grid, inside the horizon or on a
- * pole returns that error (BHR_INVALID_ARG) without launching. */
+ * pole returns that error (BHR_INVALID_ARG) without launching.  If a call
+ * that replaces a trajectory fails, the solve keeps no usable records: its
+ * step calls return BHR_INVALID_ARG until a trajectory is set. */
 int bhr_solver_set_trajectory(bhr_solver *s, const double *rows, int nrows);
 int bhr_solver_load_trajectory(bhr_solver *s, const char *path);
 
