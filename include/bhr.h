@@ -276,7 +276,9 @@ void bhr_engine_destroy(bhr_engine *e);
 int bhr_engine_submit(bhr_engine *e, const bhr_params *p, const double *traj_rows, int nrows, int64_t *id);
 /* Admits what fits, advances all running solves by
  * min(max_steps, fewest steps any of them has left), retires the finished
- * ones; *running = solves still running. */
+ * ones; *running = solves still running.  If a bounded device wait of a
+ * stage kernel gives up, the running solves' fields are unknown: this and
+ * every later call return BHR_TIMEOUT, and the engine is to be destroyed. */
 int bhr_engine_step(bhr_engine *e, int max_steps, int *running);
 int bhr_engine_poll(bhr_engine *e, int64_t id, bhr_request_info *info);
 /* Waveform rows of a finished request (layout of bhr_solver_waveform). */
