@@ -402,10 +402,10 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
       return BHR_CUDA_ERROR;
     }
   }
-  if (int st = (tile_rows == 8 || tile_rows == 16) ? encode_maps(s, tile_rows) : autotune_rows(s)) {
+  if (int rc = (tile_rows == 8 || tile_rows == 16) ? encode_maps(s, tile_rows) : autotune_rows(s)) {
     free_all(s);
     delete s;
-    return st;
+    return rc;
   }
   *out = s;
   return BHR_OK;
