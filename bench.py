@@ -419,7 +419,7 @@ def run_reference(args, rank, world):
                       "N_r": N, "N_theta": M, "dt": dt, "integrator": "SSP-RK3",
                       "source": "synthetic prograde equatorial plunge from ISCO (reference Maple source)"},
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                            "sample": f"{args.steps} full steps (reference sourced + 12 step kernels, "
+                            "sample": f"{args.steps} full step{'s' if args.steps != 1 else ''} (reference sourced + 12 step kernels, "
                                       f"HighOrder/body.cu:108-165 order) on the {M}x{N} grid, host cores"},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
