@@ -285,6 +285,8 @@ int bhr_engine_poll(bhr_engine *e, int64_t id, bhr_request_info *info);
 int bhr_engine_result(bhr_engine *e, int64_t id, double *t, double *h, double *dedt, int max_rows, int *nrows);
 int bhr_engine_stats(bhr_engine *e, bhr_engine_counters *st);
 
+/* The reason for the last failed call made on the calling thread (the
+ * string is per thread and valid until that thread's next failing call). */
 const char *bhr_last_error_string(void);
 /* Device self-check of the bounded waits (no counterpart in the reference):
  * one block waits on a shared-memory barrier that nothing completes; the
