@@ -368,6 +368,15 @@ def run_reference(args, rank, world):
     from oracle import pyoracle
     D = C.c_double
     L = C.CDLL(lib_path)
+    # All of the host's threads, whatever OMP_NUM_THREADS the launcher set
+    # (torchrun sets 1): the library's OpenMP runtime, found by its soname.
+    threads = os.cpu_count() or 1
+    try:
+        gomp = C.CDLL("libgomp.so.1")
+        gomp.omp_set_num_threads(threads)
+        threads = int(gomp.omp_get_max_threads())
+    except (OSError, AttributeError):
+        threads = int(os.environ.get("OMP_NUM_THREADS", threads))
     L.ref_source.argtypes = [D] * 16
     N, M = L.ref_N(), L.ref_M()
     w = WORKLOAD
@@ -411,7 +420,6 @@ def run_reference(args, rank, world):
         timer += dt
     el = time.perf_counter() - t0
     value = N * M * args.steps / el
-    threads = os.cpu_count()
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
