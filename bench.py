@@ -261,11 +261,13 @@ def run_ours(args, rank, local_rank, world):
     info = s2.info()
     s2.close()
     t_e2e = time.perf_counter() - t0
-    # bytes the API copies host -> device: column and row tables, r_c and
+    if dist is not None:  # every rank ran its own e2e solve: the job takes the slowest
+        t_e2e = replicas.max_over_ranks(t_e2e, dist, device="cuda")
+    # bytes the API copies host -> device: column (14) and row (4) tables, r_c and
     # theta, projection and dE/dt weights, the separable initial-data factors
     # (Gaussian data), and one 128-byte source record per step of the run
     # (sourced; built and uploaded chunk by chunk while the device steps)
-    h2d = ((13 * N + 4 * M) + (N + M) + (7 * M + M)) * 8
+    h2d = ((14 * N + 4 * M) + (N + M) + (7 * M + M)) * 8
     if prm.init_kind == bhr.BHR_INIT_GAUSSIAN:
         h2d += (N + M) * 8
     if rows is not None:
