@@ -1,17 +1,19 @@
 #!/usr/bin/env python
 """Benchmark: grid-point updates per second of the FP64 Teukolsky step.
 
-Workload (the configuration the headline metric is quoted on): FP64
-plunge-driven ringdown, s=-2, m=2, a=0.9, M=1, r* (grid coordinate) in
-[-200, 600] with N_r=8192, N_theta=128, dt = 0.25 min(dx, r_min dtheta),
+Workload (default, the size the HBM-roofline target is quoted at): FP64
+plunge-driven ringdown, s=-2, m=2, a=0.9, M=1, grid coordinate in
+[-200, 600] with N_r=16384, N_theta=256, dt = 0.25 min(dx, r_min dtheta),
 source from a prograde equatorial plunge worldline sampled at dt/2 (a
 seeded synthetic stand-in for GenOT output: no GenOT inputs exist here).
+`--workload plunge` runs the same at 8192 x 128, `--workload grid16k` the
+16384 x 256 grid source-free.
 
 A step is one full time step (source patch, three SSP-RK3 stages,
-extraction) over the whole grid.  The solver's working set (three states
-of 32 MB plus tables) fits in the 126 MB L2, so L2 is flushed by writing a
-256 MB buffer between timed steps; each step is timed with CUDA events on
-the solver's stream and the per-kernel durations are summed.
+extraction) over the whole grid.  When the three states (96 B per point)
+exceed the 126 MB L2, the K timed steps run back to back between one pair
+of CUDA events on the solver's stream; otherwise L2 is flushed by writing
+a 256 MB buffer before each step and each step is timed alone.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -38,12 +40,19 @@ sys.path.insert(0, ROOT)
 METRIC = "grid-pt updates/s (%HBM roofline); solves/s, p99 latency vs FP64 plain @1e-6"
 UNIT = "grid-pt updates/s"
 WORKLOADS = {
-    # the headline configuration: plunge-driven ringdown, 8192 x 128
-    "plunge": dict(N=8192, M=128, Xmin=-200.0, Xmax=600.0, a=0.9, m=2.0, T=1000.0, courant=0.25),
-    # the size the HBM-roofline target is quoted at (16384 x 256), source-free
-    "grid16k": dict(N=16384, M=256, Xmin=-200.0, Xmax=600.0, a=0.9, m=2.0, T=1000.0, courant=0.25),
+    # plunge-driven ringdown at the size the HBM-roofline target is quoted at (the default)
+    "plunge16k": dict(N=16384, M=256, Xmin=-200.0, Xmax=600.0, a=0.9, m=2.0, T=1000.0, courant=0.25, source=True),
+    # the same physics at the plunge configuration's own grid, 8192 x 128
+    "plunge": dict(N=8192, M=128, Xmin=-200.0, Xmax=600.0, a=0.9, m=2.0, T=1000.0, courant=0.25, source=True),
+    # 16384 x 256, source-free (Gaussian pulse initial data)
+    "grid16k": dict(N=16384, M=256, Xmin=-200.0, Xmax=600.0, a=0.9, m=2.0, T=1000.0, courant=0.25, source=False),
 }
-WORKLOAD = WORKLOADS["plunge"]
+DEFAULT_WORKLOAD = "plunge16k"
+WORKLOAD = WORKLOADS[DEFAULT_WORKLOAD]
+# The reference's own kernels on host cores (oracle/_ref, built by
+# oracle/build_ref.py with the grid fixed at compile time), per workload.
+REFERENCE_LIBS = {"plunge16k": "libref_p16k.so", "plunge": "libref_cfg2.so"}
+L2_BYTES = 126 * 1024 * 1024
 BYTES_PER_PT = 256.0  # FP64 SSP-RK3 algorithmic bytes per point per step (coefficients recomputed)
 # Mixed precision: stage 1 reads u^n and writes u1 (FP64) and delta1 (FP32),
 # stage 2 reads delta1 and writes eps2 (FP32), stage 3 reads eps2 and u1 and
@@ -77,6 +86,7 @@ def profile_traffic(workload):
     committed ncu summary of this workload (line
     'dram_bytes_per_point_per_step: X'), or None."""
     name = {("plunge", "ssprk3"): "stage_kernel_plunge8192x128.txt",
+            ("plunge16k", "ssprk3"): "stage_dram_plunge16384x256.txt",
             ("grid16k", "ssprk3"): "stage_dram_grid16384x256.txt",
             ("grid16k", "rk4"): "stage_dram_rk4_grid16384x256.txt"}.get((workload, INTEGRATOR))
     if name is None:
@@ -187,6 +197,21 @@ def workload_inputs(with_source, device=0):
     return prm, None
 
 
+def workload_config(name, N, M, dt, with_source, world):
+    """The `config` dict of a single-solve workload; both arms (ours and
+    --impl reference) print exactly this dict for the same workload."""
+    w = WORKLOADS[name]
+    prec = "FP64" if PRECISION == "fp64" else "mixed FP64/FP32"
+    return {"workload": f"{name}: {prec} s=-2 m={w['m']:g} a={w['a']:g}, {N}x{M} on "
+                        f"[{w['Xmin']:g},{w['Xmax']:g}], "
+                        + ("plunge source" if with_source else "source-free (Gaussian pulse initial data)"),
+            "N_r": N, "N_theta": M, "dt": dt,
+            "integrator": "classical RK4" if INTEGRATOR == "rk4" else "SSP-RK3",
+            "precision": PRECISION,
+            "source": "synthetic prograde equatorial plunge from ISCO, rows every dt/2" if with_source else "none",
+            "parallelism": f"replicas x{world}"}
+
+
 def run_ours(args, rank, local_rank, world):
     import torch
     import bh_ringdown_b200 as bhr
@@ -197,54 +222,68 @@ def run_ours(args, rank, local_rank, world):
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    with_source = source_available() and args.workload == "plunge"
+    with_source = WORKLOAD["source"]
+    if with_source and not source_available():
+        raise SystemExit("the particle source coefficients are unavailable in this build")
     prm, rows = workload_inputs(with_source, device=local_rank)
     N, M = prm.N, prm.M
     solver = bhr.Solver(prm)
     if rows is not None:
         solver.set_trajectory(rows)
     tiling = solver.info()["tiling"]
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    # Three states of 32 B per point larger than L2: the timed steps run back
+    # to back (each reads what the previous one wrote from HBM); otherwise L2
+    # is flushed before each step and each step is timed alone.
+    resident = 3 * 32 * N * M <= L2_BYTES
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda") if resident else None
 
     def flush_l2():
         flush.zero_()
         torch.cuda.synchronize()
 
-    # warm-up, then the timed steps: each step is one captured-graph launch
-    # bracketed by CUDA events on the solver stream, with L2 flushed before it
-    for _ in range(args.warmup):
-        flush_l2()
-        solver.time_steps(1)
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
-    total_ms = 0.0
+    # clocks are sampled from the first warm-up step to the end of the
+    # per-kernel breakdown pass
     with ClockSampler(local_rank) as clk:
-        for _ in range(args.steps):
-            flush_l2()
-            total_ms += solver.time_steps(1)
+        for _ in range(args.warmup):
+            if resident:
+                flush_l2()
+            solver.time_steps(1)
+        if dist is not None:
+            dist.barrier()
         torch.cuda.synchronize()
-    torch.cuda.synchronize()
-    # per-kernel breakdown (eager launches, events around each kernel)
-    per_kernel = np.zeros(5)
-    for _ in range(args.steps):
-        flush_l2()
-        avg, _tot = solver.profile(1)
-        per_kernel += avg
-    torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
-        total_ms = replicas.max_over_ranks(total_ms, dist, device="cuda")
+        total_ms = 0.0
+        if resident:
+            for _ in range(args.steps):
+                flush_l2()
+                total_ms += solver.time_steps(1)
+        else:
+            total_ms = solver.time_steps(args.steps)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+            total_ms = replicas.max_over_ranks(total_ms, dist, device="cuda")
+        # per-kernel breakdown (eager launches, events around each kernel): not
+        # the timed figure, which is the graph-launched step above
+        nprof = min(args.steps, 20)
+        per_kernel = np.zeros(5)
+        for _ in range(nprof):
+            if resident:
+                flush_l2()
+            avg, _tot = solver.profile(1)
+            per_kernel += avg
+        torch.cuda.synchronize()
     clocks = clk.summary()
     solver.close()
 
     value = world * N * M * args.steps / (total_ms / 1e3)
     ms_per_step = total_ms / args.steps
-    stage_ms = per_kernel[1:4] / args.steps
     peak, peak_kind = measured_peak()
     bytes_pt = (BYTES_PER_PT_MIXED if PRECISION == "mixed" else
                 BYTES_PER_PT_RK4 if INTEGRATOR == "rk4" else BYTES_PER_PT)
-    achieved = bytes_pt * N * M / (float(stage_ms.sum()) / 1e3) / 1e9
+    # The stage kernels carry the step (the launch lists in profiles/ give
+    # their share); achieved = the step's algorithmic bytes over the device
+    # time of the graph-launched step, so it can only understate the kernels.
+    achieved = bytes_pt * N * M / (ms_per_step / 1e3) / 1e9
     traffic_pp = profile_traffic(args.workload) if PRECISION == "fp64" else None
 
     # End to end through the public API: host params + host trajectory in,
@@ -282,31 +321,33 @@ def run_ours(args, rank, local_rank, world):
         cpu = cpu_baseline(prm, rows, args.cpu_seconds)
 
     if rank == 0:
+        kernel_label = ("FP64 stage 1 + FP32 mixed_stage_kernel<2,3> (192 B/pt algorithmic)"
+                        if PRECISION == "mixed" else
+                        "stage kernels <1,4,4,5> (one classical RK4 step, 384 B/pt algorithmic)"
+                        if INTEGRATOR == "rk4" else
+                        "stage kernels <1,2,3> (one SSP-RK3 step, 256 B/pt algorithmic)")
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if PRECISION == "fp64" else "f64+f32", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {'FP64' if PRECISION == 'fp64' else 'mixed FP64/FP32'} "
-                                   f"s=-2 m=2 a=0.9, {N}x{M} on [-200,600]"
-                                   + (", plunge source" if with_source else ", source-free (Gaussian pulse initial data)"),
-                       "N_r": N, "N_theta": M, "dt": prm.dt,
-                       "integrator": "classical RK4" if INTEGRATOR == "rk4" else "SSP-RK3",
-                       "source": "synthetic prograde equatorial plunge from ISCO" if with_source else "none",
-                       "stage_tiling": tiling,
-                       "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}"},
+            "config": workload_config(args.workload, N, M, prm.dt, with_source, world),
+            "timing": {"l2": ("flushed (256 MB write) before each timed step, each step timed alone" if resident else
+                              f"working set {3 * 32 * N * M / 2**20:.0f} MiB > L2 (126 MiB): "
+                              f"{args.steps} steps back to back, no flush"),
+                       "events": "CUDA events on the solver stream around graph-launched steps",
+                       "stage_tiling": tiling},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": None if traffic_pp is None else traffic_pp * N * M,
-                         "kernel": ("FP64 stage 1 + FP32 mixed_stage_kernel<2,3> (192 B/pt algorithmic)"
-                                    if PRECISION == "mixed" else
-                                    "stage_kernel<1,4,4,5> (one classical RK4 step, 384 B/pt algorithmic)"
-                                    if INTEGRATOR == "rk4" else
-                                    "stage_kernel<1,2,3> (one SSP-RK3 step, 256 B/pt algorithmic)")},
-            "kernel_ms": {"source": per_kernel[0] / args.steps, "stage1": stage_ms[0], "stage2": stage_ms[1],
-                          "stage3+4" if INTEGRATOR == "rk4" else "stage3": stage_ms[2],
-                          "extract": per_kernel[4] / args.steps,
-                          "note": "source and extract run on a side stream beside stages 1 and 2; their "
-                                  "times run from the side stream's fork to the kernel's end"},
+                         "kernel": kernel_label,
+                         "basis": f"{bytes_pt:g} B/pt x {N}x{M} points per step / ms_per_step"},
+            "kernel_ms": {"source": per_kernel[0] / nprof, "stage1": per_kernel[1] / nprof,
+                          "stage2": per_kernel[2] / nprof,
+                          "stage3+4" if INTEGRATOR == "rk4" else "stage3": per_kernel[3] / nprof,
+                          "extract": per_kernel[4] / nprof,
+                          "note": "breakdown only: eager launches each timed alone (no programmatic overlap "
+                                  "between kernels); source and extract run on a side stream beside stages 1 "
+                                  "and 2, timed from the side stream's fork to the kernel's end"},
             # per step: the stages, the step-clock kernel, the extraction (of the
             # previous step, beside stage 2) and the source when there is one
             "gpu_launches": args.steps * ((6 if with_source else 5) + (1 if INTEGRATOR == "rk4" else 0)),
@@ -353,18 +394,19 @@ def cpu_baseline(prm, rows, seconds):
 
 def run_reference(args, rank, world):
     """The reference's own HighOrder kernels compiled for and run on this
-    host's cores (oracle/_ref/libref_cfg2.so), on the same workload."""
+    host's cores (oracle/_ref/libref_<tag>.so, its grid fixed at compile
+    time), on the same workload, config and metric as our arm."""
     if rank != 0:
         return
-    if args.workload != "plunge" or PRECISION != "fp64" or INTEGRATOR != "ssprk3":
-        print(json.dumps({"impl": "reference", "unavailable": "the reference's grid is fixed at compile time; "
-                                                               "oracle/_ref is built for the 8192x128 FP64 SSP-RK3 "
-                                                               "plunge workload only"}))
+    lib_name = REFERENCE_LIBS.get(args.workload)
+    if lib_name is None or PRECISION != "fp64" or INTEGRATOR != "ssprk3":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference integrates FP64 SSP-RK3 with a source; "
+                                                               f"oracle/_ref holds builds for {sorted(REFERENCE_LIBS)}"}))
         return
     import ctypes as C
-    lib_path = os.path.join(ROOT, "oracle", "_ref", "libref_cfg2.so")
+    lib_path = os.path.join(ROOT, "oracle", "_ref", lib_name)
     if not os.path.exists(lib_path):
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_cfg2.so was not built "
+        print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref/{lib_name} was not built "
                                                                "(the reference tree was absent at build time)"}))
         return
     from oracle import pyoracle
@@ -382,6 +424,7 @@ def run_reference(args, rank, world):
     L.ref_source.argtypes = [D] * 16
     N, M = L.ref_N(), L.ref_M()
     w = WORKLOAD
+    assert (N, M) == (w["N"], w["M"]), (lib_name, N, M)
     o = pyoracle.Oracle(N, M, w["Xmin"], w["Xmax"], w["a"], w["m"], 0.01)
     # the reference's grid(), except that the radii it leaves NaN near the horizon are floored at
     # nextafter(r+), as the library does
@@ -425,12 +468,11 @@ def run_reference(args, rank, world):
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "plunge-driven ringdown FP64, s=-2 m=2 a=0.9, 8192x128 on [-200,600]",
-                      "N_r": N, "N_theta": M, "dt": dt, "integrator": "SSP-RK3",
-                      "source": "synthetic prograde equatorial plunge from ISCO (reference Maple source)"},
+           "config": workload_config(args.workload, N, M, dt, True, world),
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                            "sample": f"{args.steps} full step{'s' if args.steps != 1 else ''} (reference sourced + 12 step kernels, "
-                                      f"HighOrder/body.cu:108-165 order) on the {M}x{N} grid, host cores"},
+                            "sample": f"{args.steps} full step{'s' if args.steps != 1 else ''} (reference sourced + "
+                                      f"12 step kernels, HighOrder/body.cu:108-165 order, source from the "
+                                      f"reference's Maple block) on the {M}x{N} grid, host cores"},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
@@ -684,13 +726,13 @@ def run_serve(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=2000)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch64", "serve"], default="plunge")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch64", "serve"], default=DEFAULT_WORKLOAD)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="fp64, or mixed: FP64 state and stage 1, FP32 corrections in stages 2 and 3")
     ap.add_argument("--integrator", choices=["ssprk3", "rk4"], default="ssprk3",

@@ -127,6 +127,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     sigs = {
         "bhr_abi_version": (I, []),
         "bhr_selftest_bounded_wait": (I, [I, C.POINTER(I)]),
+        "bhr_selftest_math": (I, [I, dp, I, dp]),
         "bhr_last_error_string": (C.c_char_p, []),
         "bhr_params_default": (I, [P(_Params)]),
         "bhr_grid": (I, [P(_Params), dp, dp, dp]),
@@ -189,8 +190,17 @@ def selftest_bounded_wait(device: int = 0) -> int:
     return st.value
 
 
+def selftest_math(x: np.ndarray, device: int = 0):
+    """(rcp, 1/x, sqrt, sqrt(x)) computed on the device: the library's
+    Newton-refined reciprocal and square root beside CUDA's own."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.zeros(4 * len(x))
+    _check(load_library().bhr_selftest_math(device, _ptr(x), len(x), _ptr(out)))
+    return out.reshape(4, len(x))
+
+
 def grid(params: Params):
-    """x_c[N], r_c[N], theta[M] of HighOrder/main.c:79-198."""
+    """x_c[N], r_c[N], theta[M] of HighOrder/main.c:64-183."""
     lib = load_library()
     x, r, t = np.zeros(params.N), np.zeros(params.N), np.zeros(params.M)
     p = params.to_c()

@@ -123,12 +123,13 @@ __device__ __forceinline__ double sqrt_nr(double x) {
 // 1/bir = 1/(B0 + B1 sin^2 theta) (HighOrder/kern.cu:132-149).
 __device__ __forceinline__ double inv_bir(double b0, double b1, double s2) { return rcp_nr(fma(b1, s2, b0)); }
 
-// Launch with programmatic stream serialisation allowed: the kernel may
-// begin while its predecessor on the stream drains, and holds every read
-// of the predecessor's results behind grid_dependency_wait().
+// Launch with programmatic stream serialisation allowed (pdl): the kernel
+// may begin while its predecessor on the stream drains, and holds every
+// read of the predecessor's results behind grid_dependency_wait().  Without
+// it the launch waits for the predecessor to complete, as a plain launch.
 template <class... KArgs, class... Args>
-static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                              Args &&...args) {
+static cudaError_t launch_ex(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                             cudaStream_t st, Args &&...args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
@@ -138,8 +139,13 @@ static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, s
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = pdl ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+template <class... KArgs, class... Args>
+static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args &&...args) {
+  return launch_ex(true, kernel, grid, block, smem, st, std::forward<Args>(args)...);
 }
 
 }  // namespace

@@ -1,6 +1,6 @@
 // bhr_engine.cpp -- many solves on one device, advanced together.
 //
-// The reference runs one solve per process (HighOrder/main.c:65-70 loops the
+// The reference runs one solve per process (HighOrder/main.c:50-55 loops the
 // m modes; TD_GPU_code/run.sh submits one job per trajectory).  The engine
 // keeps every admitted solve's fields and tables resident, admits queued
 // requests while the HBM budget allows, and advances all running solves with

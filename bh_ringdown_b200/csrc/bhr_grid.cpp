@@ -12,7 +12,7 @@ namespace {
 constexpr double kThirdH = 0.33333333333333333;  // HighOrder/kern.cu:46
 }
 
-// HighOrder/main.c:79-198.  x_c uniform on [Xmin, Xmax - dx]; theta_b =
+// HighOrder/main.c:64-183.  x_c uniform on [Xmin, Xmax - dx]; theta_b =
 // b*dtheta; x~ = x / Omega with the quartic hyperboloidal layer from
 // rin = Xmin + 0.64 (Xmax - Xmin); r(x~) by Newton iteration on the Kerr
 // tortoise coordinate, marching inwards from the outer point.  Where

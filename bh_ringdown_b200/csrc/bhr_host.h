@@ -28,7 +28,7 @@ struct Grid {
   std::vector<double> x_c, r_c, theta;
 };
 
-// Grid of HighOrder/main.c:79-198, with a horizon floor where the Newton
+// Grid of HighOrder/main.c:64-183, with a horizon floor where the Newton
 // iteration would step to r <= r+ (see grid.cpp).
 Grid make_grid(const bhr_params &p);
 // The same, into caller arrays (x_c, r_c, tx of N; theta of M); no allocation.

@@ -175,7 +175,11 @@ struct BatchTile {
 // null) the bare tile of all four planes for reading u^n.
 cudaError_t encode_state_maps(void *planes, int N, int M, int rows, CUtensorMap *tm_q, CUtensorMap *tm_p,
                               CUtensorMap *tm_u);
-cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st);
+// pdl = false launches without programmatic serialisation: the stage then
+// starts only once everything before it on the stream has completed (for a
+// first launch after tables were rewritten, which the stage kernels read
+// before their grid-dependency wait).
+cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st, bool pdl = true);
 cudaError_t launch_step_clock(RunState *rs, cudaStream_t st);
 // Per-point coefficient planes [bb | 1/bir | ee] (3 x M x N) from the tables,
 // and the tensor maps over them and over the column table.
@@ -200,6 +204,7 @@ cudaError_t launch_extract_batch(const ExtractArgs *args, int nsolves, cudaStrea
 cudaError_t launch_extract(const ExtractArgs &a, cudaStream_t st);
 cudaError_t launch_closure(double *planes, int N, int M, int even_m, cudaStream_t st);
 cudaError_t launch_wait_selftest(int *status, cudaStream_t st);
+cudaError_t launch_math_selftest(const double *x, int n, double *out, cudaStream_t st);
 cudaError_t launch_init_product(double *q, const double *fa, const double *gb, int N, int M, cudaStream_t st);
 size_t stage_smem_bytes();
 cudaError_t prepare_kernels();

@@ -1065,29 +1065,30 @@ static cudaError_t by_stage(const int stage, F &&f) {
   }
 }
 
-cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st) {
+cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st, bool pdl) {
   return by_stage(stage, [&](auto sc) {
     constexpr int S = decltype(sc)::value;
     if (a.narrow) {
       const size_t smem = sizeof(StageSmem<8>) + 128;
-      return launch_pdl(stage_narrow_kernel<S>, dim3(a.N / TC, a.M / 8), dim3(32, kNarrowThreads / 32), smem, st,
-                        maps, a);
+      return launch_ex(pdl, stage_narrow_kernel<S>, dim3(a.N / TC, a.M / 8), dim3(32, kNarrowThreads / 32), smem, st,
+                       maps, a);
     }
     if (a.ring) {
       const int ntiles = (a.N / TC) * (a.M / kRingRows);
-      return launch_pdl(stage_ring_kernel<S>, dim3(std::min(ntiles, kRingBlocksPerSM * sm_count())),
-                        dim3(32, kRingThreads / 32),
-                        ring_smem_bytes(), st, maps, a);
+      return launch_ex(pdl, stage_ring_kernel<S>, dim3(std::min(ntiles, kRingBlocksPerSM * sm_count())),
+                       dim3(32, kRingThreads / 32), ring_smem_bytes(), st, maps, a);
     }
     if (a.persist) {
       const int ntiles = (a.N / TC) * (a.M / kPersistRows);
-      return launch_pdl(stage_persistent_kernel<S>, dim3(std::min(ntiles, sm_count())),
-                        dim3(32, kPersistThreads / 32), persist_smem_bytes(), st, maps, a);
+      return launch_ex(pdl, stage_persistent_kernel<S>, dim3(std::min(ntiles, sm_count())),
+                       dim3(32, kPersistThreads / 32), persist_smem_bytes(), st, maps, a);
     }
     const dim3 block(32, STAGE_THREADS / 32);
     if (a.rows == 8)
-      return launch_pdl(stage_kernel<S, 8>, dim3(a.N / TC, a.M / 8), block, sizeof(StageSmem<8>) + 128, st, maps, a);
-    return launch_pdl(stage_kernel<S, 16>, dim3(a.N / TC, a.M / 16), block, sizeof(StageSmem<16>) + 128, st, maps, a);
+      return launch_ex(pdl, stage_kernel<S, 8>, dim3(a.N / TC, a.M / 8), block, sizeof(StageSmem<8>) + 128, st, maps,
+                       a);
+    return launch_ex(pdl, stage_kernel<S, 16>, dim3(a.N / TC, a.M / 16), block, sizeof(StageSmem<16>) + 128, st, maps,
+                     a);
   });
 }
 
@@ -1198,6 +1199,24 @@ __global__ void wait_selftest_kernel(int *status) {
 
 cudaError_t launch_wait_selftest(int *status, cudaStream_t st) {
   wait_selftest_kernel<<<1, 32, 0, st>>>(status);
+  return cudaGetLastError();
+}
+
+// Self-check of the Newton-refined reciprocal and square root the stage and
+// table kernels use, beside CUDA's own correctly rounded 1.0 / x and
+// sqrt(x): out = [rcp_nr(x) | 1.0 / x | sqrt_nr(x) | sqrt(x)], n each.
+__global__ void math_selftest_kernel(const double *x, int n, double *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double v = x[i];
+  out[i] = rcp_nr(v);
+  out[n + i] = 1.0 / v;
+  out[2 * n + i] = sqrt_nr(v);
+  out[3 * n + i] = sqrt(v);
+}
+
+cudaError_t launch_math_selftest(const double *x, int n, double *out, cudaStream_t st) {
+  math_selftest_kernel<<<(n + 255) / 256, 256, 0, st>>>(x, n, out);
   return cudaGetLastError();
 }
 

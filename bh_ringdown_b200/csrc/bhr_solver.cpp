@@ -179,6 +179,33 @@ int bhr_selftest_bounded_wait(int device, int *device_status) {
   }
   return BHR_OK;
 }
+int bhr_selftest_math(int device, const double *x, int n, double *out) {
+  if (!x || !out || n <= 0) return BHR_INVALID_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    set_error("no CUDA device");
+    return BHR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) return BHR_INVALID_ARG;
+  BHR_CUDA_TRY(cudaSetDevice(device));
+  cudaStream_t st = nullptr;
+  double *d = nullptr;
+  BHR_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  const size_t bytes = sizeof(double) * static_cast<size_t>(n);
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&d), 5 * bytes, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d, x, bytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = launch_math_selftest(d, n, d + n, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d + n, 4 * bytes, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (d) cudaFreeAsync(d, st);
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  if (e != cudaSuccess) {
+    set_error(std::string("math self-check: ") + cudaGetErrorString(e));
+    return BHR_CUDA_ERROR;
+  }
+  return BHR_OK;
+}
 const char *bhr_last_error_string(void) { return g_err.c_str(); }
 double bhr_swsh(double ell, double m, double theta) { return swsh(ell, m, theta); }
 

@@ -5,7 +5,8 @@ The reference takes its source worldline from GenOT
 Q).  GenOT's adiabatic inspiral inputs are not part of the reference tree,
 so workloads here use a stand-in: a prograde equatorial Kerr geodesic that
 starts just inside the ISCO with the ISCO energy and angular momentum and
-plunges; it is integrated in Boyer-Lindquist time with RK4 and sampled on a
+plunges; it is integrated in Boyer-Lindquist time with the 8th-order
+Dormand-Prince method (scipy's DOP853, dense output) and sampled on a
 uniform time grid (body.cu consumes two rows per step, so a run with step
 dt wants rows every dt/2).
 """

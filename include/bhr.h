@@ -6,7 +6,7 @@
  *   void body(double *r_c, double *theta, double dtheta, double mass,
  *             double aa, double ss, double mm, double dx, double dt,
  *             int p, int my_rank)                  (HighOrder/body.cu:25-27)
- * driven by main() (HighOrder/main.c:40-77) with the grid and run knobs as
+ * driven by main() (HighOrder/main.c:25-62) with the grid and run knobs as
  * compile-time macros (HighOrder/parm.h:1-13), a .traj text file as source
  * input (HighOrder/body.cu:77,97-120) and hm*.dat files as output
  * (HighOrder/body.cu:63-78,204-212).  The entry points below cover that
@@ -64,8 +64,8 @@ typedef enum bhr_tiling {
 } bhr_tiling;
 
 /* Run parameters.  Replaces HighOrder/parm.h:1-13 (N, M, Xmax, Xmin, Fr, T,
- * PTSX, PTSY) and the constants of HighOrder/main.c:55-61 (mass, aa, ss,
- * dt) plus the m loop of HighOrder/main.c:65.  s = -2 is fixed, as in the
+ * PTSX, PTSY) and the constants of HighOrder/main.c:40-46 (mass, aa, ss,
+ * dt) plus the m loop of HighOrder/main.c:50-55.  s = -2 is fixed, as in the
  * reference's coefficient formulas (HighOrder/kern.cu:142). */
 typedef struct bhr_params {
   int N;              /* radial points (multiple of 64)                      */
@@ -124,7 +124,7 @@ typedef struct bhr_info {
 
 typedef struct bhr_solver bhr_solver;
 
-/* Grid of HighOrder/main.c:79-198 (x_c[N], r_c[N], theta[M]); host only. */
+/* Grid of HighOrder/main.c:64-183 (x_c[N], r_c[N], theta[M]); host only. */
 int bhr_grid(const bhr_params *p, double *x_c, double *r_c, double *theta);
 
 /* Creates a solve: grid, coefficient tables, fields, initial data on the
@@ -235,14 +235,19 @@ double bhr_swsh(double ell, double m, double theta);
  * are rejected with BHR_INVALID_ARG.  Every GPU that loads the library
  * holds that array until the process exits.  The first call on a device
  * looks up the array's device address and sets the stage kernels'
- * shared-memory size; make that first call before any stream capture.  All
- * calls share the array and it keeps the last call's contents: calls that
- * overlap on the GPU (other streams, other host threads' streams) race. */
+ * shared-memory size.  Each call waits for its stream to finish and reads
+ * a status flag back, so it must not be called while that stream is being
+ * captured.  `stream` must belong to p->device; the calling thread's
+ * current device is restored on return.  All calls share the array and it
+ * keeps the last call's contents (a call with the same grid, spin, m and
+ * dt reuses the coefficient tables; the error flag is cleared every call):
+ * calls that overlap on the GPU (other streams, other host threads'
+ * streams) race. */
 int bhr_step_noalloc(const bhr_params *p, double *state, int nsteps, void *stream);
 
 /* ---- Batch engine: many solves per device, advanced together ----------
  * No counterpart in the reference, which runs one body() per process and
- * one process per (trajectory, m) job (HighOrder/main.c:65-70).  The
+ * one process per (trajectory, m) job (HighOrder/main.c:50-55).  The
  * engine queues requests, admits them in arrival order while their device
  * memory fits `hbm_budget_bytes` (one is always admitted when none runs),
  * and advances every running solve with one launch per RK stage over a
@@ -294,6 +299,13 @@ const char *bhr_last_error_string(void);
  * returns normally with *device_status = BHR_TIMEOUT, the same path a stage
  * kernel takes when its tile data never arrive.  The device stays usable. */
 int bhr_selftest_bounded_wait(int device, int *device_status);
+/* Device self-check of the hand-written FP64 reciprocal and square root
+ * (Newton-Raphson from the hardware approximations) that the stage and
+ * coefficient kernels use (no counterpart in the reference): for the n
+ * values x, out[0..n) = the reciprocal, out[n..2n) = CUDA's 1.0 / x,
+ * out[2n..3n) = the square root, out[3n..4n) = CUDA's sqrt(x), all computed
+ * on the device. */
+int bhr_selftest_math(int device, const double *x, int n, double *out);
 int bhr_abi_version(void);
 
 #ifdef __cplusplus

@@ -9,7 +9,10 @@ parm.h unchanged).  It then compiles them with oracle/ref_emu/ into
 oracle/_ref/libref_<tag>.so.  Nothing is copied out of the reference tree
 and nothing is written outside oracle/_ref/.
 
-Usage: python oracle/build_ref.py [--ref /root/reference] [tag ...]
+Usage: python oracle/build_ref.py [--ref <reference root>] [tag ...]
+
+The reference root is --ref, else $BHR_REFERENCE_ROOT, else a directory
+named `reference` beside this repository's root.
 """
 from __future__ import annotations
 
@@ -29,8 +32,9 @@ TAGS = {
     "pin": (256, 32, -50.0, 50.0),        # small reference-domain pin grid
     "c1s": (512, 64, -100.0, 300.0),      # config-1 domain, reduced grid
     "cfg2": (8192, 128, -200.0, 600.0),   # plunge-ringdown workload grid
+    "p16k": (16384, 256, -200.0, 600.0),  # the same domain at 16384 x 256 (the default bench workload)
 }
-DEFAULT_TAGS = ("pin", "c1s", "cfg2")
+DEFAULT_TAGS = ("pin", "c1s", "cfg2", "p16k")
 
 # main.c defines globals with the same names as kern.cu's device scalars;
 # they are renamed at compile time so both link into one library.
@@ -76,9 +80,15 @@ def build_tag(ref_root: str, tag: str) -> str:
     return lib
 
 
+def default_reference_root() -> str:
+    """$BHR_REFERENCE_ROOT, else `reference` beside the repository root."""
+    return os.environ.get("BHR_REFERENCE_ROOT",
+                          os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("BHR_REFERENCE_ROOT", "/root/reference"))
+    ap.add_argument("--ref", default=default_reference_root())
     ap.add_argument("tags", nargs="*", default=list(DEFAULT_TAGS))
     args = ap.parse_args(argv)
     if not os.path.isdir(os.path.join(args.ref, "TD_GPU_code", "HighOrder")):

@@ -54,7 +54,7 @@ enum { C_BB, C_CC, C_EE, C_ARE, C_AIM, C_DRE, C_DIM, C_VRE, C_VIM };
 static double *zalloc(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
 
 /* ---------------------------------------------------------------------- */
-/* grid(): HighOrder/main.c:79-198 (uniform x, theta; Omega layer; Newton
+/* grid(): HighOrder/main.c:64-183 (uniform x, theta; Omega layer; Newton
  * inversion of the Kerr tortoise coordinate from the outer end inwards). */
 static void orc_grid(orc_solver *s) {
   const int N = s->N, M = s->M;
@@ -323,8 +323,8 @@ orc_solver *orc_create(const orc_params *p) {
   s->N = p->N;
   s->M = p->M;
   if (s->p.ext_col < 0 || s->p.ext_col >= p->N) s->p.ext_col = p->N - 1;
-  s->dx = (p->Xmax - p->Xmin) / p->N;   /* main.c:59 */
-  s->dtheta = ORC_PI_PARM / p->M;       /* main.c:60 */
+  s->dx = (p->Xmax - p->Xmin) / p->N;   /* main.c:44 */
+  s->dtheta = ORC_PI_PARM / p->M;       /* main.c:45 */
   const size_t NM = (size_t)p->N * p->M;
   s->x_c = zalloc((size_t)p->N);
   s->r_c = zalloc((size_t)p->N);

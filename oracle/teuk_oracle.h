@@ -9,7 +9,7 @@
  * It restates, in plain C with OpenMP over theta rows, the algorithm of the
  * reference TD_GPU_code/HighOrder path (file:line citations are relative to
  * the reference project root):
- *   grid()                 HighOrder/main.c:79-198
+ *   grid()                 HighOrder/main.c:64-183
  *   kernel_init            HighOrder/kern.cu:84-169
  *   kernel_rhs1/2          HighOrder/kern.cu:171-299, 452-580
  *   kernel_update1/2/3     HighOrder/kern.cu:301-318, 582-620
@@ -66,7 +66,7 @@ typedef struct orc_solver orc_solver;
 orc_solver *orc_create(const orc_params *p);
 void orc_destroy(orc_solver *s);
 
-/* Grid (main.c:79-198): x_c[N], r_c[N], theta[M]. */
+/* Grid (main.c:64-183): x_c[N], r_c[N], theta[M]. */
 void orc_get_grid(const orc_solver *s, double *x_c, double *r_c, double *theta);
 /* Coefficient plane k in order bb,cc,ee,a_re,a_im,d_re,d_im,v_re,v_im. */
 void orc_get_coeff(const orc_solver *s, int k, double *out);

@@ -24,7 +24,9 @@ sys.path.insert(0, ROOT)
 from oracle import pyoracle  # noqa: E402
 
 D = C.c_double
-REF = os.environ.get("BHR_REFERENCE_ROOT", "/root/reference")
+from oracle.build_ref import default_reference_root  # noqa: E402
+
+REF = default_reference_root()
 
 
 def ref_lib(tag):
@@ -105,14 +107,25 @@ def particle_states(a):
     return out
 
 
-def source_case(L, a, m, timer):
+# Inclined states (theta-dot and its derivative non-zero, theta off the
+# equator on both hemispheres, retrograde phi-dot) for the later fixtures.
+def inclined_states():
+    return [
+        (6.5, 1.1, 0.4, 0.95, 2.2, 4.1, -0.01, -0.0005, 0.0, 0.03, -0.001, 0.0, 0.06, 0.0004),
+        (9.0, 2.0, 1.0, 0.96, -1.5, 6.0, 0.0, 0.0, 0.0, -0.02, 0.0005, 0.0, -0.03, 0.0),
+        (4.2, 0.8, 3.3, 0.9, 1.1, 8.5, -0.15, -0.02, 0.0, 0.05, 0.004, 0.0, 0.12, 0.003),
+        (12.0, 2.5, 5.5, 0.97, 0.9, 9.0, 0.02, 0.0001, 0.0, -0.008, -0.0002, 0.0, 0.01, -0.0001),
+    ]
+
+
+def source_case(L, a, m, timer, states=None):
     N, M = L.ref_N(), L.ref_M()
     Xmin, Xmax = L.ref_Xmin(), L.ref_Xmax()
     dx = (Xmax - Xmin) / N
     x, r, t = grid_and_init(L, 1.0, a, m, 0.25 * dx)
-    states = np.array(particle_states(a))
+    states = np.array(particle_states(a))[:4] if states is None else np.array(states)
     tre_all, tim_all = [], []
-    for s in states[:4]:
+    for s in states:
         rp, tp, phip, E, lz, Q, drdt, d2r, d3r, dth, d2th, d3th, dph, d2ph = s
         L.ref_source(D(0.0), D(timer), D(rp), D(phip), D(tp), D(E), D(lz), D(Q), D(drdt), D(d2r), D(d3r), D(dth),
                      D(d2th), D(d3th), D(dph), D(d2ph))
@@ -120,7 +133,7 @@ def source_case(L, a, m, timer):
         L.ref_get_source(p(tre), p(tim))
         tre_all.append(tre.reshape(M, N))
         tim_all.append(tim.reshape(M, N))
-    return dict(N=N, M=M, Xmin=Xmin, Xmax=Xmax, a=a, m=m, timer=timer, states=states[:4], tred=np.stack(tre_all),
+    return dict(N=N, M=M, Xmin=Xmin, Xmax=Xmax, a=a, m=m, timer=timer, states=states, tred=np.stack(tre_all),
                 timd=np.stack(tim_all))
 
 
@@ -155,6 +168,12 @@ def main():
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **d)
     np.savez_compressed(os.path.join(HERE, "source_pin_a06_m2.npz"), **source_case(L, 0.6, 2.0, 37.0))
     np.savez_compressed(os.path.join(HERE, "source_pin_a09_mneg3.npz"), **source_case(L, 0.9, -3.0, 12.5))
+    # a third and fourth (a, m): the inclined states, and the remaining
+    # equatorial/plunging ones
+    np.savez_compressed(os.path.join(HERE, "source_pin_a03_m1_inclined.npz"),
+                        **source_case(L, 0.3, 1.0, 41.0, inclined_states()))
+    np.savez_compressed(os.path.join(HERE, "source_pin_a095_m4_inclined.npz"),
+                        **source_case(L, 0.95, 4.0, 80.0, inclined_states() + particle_states(0.95)[3:]))
     np.savez_compressed(os.path.join(HERE, "proj_pin.npz"), **swsh_case(L, L.ref_M()))
     # The config-1 domain [-100, 300]: the reference's grid() returns NaN
     # radii near the inner edge (r - r+ below FP64 resolution).

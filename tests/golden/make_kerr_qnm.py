@@ -9,10 +9,14 @@ interpolates linearly in a.
   BHR_REFERENCE_ROOT=<reference checkout> python tests/golden/make_kerr_qnm.py
 """
 import os
+import sys
 
 import numpy as np
 
-ROOT = os.environ.get("BHR_REFERENCE_ROOT", "/root/reference")
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+from oracle.build_ref import default_reference_root  # noqa: E402
+
+ROOT = default_reference_root()
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "kerr_qnm.txt")
 FILES = [(2, 2, 0, "n1l2m2.dat"), (2, -2, 0, "n1l2mm2.dat"), (2, 2, 1, "n2l2m2.dat"), (2, -2, 1, "n2l2mm2.dat"),
          (3, 2, 0, "n1l3m2.dat")]

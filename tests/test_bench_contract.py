@@ -35,3 +35,11 @@ def test_reference_arm_prints_the_contract_line():
     e = d["e2e"]
     assert e["value"] == d["value"] and e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
     assert d["config"]["workload"]
+    # our arm prints the same config dict for the same workload (the dt rule
+    # on the product's grid, which is host code)
+    monkeypatch = pytest.MonkeyPatch()
+    monkeypatch.setattr(bench, "WORKLOAD", bench.WORKLOADS[bench.DEFAULT_WORKLOAD])
+    prm, rows = bench.workload_inputs(True)
+    ours = bench.workload_config(bench.DEFAULT_WORKLOAD, prm.N, prm.M, prm.dt, True, 1)
+    monkeypatch.undo()
+    assert ours == d["config"]

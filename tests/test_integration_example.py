@@ -11,7 +11,9 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = os.environ.get("BHR_REFERENCE_ROOT", "/root/reference")
+from oracle.build_ref import default_reference_root  # noqa: E402
+
+REF = default_reference_root()
 HO = os.path.join(REF, "TD_GPU_code", "HighOrder")
 LIB = os.path.join(ROOT, "bh_ringdown_b200", "libbhr.so")
 

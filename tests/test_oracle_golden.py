@@ -20,7 +20,7 @@ def test_grid_coefficients_and_evolution_match_reference(case):
     N, M = int(g["N"]), int(g["M"])
     o = pyoracle.Oracle(N, M, float(g["Xmin"]), float(g["Xmax"]), float(g["a"]), float(g["m"]), float(g["dt"]))
     x, r, t = o.grid()
-    # grid(): same arithmetic, bit for bit (HighOrder/main.c:79-198)
+    # grid(): same arithmetic, bit for bit (HighOrder/main.c:64-183)
     assert np.array_equal(x, g["x_c"]) and np.array_equal(r, g["r_c"]) and np.array_equal(t, g["theta"])
     if "coeffs_every4" in g:
         for k in range(9):

@@ -25,7 +25,8 @@ def product_coef_fn():
     return pyoracle.COEF_FN(fn)
 
 
-@pytest.mark.parametrize("name", ["source_pin_a06_m2", "source_pin_a09_mneg3"])
+@pytest.mark.parametrize("name", ["source_pin_a06_m2", "source_pin_a09_mneg3", "source_pin_a03_m1_inclined",
+                                  "source_pin_a095_m4_inclined"])
 def test_deposit_matches_reference(name):
     g = np.load(os.path.join(GOLD, name + ".npz"))
     N, M, a, m = int(g["N"]), int(g["M"]), float(g["a"]), float(g["m"])

@@ -10,7 +10,9 @@ import pytest
 import bh_ringdown_b200 as bhr
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
-REF = os.environ.get("BHR_REFERENCE_ROOT", "/root/reference")
+from oracle.build_ref import default_reference_root  # noqa: E402
+
+REF = default_reference_root()
 
 
 @pytest.mark.parametrize("fn,m", [("hm2_a0.7_thi000_thf090.0_n", 2.0), ("hmm1_a0.7_thi000_thf090.0_n", -1.0)])

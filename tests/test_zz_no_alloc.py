@@ -43,6 +43,25 @@ def test_noalloc_steps_match_the_solver_on_two_calls(m, a):
     ref.close()
 
 
+def test_noalloc_calls_with_different_spin_and_m_back_to_back():
+    """The scratch's coefficient tables follow the parameters of each call:
+    alternating (a, m) on one grid, each call checked against its own solver."""
+    import torch
+    cases = [params(2.0, 0.7), params(-3.0, 0.4), params(2.0, 0.7)]
+    refs = [bhr.Solver(prm) for prm in cases[:2]]
+    states = [torch.from_numpy(np.stack(r.get_state()).copy()).to("cuda") for r in refs]
+    torch.cuda.synchronize()
+    for i, prm in enumerate(cases):
+        j = i % 2
+        bhr.step_noalloc(prm, states[j].data_ptr(), 5)
+        refs[j].step(5)
+        want = np.stack(refs[j].get_state())
+        got = states[j].cpu().numpy()
+        assert np.max(np.abs(got - want)) <= FIELD_TOL * np.max(np.abs(want)), i
+    for r in refs:
+        r.close()
+
+
 def test_noalloc_rejects_grids_beyond_its_scratch():
     import torch
     prm = bhr.Params(N=1024, M=256, Xmin=-50.0, Xmax=50.0, a=0.5, m=2.0, dt=0.01)
