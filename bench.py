@@ -316,9 +316,10 @@ def run_ours(args, rank, local_rank, world):
            "d2h_bytes_per_step": int(d2h / n_e2e), "steps": n_e2e,
            "note": "wall clock of create + trajectory upload + steps + waveform readback + destroy"}
 
-    cpu = None
+    cpu = ref_gpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(prm, rows, args.cpu_seconds)
+        ref_gpu = reference_gpu_baseline(args.workload, prm)
 
     if rank == 0:
         kernel_label = ("FP64 stage 1 + FP32 mixed_stage_kernel<2,3> (192 B/pt algorithmic)"
@@ -354,10 +355,49 @@ def run_ours(args, rank, local_rank, world):
             "e2e": e2e,
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
         }
         print(json.dumps(out))
     if dist is not None:
         dist.destroy_process_group()
+
+
+# The reference's own GPU code (HighOrder/body.cu + kern.cu compiled unchanged
+# by nvcc for sm_100a, oracle/build_ref.py), per workload: its grid and final
+# time are fixed at compile time.
+REFERENCE_GPU_EXES = {"plunge16k": "refgpu_gp16k"}
+
+
+def reference_gpu_baseline(workload, prm):
+    """Wall clock of the reference's body() run on this GPU for the
+    workload's grid, spin, m and dt with the same synthetic plunge (its
+    whole loop: set-up, the sourced SSP-RK3 steps with a host sync after
+    every kernel, the per-step D2H copy and host projections), as grid-point
+    updates per second; None when the build is absent."""
+    import subprocess
+    import tempfile
+    from bh_ringdown_b200.trajectory import synthetic_plunge
+    exe = REFERENCE_GPU_EXES.get(workload)
+    if exe is None or PRECISION != "fp64" or INTEGRATOR != "ssprk3":
+        return None
+    path = os.path.join(ROOT, "oracle", "_ref", exe)
+    if not os.path.exists(path):
+        return {"unavailable": f"oracle/_ref/{exe} was not built (the reference tree was absent at build time)"}
+    rows = synthetic_plunge(prm.a, prm.dt / 2.0, duration=60.0)
+    with tempfile.TemporaryDirectory() as work:
+        os.makedirs(os.path.join(work, "Trajectories"))
+        os.makedirs(os.path.join(work, "run"))
+        np.savetxt(os.path.join(work, "Trajectories", "a0.0_thi000_thf090.0_n.traj"), rows, fmt="%.17g")
+        out = subprocess.run([path, work, repr(prm.a), repr(prm.m), repr(prm.dt)], capture_output=True, text=True,
+                             timeout=600)
+    if out.returncode != 0:
+        return {"unavailable": f"{exe} exited {out.returncode}: {out.stderr.strip()[-300:]}"}
+    info = json.loads(out.stdout.strip().splitlines()[-1])
+    return {"value": info["N"] * info["M"] * info["nt"] / info["seconds"], "unit": UNIT, "steps": info["nt"],
+            "seconds": info["seconds"], "kind": "reference",
+            "note": "the reference's body() (HighOrder/body.cu + kern.cu, compiled unchanged for sm_100a) on this "
+                    "GPU, wall clock of the whole call: set-up, sourced SSP-RK3 steps with a sync after each of "
+                    "its 14 kernels, per-step D2H copy and host projections"}
 
 
 def cpu_baseline(prm, rows, seconds):

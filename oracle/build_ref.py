@@ -1,13 +1,17 @@
 """Build recipe for oracle/_ref: the reference's own HighOrder code on CPU.
 
-TEST INFRASTRUCTURE ONLY.  For each grid tag this script makes a folder
+TEST INFRASTRUCTURE ONLY.  For each CPU grid tag this script makes a folder
 oracle/_ref/<tag>/ holding symlinks to the reference sources where they lie
 (TD_GPU_code/HighOrder/{kern.cu,mycmplx.h,main.c,proj.c}) and a grid header
 parm.h with the tag's N, M, Xmin, Xmax (the reference fixes these at compile
 time in HighOrder/parm.h:1-13; the "ho" tag links the reference's own
 parm.h unchanged).  It then compiles them with oracle/ref_emu/ into
-oracle/_ref/libref_<tag>.so.  Nothing is copied out of the reference tree
-and nothing is written outside oracle/_ref/.
+oracle/_ref/libref_<tag>.so.  For each GPU tag it links body.cu and kern.cu
+as well, compiled unchanged by nvcc for sm_100a, with the driver
+oracle/ref_gpu/ref_gpu_main.cpp into the executable oracle/_ref/refgpu_<tag>
+(the reference's own GPU code, run on the B200 as the reference-GPU
+baseline and for the host-loop fixture).  Nothing is copied out of the
+reference tree and nothing is written outside oracle/_ref/.
 
 Usage: python oracle/build_ref.py [--ref <reference root>] [tag ...]
 
@@ -34,7 +38,7 @@ TAGS = {
     "cfg2": (8192, 128, -200.0, 600.0),   # plunge-ringdown workload grid
     "p16k": (16384, 256, -200.0, 600.0),  # the same domain at 16384 x 256 (the default bench workload)
 }
-DEFAULT_TAGS = ("pin", "c1s", "cfg2", "p16k")
+DEFAULT_TAGS = ("pin", "c1s", "cfg2", "p16k", "gpin", "gp16k")
 
 # main.c defines globals with the same names as kern.cu's device scalars;
 # they are renamed at compile time so both link into one library.
@@ -86,6 +90,49 @@ def default_reference_root() -> str:
                           os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 
 
+# GPU builds of the reference itself (body.cu + kern.cu compiled unchanged by
+# nvcc for sm_100a, with oracle/ref_gpu/ref_gpu_main.cpp in place of main()'s m
+# loop): (N, M, Xmin, Xmax, T, Fr).  T fixes the step count, as parm.h does.
+GPU_TAGS = {
+    "gpin": (256, 32, -50.0, 50.0, 300.0, 50),         # host-loop fixture: rows from k dt >= Xmax + 200
+    "gp16k": (16384, 256, -200.0, 600.0, 4.4, 50),     # the default bench grid, ~1000 steps
+}
+NVCC_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def gpu_grid_header(n, m, xmin, xmax, t, fr):
+    return grid_header(n, m, xmin, xmax).replace("#define Fr 50\n#define T  1500.0\n",
+                                                 f"#define Fr {fr}\n#define T  {t!r}\n")
+
+
+def build_gpu_tag(ref_root: str, tag: str) -> str:
+    ho = os.path.join(ref_root, "TD_GPU_code", "HighOrder")
+    d = os.path.join(OUT, tag)
+    os.makedirs(d, exist_ok=True)
+    for name in ["kern.cu", "body.cu", "mycmplx.h", "main.c", "proj.c"]:
+        link = os.path.join(d, name)
+        if os.path.lexists(link):
+            os.remove(link)
+        os.symlink(os.path.join(ho, name), link)
+    with open(os.path.join(d, "parm.h"), "w") as f:
+        f.write(gpu_grid_header(*GPU_TAGS[tag]))
+    exe = os.path.join(OUT, f"refgpu_{tag}")
+    o = {k: os.path.join(d, k + ".o") for k in ("kern", "body", "main", "proj", "drv")}
+    nv = ["nvcc", *NVCC_ARCH, "-O3", "-w", "-I", d]
+    # body.cu writes two bytes into its one-byte `snum` (HighOrder/body.cu:61,67);
+    # without fortified sprintf that stays the reference's own behaviour instead of an abort
+    run(nv + ["-c", os.path.join(d, "kern.cu"), "-o", o["kern"]])
+    run(nv + ["-Xcompiler", "-U_FORTIFY_SOURCE", "-c", os.path.join(d, "body.cu"), "-o", o["body"]])
+    # main.c and proj.c as HighOrder/build.sh compiles them (g++, C++ linkage)
+    defs = [f"-D{v}=hmc_{v}" for v in MAIN_RENAMES] + ["-Dmain=hmc_main"]
+    run(["g++", "-x", "c++", "-O2", "-w", *defs, "-I", d, "-c", os.path.join(d, "main.c"), "-o", o["main"]])
+    run(["g++", "-x", "c++", "-O2", "-w", "-c", os.path.join(d, "proj.c"), "-o", o["proj"]])
+    run(["g++", "-O2", "-std=c++17", "-Wall", "-I", d, "-c", os.path.join(HERE, "ref_gpu", "ref_gpu_main.cpp"),
+         "-o", o["drv"]])
+    run(["nvcc", *NVCC_ARCH, "-o", exe, o["drv"], o["body"], o["kern"], o["main"], o["proj"], "-lm"])
+    return exe
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=default_reference_root())
@@ -94,13 +141,16 @@ def main(argv=None) -> int:
     if not os.path.isdir(os.path.join(args.ref, "TD_GPU_code", "HighOrder")):
         print(f"build_ref: reference not found at {args.ref}; skipping", file=sys.stderr)
         return 0
-    bad = [t for t in args.tags if t not in TAGS]
+    bad = [t for t in args.tags if t not in TAGS and t not in GPU_TAGS]
     if bad:
-        print(f"unknown tags {bad}; known {sorted(TAGS)}", file=sys.stderr)
+        print(f"unknown tags {bad}; known {sorted(TAGS) + sorted(GPU_TAGS)}", file=sys.stderr)
         return 2
     os.makedirs(OUT, exist_ok=True)
+
+    def build(t):
+        return build_tag(args.ref, t) if t in TAGS else build_gpu_tag(args.ref, t)
     with ThreadPoolExecutor(max_workers=len(args.tags)) as ex:
-        for lib in ex.map(lambda t: build_tag(args.ref, t), args.tags):
+        for lib in ex.map(build, args.tags):
             print("built", os.path.relpath(lib, os.path.dirname(HERE)))
     return 0
 

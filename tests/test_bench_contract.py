@@ -14,7 +14,7 @@ import bench  # noqa: E402
 
 
 @pytest.mark.parametrize("workload,integrator,algorithmic", [("plunge", "ssprk3", 256), ("grid16k", "ssprk3", 256),
-                                                             ("grid16k", "rk4", 384)])
+                                                             ("grid16k", "rk4", 384), ("plunge16k", "ssprk3", 256)])
 def test_committed_traffic_summaries_parse(workload, integrator, algorithmic, monkeypatch):
     monkeypatch.setattr(bench, "INTEGRATOR", integrator)
     t = bench.profile_traffic(workload)
