@@ -11,7 +11,10 @@ as well, compiled unchanged by nvcc for sm_100a, with the driver
 oracle/ref_gpu/ref_gpu_main.cpp into the executable oracle/_ref/refgpu_<tag>
 (the reference's own GPU code, run on the B200 as the reference-GPU
 baseline and for the host-loop fixture).  Nothing is copied out of the
-reference tree and nothing is written outside oracle/_ref/.
+reference tree and nothing is written outside oracle/_ref/.  The "dropin"
+tag links the reference's main.c and proj.c with this repository's
+bh_ringdown_b200/integration/body_bhr.c against libbhr.so into
+oracle/_ref/dropin_run (the drop-in as a maintainer would build it).
 
 Usage: python oracle/build_ref.py [--ref <reference root>] [tag ...]
 
@@ -38,7 +41,7 @@ TAGS = {
     "cfg2": (8192, 128, -200.0, 600.0),   # plunge-ringdown workload grid
     "p16k": (16384, 256, -200.0, 600.0),  # the same domain at 16384 x 256 (the default bench workload)
 }
-DEFAULT_TAGS = ("pin", "c1s", "cfg2", "p16k", "gpin", "gp16k")
+DEFAULT_TAGS = ("pin", "c1s", "cfg2", "p16k", "gpin", "gp16k", "dropin")
 
 # main.c defines globals with the same names as kern.cu's device scalars;
 # they are renamed at compile time so both link into one library.
@@ -133,6 +136,41 @@ def build_gpu_tag(ref_root: str, tag: str) -> str:
     return exe
 
 
+# The drop-in: the reference's own main.c (its m = -5..5 loop, aa = 1e-8,
+# dt = 0.002, HighOrder/main.c:40-55) and proj.c, with
+# bh_ringdown_b200/integration/body_bhr.c in place of body.cu and kern.cu,
+# linked to libbhr.so, for a small grid: (N, M, Xmin, Xmax, T, Fr).
+DROPIN_TAGS = {"dropin": (256, 32, -50.0, 50.0, 270.0, 50)}
+
+
+def build_dropin_tag(ref_root: str, tag: str) -> str:
+    ho = os.path.join(ref_root, "TD_GPU_code", "HighOrder")
+    d = os.path.join(OUT, tag)
+    os.makedirs(d, exist_ok=True)
+    for name in ["main.c", "proj.c"]:
+        link = os.path.join(d, name)
+        if os.path.lexists(link):
+            os.remove(link)
+        os.symlink(os.path.join(ho, name), link)
+    with open(os.path.join(d, "parm.h"), "w") as f:
+        f.write(gpu_grid_header(*DROPIN_TAGS[tag]))
+    repo = os.path.dirname(HERE)
+    libdir = os.path.join(repo, "bh_ringdown_b200")
+    if not os.path.exists(os.path.join(libdir, "libbhr.so")):
+        raise RuntimeError("build libbhr.so first (make -C bh_ringdown_b200/csrc)")
+    exe = os.path.join(OUT, f"{tag}_run")
+    objs = []
+    # as HighOrder/build.sh: g++ -O -c main.c proj.c (C++ linkage), then body_bhr.c the same way
+    for src in (os.path.join(d, "main.c"), os.path.join(d, "proj.c"),
+                os.path.join(repo, "bh_ringdown_b200", "integration", "body_bhr.c")):
+        obj = os.path.join(d, os.path.basename(src).replace(".c", ".o"))
+        run(["g++", "-x", "c++", "-O", "-w", "-I", d, "-I", os.path.join(repo, "include"), "-c", src, "-o", obj])
+        objs.append(obj)
+    rpath = os.path.relpath(libdir, OUT)
+    run(["g++", "-o", exe, *objs, "-L" + libdir, "-lbhr", f"-Wl,-rpath,$ORIGIN/{rpath}", "-lm"])
+    return exe
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=default_reference_root())
@@ -141,14 +179,16 @@ def main(argv=None) -> int:
     if not os.path.isdir(os.path.join(args.ref, "TD_GPU_code", "HighOrder")):
         print(f"build_ref: reference not found at {args.ref}; skipping", file=sys.stderr)
         return 0
-    bad = [t for t in args.tags if t not in TAGS and t not in GPU_TAGS]
+    bad = [t for t in args.tags if t not in TAGS and t not in GPU_TAGS and t not in DROPIN_TAGS]
     if bad:
-        print(f"unknown tags {bad}; known {sorted(TAGS) + sorted(GPU_TAGS)}", file=sys.stderr)
+        print(f"unknown tags {bad}; known {sorted(TAGS) + sorted(GPU_TAGS) + sorted(DROPIN_TAGS)}", file=sys.stderr)
         return 2
     os.makedirs(OUT, exist_ok=True)
 
     def build(t):
-        return build_tag(args.ref, t) if t in TAGS else build_gpu_tag(args.ref, t)
+        if t in TAGS:
+            return build_tag(args.ref, t)
+        return build_gpu_tag(args.ref, t) if t in GPU_TAGS else build_dropin_tag(args.ref, t)
     with ThreadPoolExecutor(max_workers=len(args.tags)) as ex:
         for lib in ex.map(build, args.tags):
             print("built", os.path.relpath(lib, os.path.dirname(HERE)))

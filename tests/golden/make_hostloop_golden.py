@@ -77,7 +77,7 @@ def main():
         text = open(files[0]).read()
     wave = np.array([[float(v) for v in ln.split()] for ln in text.strip().splitlines()])
     np.savez_compressed(os.path.join(args.out, "hostloop_gpin_a06_m2.npz"), N=N, M=M, Xmin=XMIN, Xmax=XMAX, T=T, Fr=FR,
-                        a=A, m=MM, dt=DT, traj_duration=TRAJ_DURATION, nt=info["nt"], wave=wave,
+                        a=A, m=MM, dt=DT, traj_duration=TRAJ_DURATION, traj=rows, nt=info["nt"], wave=wave,
                         wave_file=os.path.basename(files[0]), dedt=np.array(dedt), seconds=info["seconds"])
     print(json.dumps({"rows": len(wave), "dedt_lines": len(dedt), **info}))
 

@@ -1,8 +1,9 @@
-"""The C binding INTEGRATION.md gives a maintainer (body_bhr.c, in place of
-HighOrder/body.cu and kern.cu) compiles as C and as C++ against include/bhr.h
-and the reference's parm.h macros, and, built as the reference's build.sh
-builds main.c and proj.c (g++), links against libbhr.so.  Compile and link
-only: running it needs a GPU and the reference's trajectory files."""
+"""The C binding a maintainer adds to the reference
+(bh_ringdown_b200/integration/body_bhr.c, shown in INTEGRATION.md, in
+place of HighOrder/body.cu and kern.cu) compiles as C and as C++ against
+include/bhr.h and the reference's parm.h macros, and, built as the
+reference's build.sh builds main.c and proj.c (g++), links against
+libbhr.so.  tests/test_dropin.py runs the linked program on a GPU."""
 import os
 import re
 import shutil
@@ -34,11 +35,18 @@ PARM_H = """#define N 16000
 """
 
 
+SOURCE = os.path.join(ROOT, "bh_ringdown_b200", "integration", "body_bhr.c")
+
+
 def example_source():
+    return open(SOURCE).read()
+
+
+def test_integration_doc_shows_the_committed_source():
     text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
     m = re.search(r"```c\n(/\* body_bhr\.c.*?)```", text, re.S)
     assert m, "INTEGRATION.md has no body_bhr.c block"
-    return m.group(1)
+    assert m.group(1) == example_source()
 
 
 @pytest.fixture
