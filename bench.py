@@ -388,11 +388,13 @@ def reference_gpu_baseline(workload, prm):
         os.makedirs(os.path.join(work, "Trajectories"))
         os.makedirs(os.path.join(work, "run"))
         np.savetxt(os.path.join(work, "Trajectories", "a0.0_thi000_thf090.0_n.traj"), rows, fmt="%.17g")
-        out = subprocess.run([path, work, repr(prm.a), repr(prm.m), repr(prm.dt)], capture_output=True, text=True,
-                             timeout=600)
+        out = subprocess.run([path, work, "%.17g" % prm.a, "%.17g" % prm.m, "%.17g" % prm.dt], capture_output=True,
+                             text=True, timeout=600)
     if out.returncode != 0:
         return {"unavailable": f"{exe} exited {out.returncode}: {out.stderr.strip()[-300:]}"}
     info = json.loads(out.stdout.strip().splitlines()[-1])
+    if info["nt"] <= 0:
+        return {"unavailable": f"{exe} ran no steps: {info}"}
     return {"value": info["N"] * info["M"] * info["nt"] / info["seconds"], "unit": UNIT, "steps": info["nt"],
             "seconds": info["seconds"], "kind": "reference",
             "note": "the reference's body() (HighOrder/body.cu + kern.cu, compiled unchanged for sm_100a) on this "

@@ -75,6 +75,10 @@ int main(int argc, char **argv) {
   }
   const std::string work = argv[1];
   const double a = std::atof(argv[2]), mm = std::atof(argv[3]), dt = std::atof(argv[4]);
+  if (!(dt > 0.0) || !(std::fabs(a) < 1.0)) {
+    std::fprintf(stderr, "need dt > 0 and |a| < 1 (got a = %s, dt = %s)\n", argv[2], argv[4]);
+    return 2;
+  }
   hmc_mass = 1.0;
   hmc_aa = a;
   hmc_ss = -2.0;

@@ -58,7 +58,8 @@ def main():
         os.makedirs(os.path.join(work, "Trajectories"))
         os.makedirs(os.path.join(work, "run"))
         np.savetxt(os.path.join(work, "Trajectories", "a0.0_thi000_thf090.0_n.traj"), rows, fmt="%.17g")
-        out = subprocess.run([exe, work, repr(A), repr(MM), repr(DT)], capture_output=True, text=True, timeout=600)
+        out = subprocess.run([exe, work, "%.17g" % A, "%.17g" % MM, "%.17g" % DT], capture_output=True, text=True,
+                             timeout=600)
         if out.returncode != 0:
             raise SystemExit(f"refgpu_gpin failed ({out.returncode}):\n{out.stdout[-2000:]}\n{out.stderr[-2000:]}")
         lines = out.stdout.strip().splitlines()
