@@ -58,7 +58,7 @@ class _Info(C.Structure):
                 ("steps_done", I), ("rows_done", I), ("has_source", I), ("r_plus", D), ("device_bytes", C.c_size_t),
                 ("tile_rows", I), ("persistent", I), ("tiling", I)]
 
-TILINGS = ("block8", "block16", "persistent", "block8n", "ring")  # bhr_tiling, by value
+TILINGS = ("block8", "block16", "persistent", "block8n", "ring", "strip12")  # bhr_tiling, by value
 
 
 class _RequestInfo(C.Structure):

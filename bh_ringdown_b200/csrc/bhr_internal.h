@@ -124,6 +124,23 @@ struct StageMaps {
   CUtensorMap o;  // stage output planes, box {TC, rows, 4} (TMA stores)
 };
 
+// Fused stages 1 and 2 over column strips (tiling kTilingStrip12): the state
+// and bb planes read in 136-column x 4-row boxes.
+struct StripMaps {
+  CUtensorMap st, bb;
+};
+// Column strips of 120 output columns; theta segments of seg_rows stage-2
+// rows; one work item per (strip, segment).
+struct StripGeom {
+  int nstrips, segs, seg_rows;
+};
+StripGeom strip_geometry(int N, int M);
+size_t strip_smem_bytes();
+cudaError_t encode_strip_maps(double *state, double *ctab, int N, int M, StripMaps *maps);
+// Stages 1 and 2 of one SSP-RK3 step in one launch: reads u^n, writes u2
+// (a.out) on the interior; u1 stays in shared memory.
+cudaError_t launch_stage12_strip(const StripMaps &maps, const StageArgs &a, cudaStream_t st, bool pdl = true);
+
 // Mixed precision (BHR_MIXED): SSP-RK3 rearranged so that FP32 carries only
 // O(dt^2) corrections.  With delta1 = dt L(u^n) (L with the source) and L0
 // the homogeneous operator,
@@ -191,7 +208,14 @@ cudaError_t launch_source(const SourceArgs &a, cudaStream_t st);
 // persist = 1 walks the work-list with one block per SM (16-row tiles);
 // err receives BHR_TIMEOUT if a bounded wait gives up.
 // Stage tilings (the values of bhr_tiling): kernels and tile heights.
-enum StageTiling { kTilingBlock8 = 0, kTilingBlock16 = 1, kTilingPersistent = 2, kTilingBlock8n = 3, kTilingRing = 4 };
+enum StageTiling {
+  kTilingBlock8 = 0,
+  kTilingBlock16 = 1,
+  kTilingPersistent = 2,
+  kTilingBlock8n = 3,
+  kTilingRing = 4,
+  kTilingStrip12 = 5  // stages 1 and 2 fused (launch_stage12_strip), stage 3 as block8n
+};
 constexpr int tiling_rows(int tiling) {
   return (tiling == kTilingBlock8 || tiling == kTilingBlock8n || tiling == kTilingRing) ? 8 : 16;
 }

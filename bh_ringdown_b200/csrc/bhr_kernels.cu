@@ -192,30 +192,62 @@ __device__ __forceinline__ void tile_close(StageSmem<ROWS> &S, const StageArgs &
   }
 }
 
-// All threads: the right-hand side and the Shu-Osher combination of the
-// tile's rows, written to the stage output.
-// TO_SMEM (tiles without closure points): the outputs overwrite u^n in the
-// tile buffer (each thread reads its u^n before writing there) for a TMA
-// store of the whole tile.
-template <int STAGE, int ROWS, int THREADS, bool TO_SMEM>
-__device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs &A, const int c0, const int b0,
-                                             const int tx, const int ty) {
-  constexpr int RPT = ROWS / (THREADS / 32);  // rows per thread
+// Where the row work below puts a stage's output: global memory (the
+// stage output planes), the tile's own u^n buffer (TMA-stored afterwards by
+// the persistent kernels), or a shared-memory ring (the fused strip kernel).
+enum OutMode { kOutGlobal = 0, kOutTile = 1, kOutRing = 2 };
+
+// The source patch corner and buffer of the step a tile works on.
+struct SrcNote {
+  int c0, r0, buf;
+};
+
+// A tile's shared-memory inputs as the row work reads them.  Row pointers
+// are indexed by window column (w = 0 is the tile's first column minus 4);
+// cf(f) by 2 tx + the view's column offset; window row j of q is tile row
+// j - 3.
+template <int ROWS>
+struct TileView {
+  StageSmem<ROWS> &S;
+  __device__ __forceinline__ const double *qwin(int pl, int j) const { return &S.q[pl][j][0]; }
+  __device__ __forceinline__ const double *prow(int pl, int r) const { return &S.p[pl][r][0]; }
+  __device__ __forceinline__ const double *bbrow(int r) const { return &S.bb[r][0]; }
+  __device__ __forceinline__ const double *cf(int f) const { return S.cf[f]; }
+  __device__ __forceinline__ double rf(int f, int r) const { return S.rf[f][r]; }
+  __device__ __forceinline__ const double *unrow(int pl, int r) const { return &S.un[pl][r][0]; }
+  __device__ __forceinline__ double *outrow(int pl, int r) const { return &S.un[pl][r][0]; }
+};
+
+// The right-hand side and the Shu-Osher combination of RPT rows of one
+// 64-column row segment per warp (the thread's columns a0 = c0 + 2 tx and
+// a0 + 1, window column w0 = woff + 2 tx + 4), written to the stage output.
+// inner: every column of the segment is at least 4 from both radial ends
+// (no per-column end checks).  Outputs are stored for columns in
+// [st_lo, st_hi) (interior columns only); an inner segment stores all its
+// columns unless MASKED.  nrows: the tile's rows (for the source patch
+// overlap test).
+// kOutTile: the outputs overwrite u^n in the tile buffer (each thread reads
+// its u^n before writing there) for a TMA store of the whole tile.
+// kOutRing: the outputs go to the view's output rows at window column w0.
+template <int STAGE, int RPT, int OUT, bool MASKED, class View>
+__device__ __forceinline__ void tile_rows(const View &V, const StageArgs &A, const int c0, const int b0,
+                                          const int nrows, const int tx, const int ty, const int woff,
+                                          const bool inner, const int st_lo, const int st_hi, const SrcNote note) {
   const int N = A.N, M = A.M;
   const size_t NM = static_cast<size_t>(N) * M;
-  const bool lo_cols = (c0 == 0), hi_cols = (c0 + TC + 4 > N - 3);
   int src_c0 = 0, src_r0 = 0;
   bool tile_src = false;
   const double *srcp = A.src;
   if (A.src != nullptr) {
-    src_c0 = S.src_c0;
-    src_r0 = S.src_r0;
-    srcp = A.src + static_cast<size_t>(S.src_buf) * 2 * A.PTSX * A.PTSY;
-    tile_src = (src_c0 < c0 + TC) && (src_c0 + A.PTSX > c0) && (src_r0 < b0 + ROWS) && (src_r0 + A.PTSY > b0);
+    src_c0 = note.c0;
+    src_r0 = note.r0;
+    srcp = A.src + static_cast<size_t>(note.buf) * 2 * A.PTSX * A.PTSY;
+    tile_src = (src_c0 < c0 + TC) && (src_c0 + A.PTSX > c0) && (src_r0 < b0 + nrows) && (src_r0 + A.PTSY > b0);
   }
 
-  const int a0 = c0 + 2 * tx;  // this thread's columns a0, a0+1
-  const int w0 = 2 * tx + 4;   // their window column
+  const int a0 = c0 + 2 * tx;       // this thread's columns a0, a0+1
+  const int w0 = woff + 2 * tx + 4;  // their window column
+  const int cx0 = woff + 2 * tx;     // their index in the per-column arrays
   const double dt = A.dt;
 
   // Theta derivatives of q on all of this thread's rows
@@ -229,13 +261,13 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
     double f[RPT + 6][2];
 #pragma unroll
     for (int j = 0; j < RPT + 6; j++) {
-      const double2 t = *reinterpret_cast<const double2 *>(&S.q[pl][RPT * ty + j][w0]);
+      const double2 t = *reinterpret_cast<const double2 *>(V.qwin(pl, RPT * ty + j) + w0);
       f[j][0] = t.x;
       f[j][1] = t.y;
     }
 #pragma unroll
     for (int rr = 0; rr < RPT; rr++) {
-      const double ctan_cy = S.rf[RF_CTAN][RPT * ty + rr] * A.cy;
+      const double ctan_cy = V.rf(RF_CTAN, RPT * ty + rr) * A.cy;
 #pragma unroll
       for (int c = 0; c < 2; c++) {
         const double *g = &f[rr][0] + c;  // g[2 j] = row rr + j of column c
@@ -246,16 +278,16 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
     }
   }
 
-  // The row work, instantiated once for interior tiles (no per-column end
-  // checks) and once for tiles at a radial end.
+  // The row work, instantiated once for interior segments (no per-column
+  // end checks) and once for segments at a radial end.
   auto rows = [&](auto inner_tag) {
-  constexpr bool inner = decltype(inner_tag)::value;
+  constexpr bool in = decltype(inner_tag)::value;
 #pragma unroll 1
   for (int rr = 0; rr < RPT; rr++) {
     const int r = RPT * ty + rr;
     const int b = b0 + r;
     if (b < 3 || b >= M - 3) continue;
-    if (!inner && (a0 + 1 < 3 || a0 >= N - 3)) continue;
+    if (!in && (a0 + 1 < 3 || a0 >= N - 3)) continue;
     double ll[2][2];
 #pragma unroll
     for (int q = 0; q < RPT; q++)
@@ -267,23 +299,24 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
       }
 
     // Coefficients at the two points (HighOrder/kern.cu:132-158, 192-197).
-    const double cs = S.rf[RF_COS][r];
-    const double gth = S.rf[RF_G][r];
-    const double s2 = S.rf[RF_S2][r];
+    const double cs = V.rf(RF_COS, r);
+    const double gth = V.rf(RF_G, r);
+    const double s2 = V.rf(RF_S2, r);
     double kbb[2], kee[2], kdre[2], kdim[2], kare[2], kaim[2], kvre[2], kvim[2];
     double res[4][2];
     // bb on columns a0-4 .. a0+5, and the per-column arrays, as 16-byte pairs
     double bw[10];
+    const double *bbr = V.bbrow(r);
 #pragma unroll
     for (int j = 0; j < 5; j++) {
-      const double2 t = *reinterpret_cast<const double2 *>(&S.bb[r][w0 - 4 + 2 * j]);
+      const double2 t = *reinterpret_cast<const double2 *>(bbr + w0 - 4 + 2 * j);
       bw[2 * j] = t.x;
       bw[2 * j + 1] = t.y;
     }
-    auto pair = [&](const double *base) { return *reinterpret_cast<const double2 *>(base + 2 * tx); };
-    const double2 g0 = pair(S.cf[CF_B0]), gd = pair(S.cf[CF_DT]), g2 = pair(S.cf[CF_ATN]);
-    const double2 f1 = pair(S.cf[CF_XR]), f2 = pair(S.cf[CF_YR]), f3 = pair(S.cf[CF_BI0]), f5 = pair(S.cf[CF_BRI]),
-                  f6 = pair(S.cf[CF_CR0]), f8 = pair(S.cf[CF_CIN]);
+    auto pair = [&](const double *base) { return *reinterpret_cast<const double2 *>(base + cx0); };
+    const double2 g0 = pair(V.cf(CF_B0)), gd = pair(V.cf(CF_DT)), g2 = pair(V.cf(CF_ATN));
+    const double2 f1 = pair(V.cf(CF_XR)), f2 = pair(V.cf(CF_YR)), f3 = pair(V.cf(CF_BI0)), f5 = pair(V.cf(CF_BRI)),
+                  f6 = pair(V.cf(CF_CR0)), f8 = pair(V.cf(CF_CIN));
 #pragma unroll
     for (int c = 0; c < 2; c++) {
       const int a = a0 + c;
@@ -325,7 +358,7 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
     double fc[4][2];
 #pragma unroll
     for (int pl = 0; pl < 4; pl++) {
-      const double *row = pl < 2 ? &S.q[pl][r + 3][0] : &S.p[pl - 2][r][0];
+      const double *row = pl < 2 ? V.qwin(pl, r + 3) : V.prow(pl - 2, r);
       double v[10];
 #pragma unroll
       for (int j = 0; j < 5; j++) {
@@ -338,7 +371,7 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
         const int a = a0 + c;
         const double f0 = v[4 + c];
         const double fx = d1c(v, 4 + c) * A.cx;
-        const double fk = (inner || (a >= 4 && a < N - 4)) ? ko8c(v, 4 + c) * A.cko : 0.0;
+        const double fk = (in || (a >= 4 && a < N - 4)) ? ko8c(v, 4 + c) * A.cko : 0.0;
         fc[pl][c] = f0;
         // each term folded into its accumulator by one FMA (res[0] and
         // res[1] start with the q planes' terms)
@@ -366,13 +399,13 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
     // HighOrder/kern.cu:301-318, 582-620), or classical RK4 (stage 1 with
     // dt/2, then stages 4, 4 and 5).
     const size_t base = static_cast<size_t>(b) * N + a0;
-    const bool both = inner || ((a0 >= 3) && (a0 + 1 < N - 3));
+    const bool both = (in && !MASKED) || ((a0 >= st_lo) && (a0 + 1 < st_hi));
     auto store2 = [&](double *dst, const double v0, const double v1) {
       if (both) {
         *reinterpret_cast<double2 *>(dst) = make_double2(v0, v1);
       } else {
-        if (a0 >= 3 && a0 < N - 3) dst[0] = v0;
-        if (a0 + 1 >= 3 && a0 + 1 < N - 3) dst[1] = v1;
+        if (a0 >= st_lo && a0 < st_hi) dst[0] = v0;
+        if (a0 + 1 >= st_lo && a0 + 1 < st_hi) dst[1] = v1;
       }
     };
 #pragma unroll
@@ -387,12 +420,12 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
           if (both) {
             *reinterpret_cast<float2 *>(fd) = make_float2(d0, d1);
           } else {
-            if (a0 >= 3 && a0 < N - 3) fd[0] = d0;
-            if (a0 + 1 >= 3 && a0 + 1 < N - 3) fd[1] = d1;
+            if (a0 >= st_lo && a0 < st_hi) fd[0] = d0;
+            if (a0 + 1 >= st_lo && a0 + 1 < st_hi) fd[1] = d1;
           }
         }
       } else {
-        const double2 u = *reinterpret_cast<const double2 *>(&S.un[pl][r][2 * tx]);
+        const double2 u = *reinterpret_cast<const double2 *>(V.unrow(pl, r) + cx0);
         if (STAGE == 2) {
           o[0] = 0.25 * (3.0 * u.x + fc[pl][0] + dt * res[pl][0]);
           o[1] = 0.25 * (3.0 * u.y + fc[pl][1] + dt * res[pl][1]);
@@ -415,16 +448,30 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
           o[1] = u.y + kThird * fc[pl][1] + dt * res[pl][1];
         }
       }
-      if (TO_SMEM) {
-        *reinterpret_cast<double2 *>(&S.un[pl][r][2 * tx]) = make_double2(o[0], o[1]);
-        continue;
+      if (OUT == kOutTile) {
+        *reinterpret_cast<double2 *>(V.outrow(pl, r) + cx0) = make_double2(o[0], o[1]);
+      } else if (OUT == kOutRing) {
+        store2(V.outrow(pl, r) + w0, o[0], o[1]);
+      } else {
+        store2(A.out + pl * NM + base, o[0], o[1]);
       }
-      store2(A.out + pl * NM + base, o[0], o[1]);
     }
   }
   };
-  if (!lo_cols && !hi_cols) rows(std::true_type{});
+  if (inner) rows(std::true_type{});
   else rows(std::false_type{});
+}
+
+// All threads: the right-hand side and the Shu-Osher combination of the
+// tile's rows, written to the stage output (TO_SMEM: into the tile's u^n
+// buffer, for tiles without closure points).
+template <int STAGE, int ROWS, int THREADS, bool TO_SMEM>
+__device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs &A, const int c0, const int b0,
+                                             const int tx, const int ty) {
+  const bool lo_cols = (c0 == 0), hi_cols = (c0 + TC + 4 > A.N - 3);
+  const SrcNote note{S.src_c0, S.src_r0, S.src_buf};
+  tile_rows<STAGE, ROWS / (THREADS / 32), TO_SMEM ? kOutTile : kOutGlobal, false>(
+      TileView<ROWS>{S}, A, c0, b0, ROWS, tx, ty, 0, !lo_cols && !hi_cols, 3, A.N - 3, note);
 }
 
 // One tile per block (grid N/64 x M/ROWS, two blocks per SM).
@@ -681,6 +728,306 @@ __global__ void __launch_bounds__(kNarrowThreads, 4)
   const BatchTile t = tiles[blockIdx.x];
   const BatchSolve &B = solves[t.solve];
   stage_tile<STAGE, 8, kNarrowThreads>(B.maps[STAGE - 1], B.args[STAGE - 1], t.c0, t.b0);
+}
+
+// ---- stages 1 and 2 fused over column strips (the strip12 tiling) --------
+// One 512-thread block per SM walks work items (column strip, theta
+// segment).  A strip computes both stages on kStripCols = 128 columns (two
+// 64-column warp segments): stage 1 from u^n into a shared-memory ring that
+// holds u1, stage 2 from that ring.  Stage 2's outputs are stored on the
+// strip's middle kStripOut = 120 columns only (its outer 4 on each side read
+// stage-1 values outside the computed columns), so strips overlap by 8
+// columns and u1 never goes to HBM: per grid point the launch reads u^n and
+// bb (40 B) and writes u2 (32 B), where separate stage-1 and stage-2
+// launches move 64 + 96 B (+16 B of bb).
+// Rows go down a segment in phases of kStripG = 4: in phase p warps 0-7
+// compute stage 1 on rows [R, R + 4), R = s1_lo + 4 p, and warps 8-15
+// compute stage 2 on rows [R - 7, R - 3), whose theta stencil reaches u1
+// rows up to R - 1, finished in earlier phases; one warp per row segment.
+// The u^n rows reach shared memory by TMA one phase ahead (q planes 7 rows
+// ahead of stage 1's rows, p planes and bb 4 rows ahead); column factors and
+// row factors are loaded once per item.  At the start of every phase the
+// closures of what arrived (u^n) and of what stage 1 finished (u1) are
+// rebuilt in the rings, with the extrapolation order of the other kernels
+// (HighOrder/kern.cu:320-449): pole rows of the q planes on columns
+// [3, N-3), radial ends of all planes on interior rows.  Results are
+// bit-identical to the separate stage kernels: every point is computed by
+// the same row work (tile_rows) from the same values.
+constexpr int kStripThreads = 512;
+constexpr int kStripCols = 2 * TC;            // computed columns per strip
+constexpr int kStripOut = kStripCols - 8;     // stage-2 output columns per strip
+constexpr int kStripWin = kStripCols + 8;     // window columns (stencils reach +-4)
+constexpr int kStripG = 4;                    // rows per phase
+constexpr int kStripLag = kStripG + 3;        // stage 2 trails stage 1 by this many rows
+constexpr int kQRing = 24;                    // u^n q rows held (six 4-row chunks)
+constexpr int kPRing = 16;                    // u^n p and bb rows held, and u1 rows (four chunks)
+constexpr int kStripMaxRows = 264;            // stage-1 rows of one item (row-factor buffer)
+
+struct __align__(128) StripSmem {
+  alignas(128) double qn[2][kQRing][kStripWin];  // TMA boxes {136, 4, 1}: u^n q_re, q_im
+  alignas(128) double pn[2][kPRing][kStripWin];  // u^n p_re, p_im
+  alignas(128) double bb[kPRing][kStripWin];     // bb
+  alignas(128) double q1[2][kPRing][kStripWin];  // u1 q_re, q_im (stage 1 output)
+  alignas(128) double p1[2][kPRing][kStripWin];  // u1 p_re, p_im
+  alignas(16) double cf[CF_TILE][kStripCols];    // column factors of the computed columns
+  alignas(16) double rf[RF_COUNT][kStripMaxRows];  // row factors of the item's rows
+  uint64_t bar[2];                               // loads of even / odd phases
+  int src_c0, src_r0, src_buf;
+};
+BHR_TMA_ALIGNED(StripSmem, qn);
+BHR_TMA_ALIGNED(StripSmem, pn);
+BHR_TMA_ALIGNED(StripSmem, bb);
+static_assert((4 * kStripWin * 8) % 128 == 0, "4-row TMA chunks must keep 128-byte alignment");
+static_assert(sizeof(StripSmem) + 128 <= 227 * 1024, "strip buffers exceed shared memory");
+
+// One item: column strip `s` (stage-2 outputs on columns [120 s, 120 s + 120)),
+// stage-2 rows [s2_lo, s2_hi), stage-1 rows [s1_lo, s1_hi).
+struct StripItem {
+  int cs;        // first computed column: 120 s - 4
+  int s1_lo, s1_hi, s2_lo, s2_hi;
+  int st_lo, st_hi;  // stage-2 output columns
+};
+
+__device__ __forceinline__ StripItem strip_item(const StripGeom &G, const int N, const int M, const int item) {
+  const int s = item % G.nstrips, g = item / G.nstrips;
+  StripItem it;
+  it.cs = kStripOut * s - 4;
+  it.s2_lo = 3 + g * G.seg_rows;
+  it.s2_hi = min(M - 3, it.s2_lo + G.seg_rows);
+  it.s1_lo = max(3, it.s2_lo - 3);
+  it.s1_hi = min(M - 3, it.s2_hi + 3);
+  it.st_lo = max(3, kStripOut * s);
+  it.st_hi = min(N - 3, kStripOut * s + kStripOut);
+  return it;
+}
+
+// Ring rows: u^n q rows by (r - s1_lo + 5) mod 24 (no q row below
+// s1_lo - 5 is read), everything else by (r - s1_lo) mod 16 (no row below
+// s1_lo - 10 is read).  The 4-row TMA chunks land on 4-row-aligned slots.
+static_assert(kPRing == 16, "pslot masks with 15");
+__device__ __forceinline__ int qslot(int r, int base) {
+  return static_cast<int>(static_cast<unsigned>(r - base + 5) % kQRing);
+}
+__device__ __forceinline__ int pslot(int r, int base) { return (r - base + 32) & (kPRing - 1); }
+
+// The views the row work reads: stage 1 (u^n rings in, u1 ring out) and
+// stage 2 (u1 rings in, u^n as the u^n term, global out).
+template <int STAGE>
+struct StripView {
+  StripSmem &S;
+  int b0, base, rf0, woff;
+  __device__ __forceinline__ const double *qwin(int pl, int j) const {
+    const int r = b0 - 3 + j;
+    return STAGE == 1 ? &S.qn[pl][qslot(r, base)][0] : &S.q1[pl][pslot(r, base)][0];
+  }
+  __device__ __forceinline__ const double *prow(int pl, int r) const {
+    return STAGE == 1 ? &S.pn[pl][pslot(b0 + r, base)][0] : &S.p1[pl][pslot(b0 + r, base)][0];
+  }
+  __device__ __forceinline__ const double *bbrow(int r) const { return &S.bb[pslot(b0 + r, base)][0]; }
+  __device__ __forceinline__ const double *cf(int f) const { return S.cf[f]; }
+  __device__ __forceinline__ double rf(int f, int r) const { return S.rf[f][b0 + r - rf0]; }
+  // u^n at row b0 + r, indexed by the per-column index (window column - 4)
+  __device__ __forceinline__ const double *unrow(int pl, int r) const {
+    return (pl < 2 ? &S.qn[pl][qslot(b0 + r, base)][0] : &S.pn[pl - 2][pslot(b0 + r, base)][0]) + 4;
+  }
+  __device__ __forceinline__ double *outrow(int pl, int r) const {
+    return pl < 2 ? &S.q1[pl][pslot(b0 + r, base)][0] : &S.p1[pl - 2][pslot(b0 + r, base)][0];
+  }
+};
+
+// Extrapolation closure rows of one plane row set, in the ring: the pole
+// rows (q planes) on window columns whose grid column is in [3, N-3), and
+// the radial ends (all planes) of the given interior rows.
+__device__ __forceinline__ void ring_close_poles(double (*q)[kStripWin], const bool top, const int M, const int N,
+                                                 const int cs, const int base, const int even_m, const int tid,
+                                                 bool qring) {
+  auto row = [&](int r) { return q[qring ? qslot(r, base) : pslot(r, base)]; };
+  for (int w = tid; w < kStripWin; w += kStripThreads) {
+    const int a = cs - 4 + w;
+    if (a < 3 || a >= N - 3) continue;
+    if (top) {
+      if (even_m) {
+        row(2)[w] = (4.0 * row(3)[w] - row(4)[w]) * kThird;
+        row(1)[w] = (4.0 * row(2)[w] - row(3)[w]) * kThird;
+        row(0)[w] = (4.0 * row(1)[w] - row(2)[w]) * kThird;
+      } else {
+        row(2)[w] = 0.0; row(1)[w] = 0.0; row(0)[w] = 0.0;
+      }
+    } else {
+      if (even_m) {
+        row(M - 3)[w] = (4.0 * row(M - 4)[w] - row(M - 5)[w]) * kThird;
+        row(M - 2)[w] = (4.0 * row(M - 3)[w] - row(M - 4)[w]) * kThird;
+        row(M - 1)[w] = (4.0 * row(M - 2)[w] - row(M - 3)[w]) * kThird;
+      } else {
+        row(M - 3)[w] = 0.0; row(M - 2)[w] = 0.0; row(M - 1)[w] = 0.0;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void close_end_row(double *row, const int N, const int cs) {
+  const int o = 4 - cs;  // window column of grid column a is a + o
+  if (cs - 4 < 3) {
+    row[2 + o] = (4.0 * row[3 + o] - row[4 + o]) * kThird;
+    row[1 + o] = (4.0 * row[2 + o] - row[3 + o]) * kThird;
+    row[0 + o] = (4.0 * row[1 + o] - row[2 + o]) * kThird;
+  }
+  // high end: only the closure columns inside the window (the last of
+  // them may lie beyond it, where no computed column's stencil reaches)
+  if (cs - 4 + kStripWin > N - 3) {
+    if (N - 3 + o < kStripWin) row[N - 3 + o] = (4.0 * row[N - 4 + o] - row[N - 5 + o]) * kThird;
+    if (N - 2 + o < kStripWin) row[N - 2 + o] = (4.0 * row[N - 3 + o] - row[N - 4 + o]) * kThird;
+    if (N - 1 + o < kStripWin) row[N - 1 + o] = (4.0 * row[N - 2 + o] - row[N - 3 + o]) * kThird;
+  }
+}
+
+// Thread 0: the loads a phase needs beyond the earlier phases' (first == true:
+// everything phase 0 needs), on that phase's barrier.  q planes: rows
+// [R + 3, R + 7) (first: [R - 5, R + 7)); p planes and bb: rows [R, R + 4).
+__device__ __forceinline__ void strip_issue(StripSmem &S, const StripMaps &T, const StripItem &it, const int R,
+                                            const bool first, uint64_t *bar) {
+  const uint32_t chunk = 4 * kStripWin * sizeof(double);
+  const int nq = first ? 3 : 1;
+  mbar_expect_tx(bar, chunk * (2 * nq + 2 + 1));
+  const int x = it.cs - 4;
+  for (int c = 0; c < nq; c++) {
+    const int r = first ? R - 5 + 4 * c : R + 3;
+    const int sl = qslot(r, it.s1_lo);
+    tma_load_3d(&S.qn[0][sl][0], &T.st, x, r, 0, bar);
+    tma_load_3d(&S.qn[1][sl][0], &T.st, x, r, 1, bar);
+  }
+  const int sl = pslot(R, it.s1_lo);
+  tma_load_3d(&S.pn[0][sl][0], &T.st, x, R, 2, bar);
+  tma_load_3d(&S.pn[1][sl][0], &T.st, x, R, 3, bar);
+  tma_load_3d(&S.bb[sl][0], &T.bb, x, R, 0, bar);
+}
+
+__global__ void __launch_bounds__(kStripThreads, 1)
+    stage12_strip_kernel(const __grid_constant__ StripMaps T, const __grid_constant__ StageArgs A, const StripGeom G) {
+  extern __shared__ unsigned char smem_raw[];
+  StripSmem &S = *reinterpret_cast<StripSmem *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) &
+                                                ~static_cast<uintptr_t>(127));
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+  const int N = A.N, M = A.M;
+  const int nitems = G.nstrips * G.segs;
+  // stage-1 warps 0-7, stage-2 warps 8-15: row ty % 8 / 2 of the phase, half ty % 2
+  const int grp = ty >> 3, wrow = (ty & 7) >> 1, half = ty & 1;
+  if (tid == 0) {
+    mbar_init(&S.bar[0], 1);
+    mbar_init(&S.bar[1], 1);
+    fence_barrier_init();
+  }
+  // u1 rows outside the grid are never read for a stored output; start them finite
+  for (int i = tid; i < 2 * 2 * kPRing * kStripWin; i += kStripThreads) {
+    (&S.q1[0][0][0])[i] = 0.0;
+    (&S.p1[0][0][0])[i] = 0.0;
+  }
+  grid_dependency_wait();
+  launch_dependents();
+  if (tid == 0 && A.src != nullptr) {
+    const int k = A.rs->ks;
+    S.src_c0 = A.recs[k].col0;
+    S.src_r0 = A.recs[k].row0;
+    S.src_buf = k & 1;
+  }
+  __syncthreads();
+  const SrcNote note{S.src_c0, S.src_r0, S.src_buf};
+  int ph = 0;  // phases run by this block so far (barrier parity)
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const StripItem it = strip_item(G, N, M, item);
+    if (it.s2_lo >= it.s2_hi) continue;  // uniform across the block
+    // set-up data of the item: column factors of the computed columns, row factors of its rows
+    for (int i = tid; i < CF_TILE * kStripCols; i += kStripThreads) {
+      const int f = i / kStripCols, j = i - f * kStripCols, a = it.cs + j;
+      S.cf[f][j] = (a >= 0 && a < N) ? A.coltab[static_cast<size_t>(f) * N + a] : 0.0;
+    }
+    const int nrows1 = it.s1_hi - it.s1_lo;
+    for (int i = tid; i < RF_COUNT * nrows1; i += kStripThreads) {
+      const int f = i / nrows1, r = i - f * nrows1;
+      S.rf[f][r] = A.rowtab[static_cast<size_t>(f) * M + it.s1_lo + r];
+    }
+    const bool lo_edge = it.cs - 4 < 3, hi_edge = it.cs - 4 + kStripWin > N - 3;
+    const int nph = (it.s2_hi + 3 - it.s1_lo + kStripG - 1) / kStripG + 1;
+    if (tid == 0) {
+      fence_proxy_async();  // earlier generic writes of the rings before the async-proxy loads
+      strip_issue(S, T, it, it.s1_lo, true, &S.bar[ph & 1]);
+    }
+    bool aborted = false;
+    for (int p = 0; p < nph; p++, ph++) {
+      const int R = it.s1_lo + kStripG * p;
+      const bool ok = mbar_wait_bounded(&S.bar[ph & 1], (ph >> 1) & 1);
+      if (!__syncthreads_and(ok)) {
+        if (tid == 0) atomicCAS(A.err, 0, 5 /* BHR_TIMEOUT */);
+        mbar_wait_bounded(&S.bar[ph & 1], (ph >> 1) & 1);
+        aborted = true;
+        break;
+      }
+      // Closures of what arrived for this phase (u^n q rows: the prologue's
+      // or [R + 3, R + 7); p rows [R, R + 4)) and of the u1 rows stage 1
+      // finished in the previous phase ([R - 4, R)): radial ends on interior
+      // rows, pole rows on interior columns -- disjoint points, one pass.
+      const int q_lo = p == 0 ? R - 5 : R + 3, q_hi = R + 7;
+      const bool un_top = (p == 0 && it.s1_lo == 3);
+      const bool un_bot = q_lo <= M - 1 && M - 1 < q_hi;
+      const bool u1_top = (p > 0 && R - kStripG <= 4 && 4 < R && it.s1_lo == 3);
+      const bool u1_bot = (p > 0 && R - kStripG <= M - 4 && M - 4 < R && it.s1_hi == M - 3);
+      if (lo_edge || hi_edge || un_top || un_bot || u1_top || u1_bot) {
+        if (lo_edge || hi_edge) {
+          const int nq = 2 * (q_hi - q_lo);
+          for (int i = tid; i < nq + 2 * kStripG + (p > 0 ? 4 * kStripG : 0); i += kStripThreads) {
+            double *row = nullptr;
+            int r;
+            if (i < nq) {
+              r = q_lo + i / 2;
+              row = &S.qn[i & 1][qslot(r, it.s1_lo)][0];
+            } else if (i < nq + 2 * kStripG) {
+              const int j = i - nq;
+              r = R + j / 2;
+              row = &S.pn[j & 1][pslot(r, it.s1_lo)][0];
+            } else {
+              const int j = i - nq - 2 * kStripG, pl = j & 3;
+              r = R - kStripG + j / 4;
+              if (r < it.s1_lo || r >= it.s1_hi) continue;
+              row = pl < 2 ? &S.q1[pl][pslot(r, it.s1_lo)][0] : &S.p1[pl - 2][pslot(r, it.s1_lo)][0];
+            }
+            if (r >= 3 && r < M - 3) close_end_row(row, N, it.cs);
+          }
+        }
+        for (int pl = 0; pl < 2; pl++) {
+          if (un_top) ring_close_poles(S.qn[pl], true, M, N, it.cs, it.s1_lo, A.even_m, tid, true);
+          if (un_bot) ring_close_poles(S.qn[pl], false, M, N, it.cs, it.s1_lo, A.even_m, tid, true);
+          if (u1_top) ring_close_poles(S.q1[pl], true, M, N, it.cs, it.s1_lo, A.even_m, tid, false);
+          if (u1_bot) ring_close_poles(S.q1[pl], false, M, N, it.cs, it.s1_lo, A.even_m, tid, false);
+        }
+        __syncthreads();
+      }
+      // the next phase's rows (their ring slots are not read in this one)
+      if (tid == 0) {
+        fence_proxy_async();
+        if (p + 1 < nph) strip_issue(S, T, it, R + kStripG, false, &S.bar[(ph + 1) & 1]);
+      }
+      if (grp == 0) {
+        const int b = R + wrow;
+        if (b >= it.s1_lo && b < it.s1_hi) {
+          StripView<1> V{S, R, it.s1_lo, it.s1_lo, half * TC};
+          const int c0 = it.cs + half * TC;
+          tile_rows<1, 1, kOutRing, false>(V, A, c0, R, kStripG, tx, wrow, half * TC,
+                                           c0 >= 4 && c0 + TC <= N - 4, 3, N - 3, note);
+        }
+      } else {
+        const int R2 = R - kStripLag;
+        const int b = R2 + wrow;
+        if (b >= it.s2_lo && b < it.s2_hi) {
+          StripView<2> V{S, R2, it.s1_lo, it.s1_lo, half * TC};
+          const int c0 = it.cs + half * TC;
+          tile_rows<2, 1, kOutGlobal, true>(V, A, c0, R2, kStripG, tx, wrow, half * TC,
+                                            c0 >= 4 && c0 + TC <= N - 4, it.st_lo, it.st_hi, note);
+        }
+      }
+      __syncthreads();
+    }
+    if (aborted) return;
+  }
 }
 
 // ---- closure of stored planes (HighOrder/kern.cu:622-753) ------------------
@@ -1097,6 +1444,7 @@ cudaError_t prepare_kernels() {
   const int s8 = static_cast<int>(sizeof(StageSmem<8>) + 128), s16 = static_cast<int>(sizeof(StageSmem<16>) + 128);
   const int sp = static_cast<int>(persist_smem_bytes()), sr = static_cast<int>(ring_smem_bytes());
   constexpr auto kSmem = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  if (cudaError_t r = cudaFuncSetAttribute(stage12_strip_kernel, kSmem, static_cast<int>(strip_smem_bytes()))) return r;
   for (int stage = 1; stage <= 5; stage++) {
     const cudaError_t e = by_stage(stage, [&](auto sc) {
       constexpr int S = decltype(sc)::value;
@@ -1146,6 +1494,42 @@ cudaError_t launch_stage_batch(int stage, int tiling, const BatchSolve *solves, 
                           sizeof(StageSmem<16>) + 128, st, solves, tiles);
     }
   });
+}
+
+size_t strip_smem_bytes() { return sizeof(StripSmem) + 128; }
+
+cudaError_t encode_strip_maps(double *state, double *ctab, int N, int M, StripMaps *maps) {
+  auto encode = tensor_map_encoder();
+  if (!encode) return cudaErrorNotSupported;
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const cuuint32_t box[3] = {kStripWin, kStripG, 1};
+  const cuuint64_t dims[3] = {static_cast<cuuint64_t>(N), static_cast<cuuint64_t>(M), 4};
+  const cuuint64_t strides[2] = {static_cast<cuuint64_t>(N) * 8, static_cast<cuuint64_t>(N) * M * 8};
+  const cuuint64_t bdims[3] = {static_cast<cuuint64_t>(N), static_cast<cuuint64_t>(M), 1};
+  CUresult r1 = encode(&maps->st, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, state, dims, strides, box, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r2 = encode(&maps->bb, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, ctab, bdims, strides, box, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return (r1 == CUDA_SUCCESS && r2 == CUDA_SUCCESS) ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+StripGeom strip_geometry(int N, int M) {
+  StripGeom G{};
+  G.nstrips = (N - 3 + kStripOut - 1) / kStripOut;
+  const int rows = M - 6;
+  const int max_seg = kStripMaxRows - 6;
+  G.segs = std::max(std::max(1, sm_count() / G.nstrips), (rows + max_seg - 1) / max_seg);
+  G.seg_rows = (rows + G.segs - 1) / G.segs;
+  return G;
+}
+
+cudaError_t launch_stage12_strip(const StripMaps &maps, const StageArgs &a, cudaStream_t st, bool pdl) {
+  const StripGeom G = strip_geometry(a.N, a.M);
+  const int nitems = G.nstrips * G.segs;
+  return launch_ex(pdl, stage12_strip_kernel, dim3(std::min(nitems, sm_count())), dim3(32, kStripThreads / 32),
+                   strip_smem_bytes(), st, maps, a, G);
 }
 
 cudaError_t launch_source_batch(const SourceArgs *args, int nsolves, int max_ptsy, int max_ptsx, cudaStream_t st) {

@@ -388,6 +388,11 @@ int bhr::solver_create(const bhr_params *pin, int tile_rows, bhr_solver **out) {
         tile_rows = 8;
         s->ring = 1;
       }
+      if (!std::strcmp(v, "strip12")) {  // FP64 SSP-RK3 only; otherwise block8n
+        tile_rows = 8;
+        s->narrow = 1;
+        s->strip12 = (p.precision == BHR_FP64 && p.integrator == BHR_SSPRK3) ? 1 : 0;
+      }
     }
   }
   if (p.integrator == BHR_RK4) {
@@ -469,7 +474,8 @@ int bhr_solver_info(const bhr_solver *s, bhr_info *info) {
   info->device_bytes = s->bytes;
   info->tile_rows = s->tile_rows;
   info->persistent = s->persist || s->ring;
-  info->tiling = s->ring ? BHR_TILING_RING
+  info->tiling = s->strip12 ? BHR_TILING_STRIP12
+                 : s->ring ? BHR_TILING_RING
                  : s->narrow ? BHR_TILING_BLOCK8N
                  : s->persist ? BHR_TILING_PERSISTENT
                  : s->tile_rows == 8 ? BHR_TILING_BLOCK8 : BHR_TILING_BLOCK16;
@@ -796,6 +802,10 @@ static int encode_maps(bhr_solver *s, int rows) {
       return BHR_CUDA_ERROR;
     }
   }
+  if (s->strip12 && encode_strip_maps(s->u0, s->ctab, p.N, p.M, &s->smaps) != cudaSuccess) {
+    set_error("cuTensorMapEncodeTiled failed (strip maps)");
+    return BHR_CUDA_ERROR;
+  }
   s->tile_rows = rows;
   return BHR_OK;
 }
@@ -808,33 +818,48 @@ static int encode_maps(bhr_solver *s, int rows) {
 // fastest is kept for the process.
 static int autotune_rows(bhr_solver *s) {
   static std::mutex mu;
-  static std::vector<std::array<int, 7>> cache;  // device, N, M, rows, persist, narrow, ring
+  // device, N, M, FP64 SSP-RK3, rows, persist, narrow, ring, strip12
+  static std::vector<std::array<int, 9>> cache;
   const bhr_params &p = s->p;
+  const int fused_ok = (!s->mixed && !s->rk4) ? 1 : 0;
   {
     std::lock_guard<std::mutex> lock(mu);
     for (auto &c : cache)
-      if (c[0] == p.device && c[1] == p.N && c[2] == p.M) {
-        s->persist = c[4];
-        s->narrow = c[5];
-        s->ring = c[6];
-        return encode_maps(s, c[3]);
+      if (c[0] == p.device && c[1] == p.N && c[2] == p.M && c[3] == fused_ok) {
+        s->persist = c[5];
+        s->narrow = c[6];
+        s->ring = c[7];
+        s->strip12 = c[8];
+        return encode_maps(s, c[4]);
       }
   }
-  static const int cands[5][4] = {{8, 0, 0, 0}, {16, 0, 0, 0}, {16, 1, 0, 0}, {8, 0, 1, 0}, {8, 0, 0, 1}};  // rows, persist, narrow, ring
+  // rows, persist, narrow, ring, strip12 (stages 1 and 2 in one launch: only
+  // FP64 SSP-RK3 solves; its stage 3 is block8n)
+  static const int cands[6][5] = {{8, 0, 0, 0, 0}, {16, 0, 0, 0, 0}, {16, 1, 0, 0, 0},
+                                  {8, 0, 1, 0, 0}, {8, 0, 0, 1, 0}, {8, 0, 1, 0, 1}};
+  const int ncand = fused_ok ? 6 : 5;
   double best_ms = 1e30;
   int best = 1;
   cudaEvent_t e0, e1;
   BHR_CUDA_TRY(cudaEventCreate(&e0));
   BHR_CUDA_TRY(cudaEventCreate(&e1));
-  for (int c = 0; c < 5; c++) {
+  // Stages 1 and 2 (they write only the solve's scratch stages u1, u2) of
+  // each candidate, or the fused launch that replaces them.
+  for (int c = 0; c < ncand; c++) {
     s->persist = cands[c][1];
     s->narrow = cands[c][2];
     s->ring = cands[c][3];
+    s->strip12 = cands[c][4];
     if (int st = encode_maps(s, cands[c][0])) return st;
     StageArgs A = solver_stage_args(s);
     A.src = nullptr;
     for (int rep = 0; rep < 6; rep++) {
       if (rep == 2) BHR_CUDA_TRY(cudaEventRecord(e0, s->stream));
+      if (s->strip12) {
+        A.vin = s->u0; A.un = s->u0; A.out = s->u2;
+        BHR_CUDA_TRY(launch_stage12_strip(s->smaps, A, s->stream));
+        continue;
+      }
       A.vin = s->u0; A.un = s->u0; A.out = s->u1;
       BHR_CUDA_TRY(launch_stage(1, s->maps[0], A, s->stream));
       A.vin = s->u1; A.un = s->u0; A.out = s->u2;
@@ -853,11 +878,13 @@ static int autotune_rows(bhr_solver *s) {
   cudaEventDestroy(e1);
   {
     std::lock_guard<std::mutex> lock(mu);
-    cache.push_back({p.device, p.N, p.M, cands[best][0], cands[best][1], cands[best][2], cands[best][3]});
+    cache.push_back({p.device, p.N, p.M, fused_ok, cands[best][0], cands[best][1], cands[best][2], cands[best][3],
+                     cands[best][4]});
   }
   s->persist = cands[best][1];
   s->narrow = cands[best][2];
   s->ring = cands[best][3];
+  s->strip12 = cands[best][4];
   return encode_maps(s, cands[best][0]);
 }
 
@@ -1020,6 +1047,17 @@ static int launch_step(bhr_solver *s, cudaEvent_t *ev = nullptr) {
     BHR_CUDA_TRY(join());
     A.vin = s->u1; A.un = s->u3; A.out = s->u0; A.dt = dt / 6.0;
     BHR_CUDA_TRY(launch_stage(5, s->maps[4], A, s->stream));
+  } else if (s->strip12) {
+    // Stages 1 and 2 in one launch (u1 stays on chip), beside the previous
+    // step's extraction, which reads only u^n.
+    BHR_CUDA_TRY(fork_extract());
+    A.vin = s->u0; A.un = s->u0; A.out = s->u2;
+    BHR_CUDA_TRY(launch_stage12_strip(s->smaps, A, s->stream));
+    BHR_CUDA_TRY(mark(2));
+    BHR_CUDA_TRY(mark(3));
+    BHR_CUDA_TRY(join());
+    A.vin = s->u2; A.un = s->u0; A.out = s->u0;
+    BHR_CUDA_TRY(launch_stage(3, s->maps[2], A, s->stream));
   } else {
     BHR_CUDA_TRY(launch_stage(1, s->maps[0], A, s->stream));
     BHR_CUDA_TRY(mark(2));

@@ -45,6 +45,8 @@ struct bhr_solver {
   int persist = 0;     // 1: persistent stage kernels (16-row tiles, one block per SM)
   int narrow = 0;      // 1: 8-row tiles on 128-thread blocks (four per SM)
   int ring = 0;        // 1: 8-row tiles through 2-buffer rings, two 256-thread blocks per SM
+  int strip12 = 0;     // 1: stages 1 and 2 in one launch over column strips (FP64 SSP-RK3; stage 3 block8n)
+  bhr::StripMaps smaps;
   int steps_done = 0;
   // The extraction of the last step launched has not been launched yet: it
   // runs beside the next step's first stages, or before a host read.

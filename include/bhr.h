@@ -52,15 +52,19 @@ typedef enum bhr_precision { BHR_FP64 = 0, BHR_MIXED = 1 } bhr_precision;
 typedef enum bhr_init_kind { BHR_INIT_ZERO = 0, BHR_INIT_GAUSSIAN = 1 } bhr_init_kind;
 /* Stage kernel tilings (chosen per device and grid by timing, or fixed by
  * the environment variable BHR_STAGE_TILING=block8|block16|persistent|
- * block8n|ring): one 64 x 8 or 64 x 16 tile per 256-thread block; 64 x 16
- * tiles walked by one 512-thread block per SM; 64 x 8 tiles per 128-thread
- * block, four per SM; 64 x 8 tiles walked by two 256-thread blocks per SM. */
+ * block8n|ring|strip12): one 64 x 8 or 64 x 16 tile per 256-thread block;
+ * 64 x 16 tiles walked by one 512-thread block per SM; 64 x 8 tiles per
+ * 128-thread block, four per SM; 64 x 8 tiles walked by two 256-thread
+ * blocks per SM; stages 1 and 2 fused in one launch over 128-column strips
+ * (the intermediate stage stays in shared memory; FP64 SSP-RK3 solves, stage
+ * 3 as block8n). */
 typedef enum bhr_tiling {
   BHR_TILING_BLOCK8 = 0,
   BHR_TILING_BLOCK16 = 1,
   BHR_TILING_PERSISTENT = 2,
   BHR_TILING_BLOCK8N = 3,
-  BHR_TILING_RING = 4
+  BHR_TILING_RING = 4,
+  BHR_TILING_STRIP12 = 5
 } bhr_tiling;
 
 /* Run parameters.  Replaces HighOrder/parm.h:1-13 (N, M, Xmax, Xmin, Fr, T,

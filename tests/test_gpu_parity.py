@@ -164,7 +164,7 @@ def test_headline_workload_grid_matches_oracle():
     assert rel_field_err(s.get_state(), o.get_state()) <= FIELD_TOL
 
 
-@pytest.mark.parametrize("tiling", ["block8", "block16", "persistent", "block8n", "ring"])
+@pytest.mark.parametrize("tiling", ["block8", "block16", "persistent", "block8n", "ring", "strip12"])
 def test_every_stage_tiling_matches_oracle(tiling, monkeypatch):
     """Each stage tiling (8- and 16-row tiles one per block, persistent
     blocks walking 16-row tiles, or 8-row tiles two blocks per SM, through
@@ -175,7 +175,7 @@ def test_every_stage_tiling_matches_oracle(tiling, monkeypatch):
     info = s.info()
     assert info["tiling"] == tiling
     assert info["persistent"] == (tiling in ("persistent", "ring"))
-    assert info["tile_rows"] == (8 if tiling in ("block8", "block8n", "ring") else 16)
+    assert info["tile_rows"] == (8 if tiling in ("block8", "block8n", "ring", "strip12") else 16)
     n = 120
     s.step(n)
     t, h, dedt, steps, _, _ = o.run(traj=rows, coef_fn=coef, nsteps=n)
@@ -185,7 +185,7 @@ def test_every_stage_tiling_matches_oracle(tiling, monkeypatch):
     assert np.linalg.norm(hs - h) <= WAVE_TOL * np.linalg.norm(h)
 
 
-@pytest.mark.parametrize("tiling", ["block16", "persistent", "ring"])
+@pytest.mark.parametrize("tiling", ["block16", "persistent", "ring", "strip12"])
 def test_trajectory_set_after_stepping(tiling, monkeypatch):
     """A step taken before the trajectory is set captures the step graph
     without a source; setting the trajectory must rebuild what was captured.
@@ -229,7 +229,7 @@ def test_long_trajectory_records_built_while_stepping():
     assert rel_field_err(gs, o.get_state()) <= 1e-9  # 12000 steps of rounding
 
 
-@pytest.mark.parametrize("tiling", ["block8", "block16", "persistent", "block8n", "ring"])
+@pytest.mark.parametrize("tiling", ["block8", "block16", "persistent", "block8n", "ring", "strip12"])
 @pytest.mark.parametrize("N,M", [(64, 16), (128, 16), (192, 32)])
 def test_tiny_grids_every_tiling(tiling, N, M, monkeypatch):
     """Grids of one to a dozen tiles, every tile at an edge, persistent

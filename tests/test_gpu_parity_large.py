@@ -114,3 +114,28 @@ def test_engine_batch_with_a_16384x256_member_matches_oracle():
     assert nt >= n and len(tg) == nt and np.array_equal(tg, t)
     assert np.max(np.abs(h)) > 1e-6
     assert np.linalg.norm(hg - h) <= WAVE_TOL * np.linalg.norm(h)
+
+
+@pytest.mark.parametrize("N,M", [(16384, 256), (8192, 128), (1024, 64)])
+def test_fused_strip_stages_are_bit_identical_to_separate_stages(N, M, monkeypatch):
+    """The strip12 tiling computes stages 1 and 2 in one launch with u1 kept
+    on chip; every point goes through the same arithmetic as the separate
+    stage kernels, so after sourced steps the fields and waveform rows are
+    bit-identical to the block8n tiling's, and match the oracle."""
+    n = 24
+    prm, rows, o = setup(N, M, center=10.0, ext_col=col_of(10.0, N), Fr=1, nsteps=n)
+    out = {}
+    for tiling in ("block8n", "strip12"):
+        monkeypatch.setenv("BHR_STAGE_TILING", tiling)
+        with bhr.Solver(prm) as s:
+            assert s.info()["tiling"] == tiling
+            s.set_trajectory(rows)
+            s.step(n)
+            out[tiling] = (s.get_state(), s.waveform())
+    (sa, (ta, ha, _)), (sb, (tb, hb, _)) = out["block8n"], out["strip12"]
+    for a, b in zip(sa, sb):
+        assert np.array_equal(a, b)
+    assert np.array_equal(ta, tb) and np.array_equal(ha, hb)
+    t, h, dedt, steps, _, _ = o.run(traj=rows, coef_fn=product_coef_fn(), nsteps=n)
+    assert rel_field_err(sb, o.get_state()) <= FIELD_TOL
+    assert np.linalg.norm(hb - h) <= WAVE_TOL * np.linalg.norm(h)
