@@ -918,7 +918,9 @@ __global__ void __launch_bounds__(kStripThreads, 1)
     fence_barrier_init();
   }
   // u1 rows outside the grid are never read for a stored output; start them finite
-  for (int i = tid; i < 2 * 2 * kPRing * kStripWin; i += kStripThreads) {
+  static_assert(sizeof(S.q1) == sizeof(S.p1), "u1 rings of equal size");
+  constexpr int kU1Ring = static_cast<int>(sizeof(S.q1) / sizeof(double));  // 2 planes x 16 rows x 136
+  for (int i = tid; i < kU1Ring; i += kStripThreads) {
     (&S.q1[0][0][0])[i] = 0.0;
     (&S.p1[0][0][0])[i] = 0.0;
   }
