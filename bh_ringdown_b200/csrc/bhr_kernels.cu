@@ -835,12 +835,14 @@ struct StripView {
   }
 };
 
-// Extrapolation closure rows of one plane row set, in the ring: the pole
-// rows (q planes) on window columns whose grid column is in [3, N-3), and
-// the radial ends (all planes) of the given interior rows.
+// Extrapolation closure of pole rows of one q plane in a ring, on window
+// columns whose grid column is in [3, N-3): the top rows 2, 1, 0 from rows
+// 3, 4, or those of the bottom rows M-3, M-2, M-1 (in that order, each
+// from the two rows above it) that lie in [lo, hi) -- the rows a TMA chunk
+// just brought, so no later load overwrites them.
 __device__ __forceinline__ void ring_close_poles(double (*q)[kStripWin], const bool top, const int M, const int N,
                                                  const int cs, const int base, const int even_m, const int tid,
-                                                 bool qring) {
+                                                 const bool qring, const int lo, const int hi) {
   auto row = [&](int r) { return q[qring ? qslot(r, base) : pslot(r, base)]; };
   for (int w = tid; w < kStripWin; w += kStripThreads) {
     const int a = cs - 4 + w;
@@ -854,12 +856,9 @@ __device__ __forceinline__ void ring_close_poles(double (*q)[kStripWin], const b
         row(2)[w] = 0.0; row(1)[w] = 0.0; row(0)[w] = 0.0;
       }
     } else {
-      if (even_m) {
-        row(M - 3)[w] = (4.0 * row(M - 4)[w] - row(M - 5)[w]) * kThird;
-        row(M - 2)[w] = (4.0 * row(M - 3)[w] - row(M - 4)[w]) * kThird;
-        row(M - 1)[w] = (4.0 * row(M - 2)[w] - row(M - 3)[w]) * kThird;
-      } else {
-        row(M - 3)[w] = 0.0; row(M - 2)[w] = 0.0; row(M - 1)[w] = 0.0;
+      for (int r = M - 3; r < M; r++) {
+        if (r < lo || r >= hi) continue;
+        row(r)[w] = even_m ? (4.0 * row(r - 1)[w] - row(r - 2)[w]) * kThird : 0.0;
       }
     }
   }
@@ -969,8 +968,8 @@ __global__ void __launch_bounds__(kStripThreads, 1)
       // finished in the previous phase ([R - 4, R)): radial ends on interior
       // rows, pole rows on interior columns -- disjoint points, one pass.
       const int q_lo = p == 0 ? R - 5 : R + 3, q_hi = R + 7;
-      const bool un_top = (p == 0 && it.s1_lo == 3);
-      const bool un_bot = q_lo <= M - 1 && M - 1 < q_hi;
+      const bool un_top = (p == 0 && it.s1_lo < 6);  // stage 1's window reaches rows 0..2
+      const bool un_bot = q_lo < M && M - 3 < q_hi;  // some of rows M-3..M-1 arrived
       const bool u1_top = (p > 0 && R - kStripG <= 4 && 4 < R && it.s1_lo == 3);
       const bool u1_bot = (p > 0 && R - kStripG <= M - 4 && M - 4 < R && it.s1_hi == M - 3);
       if (lo_edge || hi_edge || un_top || un_bot || u1_top || u1_bot) {
@@ -996,10 +995,10 @@ __global__ void __launch_bounds__(kStripThreads, 1)
           }
         }
         for (int pl = 0; pl < 2; pl++) {
-          if (un_top) ring_close_poles(S.qn[pl], true, M, N, it.cs, it.s1_lo, A.even_m, tid, true);
-          if (un_bot) ring_close_poles(S.qn[pl], false, M, N, it.cs, it.s1_lo, A.even_m, tid, true);
-          if (u1_top) ring_close_poles(S.q1[pl], true, M, N, it.cs, it.s1_lo, A.even_m, tid, false);
-          if (u1_bot) ring_close_poles(S.q1[pl], false, M, N, it.cs, it.s1_lo, A.even_m, tid, false);
+          if (un_top) ring_close_poles(S.qn[pl], true, M, N, it.cs, it.s1_lo, A.even_m, tid, true, 0, 0);
+          if (un_bot) ring_close_poles(S.qn[pl], false, M, N, it.cs, it.s1_lo, A.even_m, tid, true, q_lo, q_hi);
+          if (u1_top) ring_close_poles(S.q1[pl], true, M, N, it.cs, it.s1_lo, A.even_m, tid, false, 0, 0);
+          if (u1_bot) ring_close_poles(S.q1[pl], false, M, N, it.cs, it.s1_lo, A.even_m, tid, false, M - 3, M);
         }
         __syncthreads();
       }
