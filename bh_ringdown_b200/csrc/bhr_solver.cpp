@@ -149,6 +149,7 @@ double tortoise(double r, double a, double rpl, double rmn) {
 static int autotune_rows(bhr_solver *s);
 static int flush_extract(bhr_solver *s);
 
+
 extern "C" {
 
 int bhr_abi_version(void) { return BHR_ABI_VERSION; }

@@ -117,11 +117,14 @@ def test_engine_batch_with_a_16384x256_member_matches_oracle():
 
 
 @pytest.mark.parametrize("N,M", [(16384, 256), (8192, 128), (1024, 64)])
-def test_fused_strip_stages_are_bit_identical_to_separate_stages(N, M, monkeypatch):
+def test_fused_strip_stages_agree_with_separate_stages(N, M, monkeypatch):
     """The strip12 tiling computes stages 1 and 2 in one launch with u1 kept
-    on chip; every point goes through the same arithmetic as the separate
-    stage kernels, so after sourced steps the fields and waveform rows are
-    bit-identical to the block8n tiling's, and match the oracle."""
+    on chip; every point goes through the same row work as the separate
+    stage kernels (up to the compiler's fused multiply-add choices, which
+    differ between the row work's instantiations for interior and edge
+    segments, and the strip cuts the grid into segments differently), so
+    after sourced steps the fields and waveform rows agree with the block8n
+    tiling's to rounding, and match the oracle."""
     n = 24
     prm, rows, o = setup(N, M, center=10.0, ext_col=col_of(10.0, N), Fr=1, nsteps=n)
     out = {}
@@ -133,9 +136,8 @@ def test_fused_strip_stages_are_bit_identical_to_separate_stages(N, M, monkeypat
             s.step(n)
             out[tiling] = (s.get_state(), s.waveform())
     (sa, (ta, ha, _)), (sb, (tb, hb, _)) = out["block8n"], out["strip12"]
-    for a, b in zip(sa, sb):
-        assert np.array_equal(a, b)
-    assert np.array_equal(ta, tb) and np.array_equal(ha, hb)
+    assert rel_field_err(sb, sa) <= 1e-13
+    assert np.array_equal(ta, tb) and np.linalg.norm(hb - ha) <= 1e-13 * np.linalg.norm(ha)
     t, h, dedt, steps, _, _ = o.run(traj=rows, coef_fn=product_coef_fn(), nsteps=n)
     assert rel_field_err(sb, o.get_state()) <= FIELD_TOL
     assert np.linalg.norm(hb - h) <= WAVE_TOL * np.linalg.norm(h)
