@@ -779,8 +779,8 @@ def main():
                     help="fp64, or mixed: FP64 state and stage 1, FP32 corrections in stages 2 and 3")
     ap.add_argument("--integrator", choices=["ssprk3", "rk4"], default="ssprk3",
                     help="single-solve workloads: SSP-RK3 (the reference's) or classical RK4 (FP64 only)")
-    ap.add_argument("--requests", type=int, default=200, help="serve: requests in the stream")
-    ap.add_argument("--time-scale", type=float, default=0.02, help="serve: factor on every request's final time")
+    ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the stream")
+    ap.add_argument("--time-scale", type=float, default=0.01, help="serve: factor on every request's final time")
     ap.add_argument("--load", type=float, default=0.8, help="serve: arrival rate / measured capacity")
     ap.add_argument("--chunk", type=int, default=64, help="serve: steps per engine call")
     ap.add_argument("--plain-requests", type=int, default=60, help="serve: requests timed on the plain path")
