@@ -84,7 +84,7 @@ size_t solve_bytes(const bhr_params &p, int traj_rows) {
 struct bhr_engine {
   int device = 0;
   size_t budget = 0;
-  int tiling = kTilingRing;  // stage tiling of the FP64 kernels (bhr_tiling values)
+  int tiling = kTilingBlock8n;  // stage tiling of the FP64 kernels (bhr_tiling values)
   int rows = 8;              // its tile height: every solve's tensor maps use it
   cudaStream_t stream = nullptr;
   // Requests and the worker (lock wmu): the queue, solves being prepared,
@@ -456,7 +456,8 @@ int bhr_engine_create(int device, size_t hbm_budget_bytes, bhr_engine **out) {
     return set_fail(BHR_CUDA_ERROR, "engine set-up failed");
   }
   // BHR_ENGINE_TILING=block8|block16|persistent|block8n|ring selects the
-  // FP64 stage kernels over the work-list (default ring).
+  // FP64 stage kernels over the work-list (default block8n: 8-row tiles on
+  // 128-thread blocks, each prefetching the work item two SM-counts ahead).
   if (const char *v = std::getenv("BHR_ENGINE_TILING")) {
     static const char *names[] = {"block8", "block16", "persistent", "block8n", "ring"};
     for (int t = 0; t < 5; t++)

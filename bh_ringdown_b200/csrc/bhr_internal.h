@@ -81,6 +81,9 @@ struct StageArgs {
   int persist;          // 1: 16-row tiles walked by one persistent block per SM
   int narrow;           // 1: 8-row tiles on 128-thread blocks (four per SM)
   int ring;             // 1: 8-row tiles walked by two 256-thread blocks per SM, two buffers each
+  int ahead;            // one-tile-per-block kernels: each block prefetches into L2 the stage
+                        // input of the block this many places later in launch order (0: none;
+                        // launch_stage sets it)
   float *dout;          // mixed precision, stage 1: delta1 = dt L(u^n) in FP32, or nullptr
   double *zout;         // RK4 stage 2: z = (y1 + 2 y2 - u^n)/3, or nullptr
   double dt;            // the stage's step in the combination (RK4: dt/2, dt, dt/6)
@@ -232,5 +235,9 @@ cudaError_t launch_math_selftest(const double *x, int n, double *out, cudaStream
 cudaError_t launch_init_product(double *q, const double *fa, const double *gb, int N, int M, cudaStream_t st);
 size_t stage_smem_bytes();
 cudaError_t prepare_kernels();
+// Blocks ahead (in launch order) whose input a one-tile-per-block stage
+// kernel prefetches into L2: twice the SM count, or BHR_PREFETCH_AHEAD
+// (0: no prefetch).
+int stage_prefetch_ahead();
 
 }  // namespace bhr

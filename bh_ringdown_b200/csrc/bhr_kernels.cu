@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <cstddef>
+#include <cstdlib>
 #include <type_traits>
 #include <utility>
 
@@ -474,9 +475,22 @@ __device__ __forceinline__ void tile_compute(StageSmem<ROWS> &S, const StageArgs
       TileView<ROWS>{S}, A, c0, b0, ROWS, tx, ty, 0, !lo_cols && !hi_cols, 3, A.N - 3, note);
 }
 
-// One tile per block (grid N/64 x M/ROWS, two blocks per SM).
-template <int STAGE, int ROWS, int THREADS = STAGE_THREADS>
-__device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &A, const int c0, const int b0) {
+// Thread 0: prefetch into L2 the stage input of a later tile (its maps
+// and corner), so that the block which takes it, some microseconds on,
+// finds its loads in L2 instead of waiting for HBM at the start of its life.
+template <int STAGE>
+__device__ __forceinline__ void tile_prefetch(const StageMaps &T, const int c0, const int b0) {
+  tma_prefetch_3d(&T.q, c0 - 4, b0 - 3, 0);
+  tma_prefetch_3d(&T.p, c0 - 4, b0, 2);
+  tma_prefetch_3d(&T.coef_bb, c0 - 4, b0, 0);
+  if (STAGE != 1) tma_prefetch_3d(&T.u, c0, b0, 0);
+}
+
+// One tile per block (grid N/64 x M/ROWS, two blocks per SM).  Thread 0
+// prefetches the tile `ahead` names, if any (after the grid dependency).
+template <int STAGE, int ROWS, int THREADS, class Ahead>
+__device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &A, const int c0, const int b0,
+                                           const Ahead ahead) {
   extern __shared__ unsigned char smem_raw[];
   StageSmem<ROWS> &S = *reinterpret_cast<StageSmem<ROWS> *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
@@ -493,6 +507,9 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
   if (tid == 0) {
     tile_issue_state<STAGE>(S, T, c0, b0);
     tile_note_source(S, A);
+    const StageMaps *pm;
+    int pc0, pb0;
+    if (ahead(pm, pc0, pb0)) tile_prefetch<STAGE>(*pm, pc0, pb0);
   }
   const bool ok = mbar_wait_bounded(&S.bar, 0);
   if (!__syncthreads_and(ok)) {
@@ -505,10 +522,42 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
   tile_compute<STAGE, ROWS, THREADS, false>(S, A, c0, b0, tx, ty);
 }
 
+// Single solve: the block's tile is blockIdx.y * gridDim.x + blockIdx.x in
+// launch order; the tile `n` places later (n = A.ahead, 0: none).
+template <int ROWS>
+struct GridAhead {
+  const StageMaps *T;
+  int n;
+  __device__ __forceinline__ bool operator()(const StageMaps *&pm, int &c0, int &b0) const {
+    const int L = blockIdx.y * gridDim.x + blockIdx.x + n;
+    if (n <= 0 || L >= static_cast<int>(gridDim.x * gridDim.y)) return false;
+    pm = T;
+    c0 = (L % gridDim.x) * TC;
+    b0 = (L / gridDim.x) * ROWS;
+    return true;
+  }
+};
+// Batch: the work item `n` places later in the list.
+template <int STAGE>
+struct ListAhead {
+  const BatchSolve *solves;
+  const BatchTile *tiles;
+  int n;
+  __device__ __forceinline__ bool operator()(const StageMaps *&pm, int &c0, int &b0) const {
+    const int L = blockIdx.x + n;
+    if (n <= 0 || L >= static_cast<int>(gridDim.x)) return false;
+    const BatchTile w = tiles[L];
+    pm = &solves[w.solve].maps[STAGE - 1];
+    c0 = w.c0;
+    b0 = w.b0;
+    return true;
+  }
+};
+
 template <int STAGE, int ROWS>
 __global__ void __launch_bounds__(STAGE_THREADS, 2)
     stage_kernel(const __grid_constant__ StageMaps T, const StageArgs A) {
-  stage_tile<STAGE, ROWS>(T, A, blockIdx.x * TC, blockIdx.y * ROWS);
+  stage_tile<STAGE, ROWS, STAGE_THREADS>(T, A, blockIdx.x * TC, blockIdx.y * ROWS, GridAhead<ROWS>{&T, A.ahead});
 }
 
 // 8-row tiles on 128-thread blocks: four blocks (16 warps) per SM, so four
@@ -517,16 +566,17 @@ constexpr int kNarrowThreads = 128;
 template <int STAGE>
 __global__ void __launch_bounds__(kNarrowThreads, 4)
     stage_narrow_kernel(const __grid_constant__ StageMaps T, const StageArgs A) {
-  stage_tile<STAGE, 8, kNarrowThreads>(T, A, blockIdx.x * TC, blockIdx.y * 8);
+  stage_tile<STAGE, 8, kNarrowThreads>(T, A, blockIdx.x * TC, blockIdx.y * 8, GridAhead<8>{&T, A.ahead});
 }
 
 // Several solves advanced together: block -> (solve, tile) from the work-list.
 template <int STAGE, int ROWS>
 __global__ void __launch_bounds__(STAGE_THREADS, 2)
-    stage_batch_kernel(const BatchSolve *solves, const BatchTile *tiles) {
+    stage_batch_kernel(const BatchSolve *solves, const BatchTile *tiles, int ahead) {
   const BatchTile t = tiles[blockIdx.x];
   const BatchSolve &B = solves[t.solve];
-  stage_tile<STAGE, ROWS>(B.maps[STAGE - 1], B.args[STAGE - 1], t.c0, t.b0);
+  stage_tile<STAGE, ROWS, STAGE_THREADS>(B.maps[STAGE - 1], B.args[STAGE - 1], t.c0, t.b0,
+                                        ListAhead<STAGE>{solves, tiles, ahead});
 }
 
 // ---- persistent stage kernels -------------------------------------------
@@ -724,10 +774,11 @@ __global__ void __launch_bounds__(kRingThreads, kRingBlocksPerSM)
 
 template <int STAGE>
 __global__ void __launch_bounds__(kNarrowThreads, 4)
-    stage_narrow_batch_kernel(const BatchSolve *solves, const BatchTile *tiles) {
+    stage_narrow_batch_kernel(const BatchSolve *solves, const BatchTile *tiles, int ahead) {
   const BatchTile t = tiles[blockIdx.x];
   const BatchSolve &B = solves[t.solve];
-  stage_tile<STAGE, 8, kNarrowThreads>(B.maps[STAGE - 1], B.args[STAGE - 1], t.c0, t.b0);
+  stage_tile<STAGE, 8, kNarrowThreads>(B.maps[STAGE - 1], B.args[STAGE - 1], t.c0, t.b0,
+                                       ListAhead<STAGE>{solves, tiles, ahead});
 }
 
 // ---- stages 1 and 2 fused over column strips (the strip12 tiling) --------
@@ -750,9 +801,10 @@ __global__ void __launch_bounds__(kNarrowThreads, 4)
 // closures of what arrived (u^n) and of what stage 1 finished (u1) are
 // rebuilt in the rings, with the extrapolation order of the other kernels
 // (HighOrder/kern.cu:320-449): pole rows of the q planes on columns
-// [3, N-3), radial ends of all planes on interior rows.  Results are
-// bit-identical to the separate stage kernels: every point is computed by
-// the same row work (tile_rows) from the same values.
+// [3, N-3), radial ends of all planes on interior rows.  Every point is
+// computed by the same row work (tile_rows) from the same values as in the
+// separate stage kernels, so results agree with them to rounding (the
+// compiler's fused multiply-add choices may differ between instantiations).
 constexpr int kStripThreads = 512;
 constexpr int kStripCols = 2 * TC;            // computed columns per strip
 constexpr int kStripOut = kStripCols - 8;     // stage-2 output columns per strip
@@ -1413,7 +1465,23 @@ static cudaError_t by_stage(const int stage, F &&f) {
   }
 }
 
-cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a, cudaStream_t st, bool pdl) {
+// Blocks ahead (in launch order) whose stage input a one-tile-per-block
+// stage kernel prefetches into L2: twice the SM count (half a wave of
+// block8n's four blocks per SM, one wave of block8's two), or
+// BHR_PREFETCH_AHEAD (0 turns the prefetch off).  Measured at 16384 x 256,
+// block8n: 220 us per step without, 203 us with 259-333 blocks ahead, 210
+// at 592, 246 at 1184 (prefetched lines evicted before use).
+int stage_prefetch_ahead() {
+  static const int env = [] {
+    const char *v = std::getenv("BHR_PREFETCH_AHEAD");
+    return v ? std::max(0, std::atoi(v)) : -1;
+  }();
+  return env >= 0 ? env : 2 * sm_count();
+}
+
+cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a_in, cudaStream_t st, bool pdl) {
+  StageArgs a = a_in;
+  a.ahead = (a.persist || a.ring) ? 0 : stage_prefetch_ahead();
   return by_stage(stage, [&](auto sc) {
     constexpr int S = decltype(sc)::value;
     if (a.narrow) {
@@ -1486,13 +1554,13 @@ cudaError_t launch_stage_batch(int stage, int tiling, const BatchSolve *solves, 
                           dim3(32, kRingThreads / 32), ring_smem_bytes(), st, solves, tiles, ntiles, err);
       case kTilingBlock8n:
         return launch_pdl(stage_narrow_batch_kernel<S>, dim3(ntiles), dim3(32, kNarrowThreads / 32),
-                          sizeof(StageSmem<8>) + 128, st, solves, tiles);
+                          sizeof(StageSmem<8>) + 128, st, solves, tiles, stage_prefetch_ahead());
       case kTilingBlock8:
         return launch_pdl(stage_batch_kernel<S, 8>, dim3(ntiles), dim3(32, STAGE_THREADS / 32),
-                          sizeof(StageSmem<8>) + 128, st, solves, tiles);
+                          sizeof(StageSmem<8>) + 128, st, solves, tiles, stage_prefetch_ahead());
       default:
         return launch_pdl(stage_batch_kernel<S, 16>, dim3(ntiles), dim3(32, STAGE_THREADS / 32),
-                          sizeof(StageSmem<16>) + 128, st, solves, tiles);
+                          sizeof(StageSmem<16>) + 128, st, solves, tiles, stage_prefetch_ahead());
     }
   });
 }

@@ -61,9 +61,43 @@ __device__ __forceinline__ float ko8f(const float *v, int c) {
   return skf(v, c, 4) - 8.0f * skf(v, c, 3) + 28.0f * skf(v, c, 2) - 56.0f * skf(v, c, 1);
 }
 
-// One 64 x 16 tile (columns c0.., rows b0..) of stage 2 or 3.
+// Single solve: the tile `n` places after this block's in launch order
+// (n = 0: none).
+struct MixGridAhead {
+  const MixedMaps *T;
+  int n;
+  __device__ __forceinline__ bool operator()(const MixedMaps *&pm, int &c0, int &b0) const {
+    const int L = blockIdx.y * gridDim.x + blockIdx.x + n;
+    if (n <= 0 || L >= static_cast<int>(gridDim.x * gridDim.y)) return false;
+    pm = T;
+    c0 = (L % gridDim.x) * TC;
+    b0 = (L / gridDim.x) * kMixRows;
+    return true;
+  }
+};
+// Batch: the work item `n` places later in the list.
 template <int STAGE>
-__device__ __forceinline__ void mixed_tile(const MixedMaps &T, const MixedArgs &A, const int c0, const int b0) {
+struct MixListAhead {
+  const MixedBatch *solves;
+  const BatchTile *tiles;
+  int n;
+  __device__ __forceinline__ bool operator()(const MixedMaps *&pm, int &c0, int &b0) const {
+    const int L = blockIdx.x + n;
+    if (n <= 0 || L >= static_cast<int>(gridDim.x)) return false;
+    const BatchTile w = tiles[L];
+    pm = &solves[w.pad].maps[STAGE - 2];
+    c0 = w.c0;
+    b0 = w.b0;
+    return true;
+  }
+};
+
+// One 64 x 16 tile (columns c0.., rows b0..) of stage 2 or 3.  Thread 0
+// prefetches into L2 the input of the later tile `ahead` names, so that the
+// block which takes it finds its loads there.
+template <int STAGE, class Ahead>
+__device__ __forceinline__ void mixed_tile(const MixedMaps &T, const MixedArgs &A, const int c0, const int b0,
+                                           const Ahead ahead) {
   constexpr int ROWS = kMixRows, RPT = ROWS / (kMixThreads / 32);
   extern __shared__ unsigned char smem_raw[];
   MixSmem<STAGE> &S = *reinterpret_cast<MixSmem<STAGE> *>(
@@ -91,6 +125,14 @@ __device__ __forceinline__ void mixed_tile(const MixedMaps &T, const MixedArgs &
     tma_load_3d(&S.q[0][0][0], &T.q, c0 - 4, b0 - 3, 0, &S.bar);
     tma_load_3d(&S.p[0][0][0], &T.p, c0 - 4, b0, 2, &S.bar);
     if (STAGE == 3) tma_load_3d(&S.u1[0][0][0], &T.u1, c0, b0, 0, &S.bar);
+    const MixedMaps *pm;
+    int pc0, pb0;
+    if (ahead(pm, pc0, pb0)) {
+      tma_prefetch_3d(&pm->q, pc0 - 4, pb0 - 3, 0);
+      tma_prefetch_3d(&pm->p, pc0 - 4, pb0, 2);
+      tma_prefetch_3d(&pm->bb, pc0, pb0, 0);
+      if (STAGE == 3) tma_prefetch_3d(&pm->u1, pc0, pb0, 0);
+    }
   }
   const bool ok = mbar_wait_bounded(&S.bar, 0);
   if (!__syncthreads_and(ok)) {
@@ -290,17 +332,18 @@ __device__ __forceinline__ void mixed_tile(const MixedMaps &T, const MixedArgs &
 
 template <int STAGE>
 __global__ void __launch_bounds__(kMixThreads, 3)
-    mixed_stage_kernel(const __grid_constant__ MixedMaps T, const MixedArgs A) {
-  mixed_tile<STAGE>(T, A, blockIdx.x * TC, blockIdx.y * kMixRows);
+    mixed_stage_kernel(const __grid_constant__ MixedMaps T, const MixedArgs A, int ahead) {
+  mixed_tile<STAGE>(T, A, blockIdx.x * TC, blockIdx.y * kMixRows, MixGridAhead{&T, ahead});
 }
 
 // Mixed-precision solves of a batch: block -> (solve, tile); the tile's pad
 // field indexes the MixedBatch array.
 template <int STAGE>
-__global__ void __launch_bounds__(kMixThreads, 3) mixed_batch_kernel(const MixedBatch *solves, const BatchTile *tiles) {
+__global__ void __launch_bounds__(kMixThreads, 3)
+    mixed_batch_kernel(const MixedBatch *solves, const BatchTile *tiles, int ahead) {
   const BatchTile t = tiles[blockIdx.x];
   const MixedBatch &B = solves[t.pad];
-  mixed_tile<STAGE>(B.maps[STAGE - 2], B.args[STAGE - 2], t.c0, t.b0);
+  mixed_tile<STAGE>(B.maps[STAGE - 2], B.args[STAGE - 2], t.c0, t.b0, MixListAhead<STAGE>{solves, tiles, ahead});
 }
 
 // bb, ee = Ataurho + bb, d_re = (Brho_re - bb Btau_re) - bb' ee and
@@ -400,16 +443,18 @@ cudaError_t prepare_mixed_kernels() {
 
 cudaError_t launch_mixed_stage(int stage, const MixedMaps &maps, const MixedArgs &a, cudaStream_t st) {
   const dim3 grid(a.N / TC, a.M / kMixRows), block(32, kMixThreads / 32);
-  if (stage == 2) return launch_pdl(mixed_stage_kernel<2>, grid, block, mix_smem_bytes<2>(), st, maps, a);
-  return launch_pdl(mixed_stage_kernel<3>, grid, block, mix_smem_bytes<3>(), st, maps, a);
+  const int ahead = stage_prefetch_ahead();
+  if (stage == 2) return launch_pdl(mixed_stage_kernel<2>, grid, block, mix_smem_bytes<2>(), st, maps, a, ahead);
+  return launch_pdl(mixed_stage_kernel<3>, grid, block, mix_smem_bytes<3>(), st, maps, a, ahead);
 }
 
 cudaError_t launch_mixed_batch(int stage, const MixedBatch *solves, const BatchTile *tiles, int ntiles,
                                cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
   const dim3 grid(ntiles), block(32, kMixThreads / 32);
-  if (stage == 2) return launch_pdl(mixed_batch_kernel<2>, grid, block, mix_smem_bytes<2>(), st, solves, tiles);
-  return launch_pdl(mixed_batch_kernel<3>, grid, block, mix_smem_bytes<3>(), st, solves, tiles);
+  const int ahead = stage_prefetch_ahead();
+  if (stage == 2) return launch_pdl(mixed_batch_kernel<2>, grid, block, mix_smem_bytes<2>(), st, solves, tiles, ahead);
+  return launch_pdl(mixed_batch_kernel<3>, grid, block, mix_smem_bytes<3>(), st, solves, tiles, ahead);
 }
 
 cudaError_t launch_mixed_coef(const double *coltab, const double *rowtab, const double *bbt, float *kc, int N, int M,
