@@ -12,7 +12,9 @@ The test checks the eleven files' names and row format (the columns
 QNM_Extraction's loadwaveforms reads: time, then h+ and hx for
 l = |m|..|m|+6, QNM_Extraction/Library/ringdownlib.py:102-109), that the
 rows start at t = Xmax + 200 every Fr steps, and that the m = 2 file is
-byte-identical to the same solve run through the Python binding."""
+byte-identical to the same solve run through the Python binding.  Both runs
+fix the stage tiling (BHR_STAGE_TILING): the autotuner times the tilings in
+each process, and different tilings agree to rounding, not bit for bit."""
 import os
 import subprocess
 
@@ -29,6 +31,7 @@ EXE = os.path.join(ROOT, "oracle", "_ref", "dropin_run")
 NAME = "a0.0_thi000_thf090.0_n"
 N, M, XMIN, XMAX, T, FR = 256, 32, -50.0, 50.0, 270.0, 50
 AA, DT = 1e-8, 0.002  # HighOrder/main.c:41,46
+TILING = "block8n"
 
 
 @pytest.fixture(scope="module")
@@ -41,7 +44,8 @@ def dropin_run(tmp_path_factory):
     traj = work / "Trajectories" / f"{NAME}.traj"
     # started well inside the ISCO, so the particle plunges within the run
     np.savetxt(traj, synthetic_plunge(AA, DT / 2.0, duration=T, r_offset=1.0), fmt="%.17g")
-    out = subprocess.run([EXE], cwd=work / "run", capture_output=True, text=True, timeout=900)
+    env = dict(os.environ, BHR_STAGE_TILING=TILING)
+    out = subprocess.run([EXE], cwd=work / "run", capture_output=True, text=True, timeout=900, env=env)
     assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
     assert "bhr:" not in out.stderr, out.stderr[-2000:]
     return work
@@ -62,10 +66,12 @@ def test_dropin_writes_one_reference_format_file_per_mode(dropin_run):
         assert np.max(np.abs(data[:, 1:])) > 0
 
 
-def test_dropin_m2_file_equals_the_python_binding_run(dropin_run, tmp_path):
+def test_dropin_m2_file_equals_the_python_binding_run(dropin_run, tmp_path, monkeypatch):
+    monkeypatch.setenv("BHR_STAGE_TILING", TILING)
     prm = bhr.Params(N=N, M=M, Xmin=XMIN, Xmax=XMAX, T=T, Fr=FR, PTSX=128, PTSY=128, out_start=XMAX + 200.0,
                      mass=1.0, a=AA, m=2.0, dt=DT, device=0)
     with bhr.Solver(prm) as s:
+        assert s.info()["tiling"] == TILING
         s.load_trajectory(str(dropin_run / "Trajectories" / f"{NAME}.traj"))
         s.run(str(tmp_path), NAME)
     for suffix in (".dat", ".dat.full"):
