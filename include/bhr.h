@@ -294,6 +294,61 @@ int bhr_engine_poll(bhr_engine *e, int64_t id, bhr_request_info *info);
 int bhr_engine_result(bhr_engine *e, int64_t id, double *t, double *h, double *dedt, int max_rows, int *nrows);
 int bhr_engine_stats(bhr_engine *e, bhr_engine_counters *st);
 
+/* ---- trajectory generation (GenOT) --------------------------------------
+ * Host code (no device work) restating GenOT, the reference's generator of
+ * the .traj worldlines the solver reads: an adiabatic inspiral (tabulated,
+ * from frequency-domain fluxes), the generalised Ori-Thorne transition and
+ * the geodesic plunge, in Mino time (GenOT/ParamWLMino.cc), then that
+ * worldline in Boyer-Lindquist time (GenOT/WL_BL.cc).  Units G = c = M = 1. */
+typedef struct bhr_genot_params {
+  double a;        /* black-hole spin (ParamWLMino argument 1)                */
+  double eta;      /* mass ratio (argument 2)                                 */
+  double LTi, LTf; /* Ori-Thorne times at which the transition begins and
+                      ends (arguments 4, 5)                                   */
+  double r_start;  /* radius at which the output starts (argument 6)          */
+  double dl;       /* Mino-time step of the output: 0.1 in the reference      */
+  int model;       /* E, L, Q through the transition (argument 7): 1 = LSO
+                      values plus a constant and a quadratic term, 2 = plus a
+                      quadratic and a cubic term                              */
+} bhr_genot_params;
+/* The Mino-time worldline (GenOT/ParamWLMino.cc:332-531).  insp: n_insp rows
+ * of 11 columns, the adiabatic inspiral table (time, Mino time, r,
+ * eccentricity, theta_inc in degrees, E, L, Q, and the E, L, Q fluxes, Mino
+ * time and fluxes with the mass ratio scaled out; its last row is the last
+ * stable orbit).  ot: n_ot rows (T, X) of the Ori-Thorne function, the
+ * solution of X'' = -X^2 - T that approaches sqrt(-T) as T -> -infinity.
+ * Writes rows (lambda, r, theta_inc, E, L, Q) from r_start until r passes
+ * r+ - 0.5 or lambda passes the end of the transition by 100; out = NULL
+ * only counts them (*n_out).  Inputs the reference exits on (model, LTf
+ * past the table, r_start or a Mino time outside the inspiral table) and a
+ * negative A or B return BHR_INVALID_ARG. */
+int bhr_genot_mino(const bhr_genot_params *p, const double *insp, int n_insp, const double *ot, int n_ot,
+                   double *out, int max_rows, int *n_out);
+typedef struct bhr_genot_bl_params {
+  double a;            /* spin (WL_BL argument 1)                             */
+  double lambda_start; /* Mino time at which the worldline starts (argument 3) */
+  double t_stop;       /* BL time at which it stops (argument 4)              */
+  double chi0_deg;     /* initial polar phase chi, cos(theta) =
+                          sin(theta_inc) cos(chi) (argument 5)                */
+  double phi0_deg;     /* initial axial angle (argument 6)                    */
+  double dt;           /* BL time step: 0.001 in the reference                */
+} bhr_genot_bl_params;
+/* The worldline in BL time (GenOT/WL_BL.cc:7-261): classical RK4 in t for
+ * (lambda, chi, phi) over splines of the Mino-time rows (n_mino rows of 6,
+ * as bhr_genot_mino writes them; the look-ups use rows 1..n_mino-1, as the
+ * reference's do).  Rows t, r, theta, dr/dt, dtheta/dt, dphi/dt, phi, E,
+ * L, Q (the .traj columns) for t = 0, dt, ... <= t_stop: every stride-th
+ * row to out (when not NULL), every row to the text file path (when not
+ * NULL; the reference's "%.12e" format).  *thf_deg and *thdot_pos: theta
+ * (degrees) and the sign of dtheta/dlambda at the last row (the reference
+ * names the file by them).  With out, path and thf_deg all NULL only
+ * *n_out is set (the rows out would receive). */
+int bhr_genot_bl(const bhr_genot_bl_params *p, const double *mino, int n_mino, int stride, double *out, int max_rows,
+                 int *n_out, double *thf_deg, int *thdot_pos, const char *path);
+/* The reference's .traj file name, a<a>_thi<theta_inc>_thf<theta_f>_<p|n>.traj
+ * (GenOT/WL_BL.cc:101-153). */
+int bhr_genot_traj_name(double a, double thi0_deg, double thf_deg, int thdot_pos, char *buf, int buflen);
+
 /* The reason for the last failed call made on the calling thread (the
  * string is per thread and valid until that thread's next failing call). */
 const char *bhr_last_error_string(void);

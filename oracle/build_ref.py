@@ -14,7 +14,10 @@ baseline and for the host-loop fixture).  Nothing is copied out of the
 reference tree and nothing is written outside oracle/_ref/.  The "dropin"
 tag links the reference's main.c and proj.c with this repository's
 bh_ringdown_b200/integration/body_bhr.c against libbhr.so into
-oracle/_ref/dropin_run (the drop-in as a maintainer would build it).
+oracle/_ref/dropin_run (the drop-in as a maintainer would build it).  The
+"genot" tag compiles the reference's trajectory generator, GenOT/
+ParamWLMino.cc and GenOT/WL_BL.cc, where they lie, as GenOT/README:30-31
+does (g++ ... -lm), into oracle/_ref/genot/{ParamWLMino,WL_BL}.
 
 Usage: python oracle/build_ref.py [--ref <reference root>] [tag ...]
 
@@ -41,7 +44,7 @@ TAGS = {
     "cfg2": (8192, 128, -200.0, 600.0),   # plunge-ringdown workload grid
     "p16k": (16384, 256, -200.0, 600.0),  # the same domain at 16384 x 256 (the default bench workload)
 }
-DEFAULT_TAGS = ("pin", "c1s", "cfg2", "p16k", "gpin", "gp16k", "dropin")
+DEFAULT_TAGS = ("pin", "c1s", "cfg2", "p16k", "gpin", "gp16k", "dropin", "genot")
 
 # main.c defines globals with the same names as kern.cu's device scalars;
 # they are renamed at compile time so both link into one library.
@@ -171,6 +174,19 @@ def build_dropin_tag(ref_root: str, tag: str) -> str:
     return exe
 
 
+# The reference's trajectory generator, its two programs built as its README
+# says (GenOT/README:30-31).
+GENOT_PROGRAMS = ("ParamWLMino", "WL_BL")
+
+
+def build_genot(ref_root: str, tag: str = "genot") -> str:
+    d = os.path.join(OUT, tag)
+    os.makedirs(d, exist_ok=True)
+    for prog in GENOT_PROGRAMS:
+        run(["g++", "-O2", "-w", os.path.join(ref_root, "GenOT", prog + ".cc"), "-o", os.path.join(d, prog), "-lm"])
+    return d
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=default_reference_root())
@@ -179,15 +195,18 @@ def main(argv=None) -> int:
     if not os.path.isdir(os.path.join(args.ref, "TD_GPU_code", "HighOrder")):
         print(f"build_ref: reference not found at {args.ref}; skipping", file=sys.stderr)
         return 0
-    bad = [t for t in args.tags if t not in TAGS and t not in GPU_TAGS and t not in DROPIN_TAGS]
+    known = sorted(TAGS) + sorted(GPU_TAGS) + sorted(DROPIN_TAGS) + ["genot"]
+    bad = [t for t in args.tags if t not in known]
     if bad:
-        print(f"unknown tags {bad}; known {sorted(TAGS) + sorted(GPU_TAGS) + sorted(DROPIN_TAGS)}", file=sys.stderr)
+        print(f"unknown tags {bad}; known {known}", file=sys.stderr)
         return 2
     os.makedirs(OUT, exist_ok=True)
 
     def build(t):
         if t in TAGS:
             return build_tag(args.ref, t)
+        if t == "genot":
+            return build_genot(args.ref, t)
         return build_gpu_tag(args.ref, t) if t in GPU_TAGS else build_dropin_tag(args.ref, t)
     with ThreadPoolExecutor(max_workers=len(args.tags)) as ex:
         for lib in ex.map(build, args.tags):
