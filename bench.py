@@ -179,19 +179,28 @@ def make_params(device=0, dt=None):
                       integrator=bhr.BHR_RK4 if INTEGRATOR == "rk4" else bhr.BHR_SSPRK3)
 
 
+# The plunge workloads' source: GenOT's transition-to-plunge worldline for
+# mass ratio 1e-3 from the ISCO, rows every dt/2 (the reference's step reads
+# two rows), 60 M of it (more than any timed or e2e run reaches).
+PLUNGE_ETA, PLUNGE_DURATION = 1e-3, 60.0
+
+
+def plunge_rows(a, dt):
+    from bh_ringdown_b200.genot import transition_plunge
+    return transition_plunge(a, PLUNGE_ETA, dt / 2.0, PLUNGE_DURATION)
+
+
 def workload_inputs(with_source, device=0):
     """(params, trajectory rows or None).  Without a source the run starts
     from a Gaussian pulse instead (psi = exp(-(x-20)^2/8) swsh(2,2))."""
     import bh_ringdown_b200 as bhr
-    from bh_ringdown_b200.trajectory import synthetic_plunge
     prm = make_params(device)
     x, r, th = bhr.grid(prm)
     dx = (prm.Xmax - prm.Xmin) / prm.N
     dt = prm.courant * min(dx, r[0] * np.pi / prm.M)
     prm.dt = dt
     if with_source:
-        rows = synthetic_plunge(prm.a, dt / 2.0, duration=60.0)
-        return prm, rows
+        return prm, plunge_rows(prm.a, dt)
     prm.init_kind = bhr.BHR_INIT_GAUSSIAN
     prm.init_center, prm.init_width, prm.init_ell = 20.0, 2.0, 2.0
     return prm, None
@@ -208,7 +217,8 @@ def workload_config(name, N, M, dt, with_source, world):
             "N_r": N, "N_theta": M, "dt": dt,
             "integrator": "classical RK4" if INTEGRATOR == "rk4" else "SSP-RK3",
             "precision": PRECISION,
-            "source": "synthetic prograde equatorial plunge from ISCO, rows every dt/2" if with_source else "none",
+            "source": (f"GenOT transition-to-plunge worldline (prograde equatorial, eta={PLUNGE_ETA:g}, from the "
+                       "ISCO; stand-in inspiral table), rows every dt/2") if with_source else "none",
             "parallelism": f"replicas x{world}"}
 
 
@@ -376,14 +386,13 @@ def reference_gpu_baseline(workload, prm):
     updates per second; None when the build is absent."""
     import subprocess
     import tempfile
-    from bh_ringdown_b200.trajectory import synthetic_plunge
     exe = REFERENCE_GPU_EXES.get(workload)
     if exe is None or PRECISION != "fp64" or INTEGRATOR != "ssprk3":
         return None
     path = os.path.join(ROOT, "oracle", "_ref", exe)
     if not os.path.exists(path):
         return {"unavailable": f"oracle/_ref/{exe} was not built (the reference tree was absent at build time)"}
-    rows = synthetic_plunge(prm.a, prm.dt / 2.0, duration=60.0)
+    rows = plunge_rows(prm.a, prm.dt)
     with tempfile.TemporaryDirectory() as work:
         os.makedirs(os.path.join(work, "Trajectories"))
         os.makedirs(os.path.join(work, "run"))
@@ -475,8 +484,7 @@ def run_reference(args, rank, world):
     dx = (w["Xmax"] - w["Xmin"]) / N
     dt = w["courant"] * min(dx, r[0] * np.pi / M)
     L.ref_init(D(1.0), D(w["a"]), D(w["m"]), D(dt), th.ctypes.data_as(C.c_void_p), r.ctypes.data_as(C.c_void_p))
-    from bh_ringdown_b200.trajectory import synthetic_plunge
-    rows = synthetic_plunge(w["a"], dt / 2.0, duration=60.0)
+    rows = plunge_rows(w["a"], dt)
     er, ei = np.zeros(M), np.zeros(M)
 
     # body.cu:97-124 consumption of the trajectory rows, restated.

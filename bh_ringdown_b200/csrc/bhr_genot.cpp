@@ -222,7 +222,7 @@ double dchi_dl(double a, double chi, double thi, double E, double L, double Q) {
 extern "C" {
 
 int bhr_genot_mino(const bhr_genot_params *p, const double *insp, int n_insp, const double *ot, int n_ot,
-                   double *out, int max_rows, int *n_out) {
+                   double *out, int max_rows, int *n_out, double *transition) {
   if (n_out) *n_out = 0;
   if (!p || !insp || !ot || !n_out || n_insp < 4 || n_ot < 4)
     return fail(BHR_INVALID_ARG, "bhr_genot_mino: null argument or too few table rows");
@@ -271,6 +271,12 @@ int bhr_genot_mino(const bhr_genot_params *p, const double *insp, int n_insp, co
   const Spline *ID[3] = {&I.dE, &I.dL, &I.dQ};
   for (int c = 0; c < 3; c++) T.join(c, lTi, IC[c]->value(lTi + off), ID[c]->value(lTi + off));
   const double Ep = T.C_of(0, lTf), Lp = T.C_of(1, lTf), Qp = T.C_of(2, lTf);  // the plunge's constants
+  if (transition) {
+    transition[0] = lTi;
+    transition[1] = lTf;
+    transition[2] = rTi;
+    transition[3] = T.r_of(lTf);
+  }
   if (I.r.y(0) < p->r_start)
     return fail(BHR_INVALID_ARG, "bhr_genot_mino: r_start is outside the inspiral table");
   const double lstart = I.lambda_at(p->r_start) - off;

@@ -51,7 +51,7 @@ def _lib():
         return lib
     dp = C.POINTER(D)
     lib.bhr_genot_mino.restype = I
-    lib.bhr_genot_mino.argtypes = [C.POINTER(GenotParams), dp, I, dp, I, dp, I, C.POINTER(I)]
+    lib.bhr_genot_mino.argtypes = [C.POINTER(GenotParams), dp, I, dp, I, dp, I, C.POINTER(I), dp]
     lib.bhr_genot_bl.restype = I
     lib.bhr_genot_bl.argtypes = [C.POINTER(GenotBLParams), dp, I, I, dp, I, C.POINTER(I), dp, C.POINTER(I),
                                  C.c_char_p]
@@ -167,9 +167,12 @@ def synthetic_inspiral(a: float, r_start: float, rows: int = 2000, fine: int = 4
 
 # ---- the two steps ----------------------------------------------------------
 def mino_worldline(a: float, eta: float, insp: np.ndarray, LTi: float, LTf: float, r_start: float,
-                   model: int = 2, dl: float = 0.1, ot: Optional[np.ndarray] = None) -> np.ndarray:
+                   model: int = 2, dl: float = 0.1, ot: Optional[np.ndarray] = None,
+                   transition: Optional[np.ndarray] = None) -> np.ndarray:
     """Rows (lambda, r, theta_inc, E, L, Q): ParamWLMino's output for
-    arguments a, eta, the inspiral table, LTi, LTf, r_start and model."""
+    arguments a, eta, the inspiral table, LTi, LTf, r_start and model.
+    transition (4 floats, optional) receives lambda and r where the
+    transition begins and ends."""
     lib = _lib()
     insp = np.ascontiguousarray(insp, dtype=np.float64)
     ot = np.ascontiguousarray(ot_table() if ot is None else ot, dtype=np.float64)
@@ -177,10 +180,13 @@ def mino_worldline(a: float, eta: float, insp: np.ndarray, LTi: float, LTf: floa
         raise ValueError("inspiral table needs 11 columns, the Ori-Thorne table 2")
     p = GenotParams(a, eta, LTi, LTf, r_start, dl, model)
     n = I(0)
-    _check(lib.bhr_genot_mino(C.byref(p), _ptr(insp), len(insp), _ptr(ot), len(ot), None, 0, C.byref(n)))
+    tr = np.zeros(4)
+    _check(lib.bhr_genot_mino(C.byref(p), _ptr(insp), len(insp), _ptr(ot), len(ot), None, 0, C.byref(n), None))
     out = np.zeros((n.value, 6))
     _check(lib.bhr_genot_mino(C.byref(p), _ptr(insp), len(insp), _ptr(ot), len(ot), _ptr(out), n.value,
-                              C.byref(n)))
+                              C.byref(n), _ptr(tr)))
+    if transition is not None:
+        transition[:] = (tr[0], tr[2], tr[1], tr[3])
     return out[: n.value]
 
 
@@ -225,6 +231,24 @@ def write_traj(directory: str, mino: np.ndarray, a: float, lambda_start: float, 
     if thf2 != thf:
         raise BhrError(1, "bl_worldline: the two passes disagree")
     return path
+
+
+def transition_plunge(a: float, eta: float, dt_row: float, duration: float, inclination_deg: float = 0.0,
+                      LTi: float = -3.0, LTf: float = 2.35, model: int = 2, chi0_deg: float = 0.0) -> np.ndarray:
+    """A transition-to-plunge source worldline as .traj rows every dt_row
+    in BL time for `duration`: the stand-in inspiral of spin a (from 1 M
+    outside the ISCO), GenOT's Mino-time worldline for mass ratio eta
+    (LTi = -3, LTf = 2.35, the values GenOT/README:159-166 recommends;
+    model 2), and its BL-time worldline from the Mino time at which the
+    transition begins, near the ISCO.  After the plunge the particle
+    approaches the horizon for the rest of the duration, as the reference's
+    files do."""
+    r_isco = _isco(a)
+    insp = synthetic_inspiral(a, r_isco + 1.0, inclination_deg=inclination_deg)
+    tr = np.zeros(4)
+    mino = mino_worldline(a, eta, insp, LTi, LTf, r_isco + 0.5, model=model, transition=tr)
+    rows, _, _ = bl_worldline(mino, a, tr[0], duration, chi0_deg, 0.0, dt=dt_row)
+    return rows
 
 
 def read_insp(path: str) -> np.ndarray:

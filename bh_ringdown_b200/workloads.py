@@ -8,7 +8,8 @@
 * ``serve_requests``: a Poisson request stream, 70 % source-free solves
   (N_r in {2048, 4096}, N_theta in {64, ..., 128}, a in [0, 0.99]) and 30 %
   plunge-driven solves (a in [0, 0.95], 8192 x 128 on [-200, 600], T = 1000,
-  source from a prograde equatorial plunge from the ISCO).
+  source from GenOT's transition-to-plunge worldline, prograde equatorial,
+  mass ratio 1e-3, from the ISCO).
 
 There is no public request log for this solver: these are synthetic
 stand-ins with the sizes and value ranges above.  ``time_scale`` shortens
@@ -24,7 +25,7 @@ from typing import List, Optional
 import numpy as np
 
 from . import BHR_FP64, BHR_INIT_GAUSSIAN, Params
-from .trajectory import synthetic_plunge
+from .genot import transition_plunge
 
 SEED = 20261203
 
@@ -89,7 +90,7 @@ def serve_requests(n: int = 2000, rate_per_s: float = 1.0, seed: int = SEED, tim
             prm = plunge_params(a, 1000.0 * time_scale, precision=precision)
             key = (a, prm.dt)
             if key not in trajs:
-                trajs[key] = synthetic_plunge(a, prm.dt / 2.0, duration=prm.T)
+                trajs[key] = transition_plunge(a, 1e-3, prm.dt / 2.0, prm.T)
             out.append(Request(prm, trajs[key], t, "plunge"))
         else:
             a = rng.uniform(0.0, 0.99)

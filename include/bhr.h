@@ -319,11 +319,14 @@ typedef struct bhr_genot_params {
  * solution of X'' = -X^2 - T that approaches sqrt(-T) as T -> -infinity.
  * Writes rows (lambda, r, theta_inc, E, L, Q) from r_start until r passes
  * r+ - 0.5 or lambda passes the end of the transition by 100; out = NULL
- * only counts them (*n_out).  Inputs the reference exits on (model, LTf
- * past the table, r_start or a Mino time outside the inspiral table) and a
- * negative A or B return BHR_INVALID_ARG. */
+ * only counts them (*n_out).  transition (4 doubles, may be NULL) receives
+ * the Mino times at which the transition begins and ends and r there
+ * (the output's lambda runs on the transition's origin).  Inputs the
+ * reference exits on (model, LTf past the table, r_start or a Mino time
+ * outside the inspiral table) and a negative A or B return
+ * BHR_INVALID_ARG. */
 int bhr_genot_mino(const bhr_genot_params *p, const double *insp, int n_insp, const double *ot, int n_ot,
-                   double *out, int max_rows, int *n_out);
+                   double *out, int max_rows, int *n_out, double *transition);
 typedef struct bhr_genot_bl_params {
   double a;            /* spin (WL_BL argument 1)                             */
   double lambda_start; /* Mino time at which the worldline starts (argument 3) */
