@@ -99,6 +99,8 @@ struct bhr_engine {
   std::vector<Running> to_release;
   int releasing = 0;  // finished solves being read back and released
   size_t used = 0;
+  int64_t head_id = -1;   // the oldest queued request when it last did not fit
+  int head_bypassed = 0;  // later requests prepared ahead of it since
   int64_t next_id = 1;
   bool stop = false;
   std::thread worker;
@@ -320,21 +322,35 @@ Finished finish(bhr_solver *s, const Running &R) {
   return f;
 }
 
+// Later requests prepared ahead of the oldest queued one while it does not
+// fit the budget, before admission waits for it (so it is not starved).
+constexpr int kMaxBypass = 64;
+
 // The worker: releases finished solves, then prepares queued requests in
 // arrival order while their estimated bytes fit the budget (one always
-// when nothing else holds memory).
+// when nothing else holds memory).  When the oldest does not fit, the
+// first later one that does goes ahead of it, up to kMaxBypass of them.
 void worker_loop(bhr_engine *e) {
   cudaSetDevice(e->device);
   std::unique_lock<std::mutex> lock(e->wmu);
   for (;;) {
-    auto fits = [&] {
-      if (e->queue.empty()) return false;
-      const Request &r = e->queue.front();
-      const size_t need = solve_bytes(r.p, static_cast<int>(r.traj.size() / 10));
-      const bool idle = e->used == 0;
-      return idle || e->used + need <= e->budget;
+    // index in the queue of the request to prepare next, or -1
+    auto pick = [&]() -> int {
+      if (e->queue.empty()) return -1;
+      auto fits = [&](const Request &r) {
+        return e->used == 0 || e->used + solve_bytes(r.p, static_cast<int>(r.traj.size() / 10)) <= e->budget;
+      };
+      if (fits(e->queue.front())) return 0;
+      if (e->queue.front().id != e->head_id) {
+        e->head_id = e->queue.front().id;
+        e->head_bypassed = 0;
+      }
+      if (e->head_bypassed >= kMaxBypass) return -1;
+      for (size_t i = 1; i < e->queue.size(); i++)
+        if (fits(e->queue[i])) return static_cast<int>(i);
+      return -1;
     };
-    e->wcv.wait(lock, [&] { return e->stop || !e->to_release.empty() || fits(); });
+    e->wcv.wait(lock, [&] { return e->stop || !e->to_release.empty() || pick() >= 0; });
     if (e->stop) return;
     if (!e->to_release.empty()) {
       std::vector<Running> rel;
@@ -358,8 +374,10 @@ void worker_loop(bhr_engine *e) {
       lock.lock();
       continue;
     }
-    Request r = std::move(e->queue.front());
-    e->queue.pop_front();
+    const int at = pick();
+    Request r = std::move(e->queue[static_cast<size_t>(at)]);
+    e->queue.erase(e->queue.begin() + at);
+    if (at > 0) e->head_bypassed++;
     const size_t need = solve_bytes(r.p, static_cast<int>(r.traj.size() / 10));
     e->used += need;
     e->preparing.insert(r.id);

@@ -201,6 +201,26 @@ def test_budget_admits_one_at_a_time_when_tight():
             assert np.array_equal(h, h0)
 
 
+def test_requests_that_fit_go_ahead_of_one_that_does_not():
+    """Budget for one large solve and some small ones: with a large one
+    running, a second large request waits while the small requests behind
+    it are admitted (no head-of-line blocking), and all finish as alone."""
+    big = [gauss(2048, 256, -50.0, 50.0, 0.5, 2.0, 15.0, center=4.0 + k) for k in range(2)]
+    small = [gauss(256, 32, -50.0, 50.0, 0.7, 2.0, 5.0, center=5.0 + k) for k in range(2)]
+    with bhr.Engine(hbm_budget_bytes=80 << 20) as e:
+        ids = [e.submit(p) for p in big + small]
+        e.run_all(chunk=8)
+        info = [e.poll(i) for i in ids]
+        assert all(x["state"] == bhr.Engine.DONE for x in info), info
+        # the second large solve starts after the first finished; the small ones before that
+        assert info[1]["start_s"] >= info[0]["finish_s"]
+        assert info[2]["start_s"] < info[0]["finish_s"] and info[3]["start_s"] < info[0]["finish_s"]
+        res = [e.result(i) for i in ids]
+    for p, (t, h, d) in zip(big + small, res):
+        t0, h0, d0 = run_alone(p, None)
+        assert np.array_equal(t, t0) and np.array_equal(h, h0)
+
+
 def test_invalid_request_fails_alone():
     good = requests()[0]
     bad = gauss(200, 32, -50.0, 50.0, 0.5, 2.0, 10.0)  # N not a multiple of 64
