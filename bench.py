@@ -240,7 +240,7 @@ def run_ours(args, rank, local_rank, world):
     solver = bhr.Solver(prm)
     if rows is not None:
         solver.set_trajectory(rows)
-    tiling = solver.info()["tiling"]
+    tiling, ahead = solver.info()["tiling"], solver.info()["prefetch_ahead"]
     # Three states of 32 B per point larger than L2: the timed steps run back
     # to back (each reads what the previous one wrote from HBM); otherwise L2
     # is flushed before each step and each step is timed alone.
@@ -346,7 +346,7 @@ def run_ours(args, rank, local_rank, world):
                               f"working set {3 * 32 * N * M / 2**20:.0f} MiB > L2 (126 MiB): "
                               f"{args.steps} steps back to back, no flush"),
                        "events": "CUDA events on the solver stream around graph-launched steps",
-                       "stage_tiling": tiling},
+                       "stage_tiling": tiling, "prefetch_ahead_blocks": ahead},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": None if traffic_pp is None else traffic_pp * N * M,

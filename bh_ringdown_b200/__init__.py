@@ -56,7 +56,7 @@ class Particle(C.Structure):
 class _Info(C.Structure):
     _fields_ = [("N", I), ("M", I), ("dx", D), ("dtheta", D), ("dt", D), ("nt", I), ("Fr", I),
                 ("steps_done", I), ("rows_done", I), ("has_source", I), ("r_plus", D), ("device_bytes", C.c_size_t),
-                ("tile_rows", I), ("persistent", I), ("tiling", I)]
+                ("tile_rows", I), ("persistent", I), ("tiling", I), ("prefetch_ahead", I)]
 
 TILINGS = ("block8", "block16", "persistent", "block8n", "ring", "strip12")  # bhr_tiling, by value
 

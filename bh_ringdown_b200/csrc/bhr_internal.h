@@ -82,8 +82,8 @@ struct StageArgs {
   int narrow;           // 1: 8-row tiles on 128-thread blocks (four per SM)
   int ring;             // 1: 8-row tiles walked by two 256-thread blocks per SM, two buffers each
   int ahead;            // one-tile-per-block kernels: each block prefetches into L2 the stage
-                        // input of the block this many places later in launch order (0: none;
-                        // launch_stage sets it)
+                        // input of the block this many places later in launch order (0: none,
+                        // -1: stage_prefetch_ahead's default; launch_stage resolves it)
   float *dout;          // mixed precision, stage 1: delta1 = dt L(u^n) in FP32, or nullptr
   double *zout;         // RK4 stage 2: z = (y1 + 2 y2 - u^n)/3, or nullptr
   double dt;            // the stage's step in the combination (RK4: dt/2, dt, dt/6)
@@ -236,8 +236,10 @@ cudaError_t launch_init_product(double *q, const double *fa, const double *gb, i
 size_t stage_smem_bytes();
 cudaError_t prepare_kernels();
 // Blocks ahead (in launch order) whose input a one-tile-per-block stage
-// kernel prefetches into L2: twice the SM count, or BHR_PREFETCH_AHEAD
-// (0: no prefetch).
-int stage_prefetch_ahead();
+// kernel prefetches into L2: BHR_PREFETCH_AHEAD when set (0: no prefetch),
+// else `requested` when >= 0, else twice the SM count.
+int stage_prefetch_ahead(int requested = -1);
+// The device's SM count (cached per device).
+int device_sm_count();
 
 }  // namespace bhr

@@ -1467,21 +1467,24 @@ static cudaError_t by_stage(const int stage, F &&f) {
 
 // Blocks ahead (in launch order) whose stage input a one-tile-per-block
 // stage kernel prefetches into L2: twice the SM count (half a wave of
-// block8n's four blocks per SM, one wave of block8's two), or
+// block8n's four blocks per SM, one wave of block8's two) unless the caller
+// asks for another distance (the solver's autotuner times a few), or
 // BHR_PREFETCH_AHEAD (0 turns the prefetch off).  Measured at 16384 x 256,
 // block8n: 220 us per step without, 203 us with 259-333 blocks ahead, 210
 // at 592, 246 at 1184 (prefetched lines evicted before use).
-int stage_prefetch_ahead() {
+int stage_prefetch_ahead(const int requested) {
   static const int env = [] {
     const char *v = std::getenv("BHR_PREFETCH_AHEAD");
     return v ? std::max(0, std::atoi(v)) : -1;
   }();
-  return env >= 0 ? env : 2 * sm_count();
+  if (env >= 0) return env;
+  return requested >= 0 ? requested : 2 * sm_count();
 }
+int device_sm_count() { return sm_count(); }
 
 cudaError_t launch_stage(int stage, const StageMaps &maps, const StageArgs &a_in, cudaStream_t st, bool pdl) {
   StageArgs a = a_in;
-  a.ahead = (a.persist || a.ring) ? 0 : stage_prefetch_ahead();
+  a.ahead = (a.persist || a.ring) ? 0 : stage_prefetch_ahead(a.ahead);
   return by_stage(stage, [&](auto sc) {
     constexpr int S = decltype(sc)::value;
     if (a.narrow) {

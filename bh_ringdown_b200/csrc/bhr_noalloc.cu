@@ -172,6 +172,7 @@ extern "C" int bhr_step_noalloc(const bhr_params *p, double *state, int nsteps, 
 
   const double third = 0.33333333333333333;
   StageArgs A{};
+  A.ahead = -1;  // the default L2 prefetch distance
   A.coltab = coltab;
   A.rowtab = rowtab;
   A.src = nullptr;

@@ -475,6 +475,7 @@ int bhr_solver_info(const bhr_solver *s, bhr_info *info) {
   info->device_bytes = s->bytes;
   info->tile_rows = s->tile_rows;
   info->persistent = s->persist || s->ring;
+  info->prefetch_ahead = (s->persist || s->ring) ? 0 : stage_prefetch_ahead(s->ahead);
   info->tiling = s->strip12 ? BHR_TILING_STRIP12
                  : s->ring ? BHR_TILING_RING
                  : s->narrow ? BHR_TILING_BLOCK8N
@@ -813,14 +814,16 @@ static int encode_maps(bhr_solver *s, int rows) {
 
 
 // Stage tiling autotuner: per (device, N, M) the stage kernels are timed
-// with 8- and 16-row tiles one per 256-thread block, 8-row tiles on
-// 128-thread blocks, the persistent 16-row kernels and the 8-row ring, on
-// stages 1 and 2 (which write only the solve's scratch stages u1, u2); the
+// on stages 1 and 2 (which write only the solve's scratch stages u1, u2):
+// 8-row tiles on 128-thread blocks with the L2 prefetch one, two or four
+// SM-counts ahead or none (the staging depth), 8- and 16-row tiles one per
+// 256-thread block, the persistent 16-row kernels, the 8-row ring, and
+// stages 1 and 2 fused in one launch (FP64 SSP-RK3 solves only); the
 // fastest is kept for the process.
 static int autotune_rows(bhr_solver *s) {
   static std::mutex mu;
-  // device, N, M, FP64 SSP-RK3, rows, persist, narrow, ring, strip12
-  static std::vector<std::array<int, 9>> cache;
+  // device, N, M, FP64 SSP-RK3, rows, persist, narrow, ring, strip12, ahead
+  static std::vector<std::array<int, 10>> cache;
   const bhr_params &p = s->p;
   const int fused_ok = (!s->mixed && !s->rk4) ? 1 : 0;
   {
@@ -831,26 +834,32 @@ static int autotune_rows(bhr_solver *s) {
         s->narrow = c[6];
         s->ring = c[7];
         s->strip12 = c[8];
+        s->ahead = c[9];
         return encode_maps(s, c[4]);
       }
   }
   // rows, persist, narrow, ring, strip12 (stages 1 and 2 in one launch: only
-  // FP64 SSP-RK3 solves; its stage 3 is block8n)
-  static const int cands[6][5] = {{8, 0, 0, 0, 0}, {16, 0, 0, 0, 0}, {16, 1, 0, 0, 0},
-                                  {8, 0, 1, 0, 0}, {8, 0, 0, 1, 0}, {8, 0, 1, 0, 1}};
-  const int ncand = fused_ok ? 6 : 5;
+  // FP64 SSP-RK3 solves; its stage 3 is block8n), prefetch distance in SM
+  // counts (-1: none)
+  static const int cands[9][6] = {{8, 0, 1, 0, 0, 2}, {8, 0, 1, 0, 0, 1}, {8, 0, 1, 0, 0, 4}, {8, 0, 1, 0, 0, -1},
+                                  {8, 0, 0, 0, 0, 2}, {16, 0, 0, 0, 0, 2}, {16, 1, 0, 0, 0, 0},
+                                  {8, 0, 0, 1, 0, 0}, {8, 0, 1, 0, 1, 2}};
+  const int ncand = fused_ok ? 9 : 8;
+  const int nsm = device_sm_count();
   double best_ms = 1e30;
-  int best = 1;
+  int best = 0;
   cudaEvent_t e0, e1;
   BHR_CUDA_TRY(cudaEventCreate(&e0));
   BHR_CUDA_TRY(cudaEventCreate(&e1));
   // Stages 1 and 2 (they write only the solve's scratch stages u1, u2) of
   // each candidate, or the fused launch that replaces them.
+  auto ahead_of = [&](int c) { return cands[c][5] < 0 ? 0 : cands[c][5] * nsm; };
   for (int c = 0; c < ncand; c++) {
     s->persist = cands[c][1];
     s->narrow = cands[c][2];
     s->ring = cands[c][3];
     s->strip12 = cands[c][4];
+    s->ahead = ahead_of(c);
     if (int st = encode_maps(s, cands[c][0])) return st;
     StageArgs A = solver_stage_args(s);
     A.src = nullptr;
@@ -880,12 +889,13 @@ static int autotune_rows(bhr_solver *s) {
   {
     std::lock_guard<std::mutex> lock(mu);
     cache.push_back({p.device, p.N, p.M, fused_ok, cands[best][0], cands[best][1], cands[best][2], cands[best][3],
-                     cands[best][4]});
+                     cands[best][4], ahead_of(best)});
   }
   s->persist = cands[best][1];
   s->narrow = cands[best][2];
   s->ring = cands[best][3];
   s->strip12 = cands[best][4];
+  s->ahead = ahead_of(best);
   return encode_maps(s, cands[best][0]);
 }
 
@@ -909,6 +919,7 @@ StageArgs bhr::solver_stage_args(bhr_solver *s) {
   A.persist = s->persist;
   A.narrow = s->narrow;
   A.ring = s->ring;
+  A.ahead = s->ahead;
   A.dt = p.dt;
   A.cx = 0.016666666666667 * odx;
   A.cy = 0.05 * third * odth;

@@ -44,6 +44,7 @@ struct bhr_solver {
   int tile_rows = 16; // stage tile height chosen for this grid
   int persist = 0;     // 1: persistent stage kernels (16-row tiles, one block per SM)
   int narrow = 0;      // 1: 8-row tiles on 128-thread blocks (four per SM)
+  int ahead = -1;      // L2 prefetch distance of the one-tile-per-block stage kernels (-1: default)
   int ring = 0;        // 1: 8-row tiles through 2-buffer rings, two 256-thread blocks per SM
   int strip12 = 0;     // 1: stages 1 and 2 in one launch over column strips (FP64 SSP-RK3; stage 3 block8n)
   bhr::StripMaps smaps;

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define BHR_ABI_VERSION 2
+#define BHR_ABI_VERSION 3
 
 typedef enum bhr_status {
   BHR_OK = 0,
@@ -124,6 +124,10 @@ typedef struct bhr_info {
   int tile_rows;      /* stage tile height the autotuner chose (8 or 16)   */
   int persistent;     /* 1: persistent stage kernels (one block per SM)      */
   int tiling;         /* bhr_tiling: the stage kernels this solve runs       */
+  int prefetch_ahead; /* one-tile-per-block tilings: each block prefetches into
+                         L2 the stage input of the block this many places
+                         later in launch order (0: none); autotuned with the
+                         tiling                                              */
 } bhr_info;
 
 typedef struct bhr_solver bhr_solver;

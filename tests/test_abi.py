@@ -27,7 +27,7 @@ def test_library_loads_and_exports_every_declared_symbol():
     assert len(names) >= 20
     for n in names:
         assert hasattr(lib, n), n
-    assert lib.bhr_abi_version() == 2
+    assert lib.bhr_abi_version() == 3
 
 
 def test_params_default_are_the_reference_values():
