@@ -1,7 +1,7 @@
 """ctypes binding of the FP64 CPU oracle (oracle/liboracle.so).
 
 TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
-cpu_baseline leg of bench.py as the checker.  The product never imports it.
+cpu_baseline leg of bench.py as the oracle.  The product never imports it.
 """
 from __future__ import annotations
 

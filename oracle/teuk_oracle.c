@@ -1,7 +1,7 @@
 /*
  * teuk_oracle.c -- FP64 CPU oracle for the 2+1 s=-2 Teukolsky evolution.
  *
- * TEST INFRASTRUCTURE ONLY: the checker that tests/, __graft_entry__.smoke()
+ * TEST INFRASTRUCTURE ONLY: the oracle that tests/, __graft_entry__.smoke()
  * and bench.py's cpu_baseline leg compare the CUDA path against.  Nothing in
  * the product library links or calls this file.
  *

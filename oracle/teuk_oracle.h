@@ -1,7 +1,7 @@
 /*
  * teuk_oracle.h -- FP64 CPU oracle for the 2+1 s=-2 Teukolsky evolution.
  *
- * TEST INFRASTRUCTURE ONLY.  This library is the checker: tests/,
+ * TEST INFRASTRUCTURE ONLY.  This library is the oracle: tests/,
  * __graft_entry__.smoke() and the cpu_baseline leg of bench.py load it to
  * compare the CUDA path against.  It is never linked into, called by, or
  * shipped with the product library (bh_ringdown_b200).

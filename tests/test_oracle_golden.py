@@ -41,7 +41,7 @@ def test_grid_coefficients_and_evolution_match_reference(case):
         ref = g["final"][f]
         scale = max(np.max(np.abs(ref)), 1e-300)
         assert np.max(np.abs(st[f] - ref)) <= 1e-12 * scale, (case, f, np.max(np.abs(st[f] - ref)) / scale)
-    # psi at column N-1 every step (d_qre_buff/d_qim_buff), judged on the
+    # psi at column N-1 every step (d_qre_buff/d_qim_buff), compared on the
     # scale of the field: far from the pulse the column holds rounding noise.
     scale = np.max(np.abs(g["final"][:2]))
     assert np.max(np.abs(ext - g["ext"])) <= 1e-12 * scale
