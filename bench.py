@@ -234,7 +234,7 @@ def run_ours(args, rank, local_rank, world):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     with_source = WORKLOAD["source"]
     if with_source and not source_available():
-        raise SystemExit("the particle source coefficients are unavailable in this build")
+        raise SystemExit("the particle source coefficients are unavailable in libbhr.so")
     prm, rows = workload_inputs(with_source, device=local_rank)
     N, M = prm.N, prm.M
     solver = bhr.Solver(prm)

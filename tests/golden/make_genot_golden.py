@@ -12,7 +12,7 @@ working directory, where ParamWLMino reads it.  WL_BL keeps eleven
 Recorded: the inspiral table, a subsample of the Mino-time rows and of the
 .traj rows (every row of both is compared when the programs are present,
 by tests/test_genot.py), the .traj file name, and every 1000th row of the
-reference's own OT_X_vs_L.dat (the table this build's ot_table replaces).
+reference's own OT_X_vs_L.dat (the table genot.ot_table replaces).
 Nothing of the generator is restated here: this script only writes inputs
 and reads the reference's outputs.
 
