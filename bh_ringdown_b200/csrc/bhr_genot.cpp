@@ -194,6 +194,14 @@ int fail(int code, const std::string &msg) {
   return code;
 }
 
+// Column c of n rows of `width` doubles strictly increases (the splines'
+// knots; the reference stops on a repeated knot).
+bool increasing(const double *rows, int n, int width, int c) {
+  for (int i = 1; i < n; i++)
+    if (!(rows[static_cast<size_t>(i) * width + c] > rows[static_cast<size_t>(i - 1) * width + c])) return false;
+  return true;
+}
+
 // The three BL-time derivatives of the worldline with respect to Mino time
 // (GenOT/WL_BL.cc:340-380): dt/dlambda, dphi/dt and dchi/dlambda, where
 // cos(theta) = sin(theta_inc) cos(chi).
@@ -229,6 +237,9 @@ int bhr_genot_mino(const bhr_genot_params *p, const double *insp, int n_insp, co
   if (p->model != 1 && p->model != 2) return fail(BHR_INVALID_ARG, "bhr_genot_mino: model must be 1 or 2");
   if (!(p->eta > 0.0) || !(p->dl > 0.0) || !(std::fabs(p->a) < 1.0))
     return fail(BHR_INVALID_ARG, "bhr_genot_mino: need eta > 0, dl > 0, |a| < 1");
+  if (!increasing(insp, n_insp, 11, 1) || !increasing(ot, n_ot, 2, 0))
+    return fail(BHR_INVALID_ARG, "bhr_genot_mino: Mino time of the inspiral table and T of the Ori-Thorne table "
+                                 "must increase");
   const double a = p->a, eta = p->eta;
   const Inspiral I(insp, n_insp, eta);
   // LSO: the inspiral table's last row
@@ -340,6 +351,8 @@ int bhr_genot_bl(const bhr_genot_bl_params *p, const double *mino, int n_mino, i
   if (!p || !mino || !n_out || n_mino < 4 || stride < 1)
     return fail(BHR_INVALID_ARG, "bhr_genot_bl: null argument, too few rows or stride < 1");
   if (!(p->dt > 0.0) || !(std::fabs(p->a) < 1.0)) return fail(BHR_INVALID_ARG, "bhr_genot_bl: need dt > 0, |a| < 1");
+  if (!increasing(mino + 6, n_mino - 1, 6, 0))
+    return fail(BHR_INVALID_ARG, "bhr_genot_bl: the worldline's Mino time must increase");
   // rows of BL time: t = 0, dt, 2 dt, ... (accumulated) while t <= t_stop
   int nrows = 0;
   for (double t = 0.0; t <= p->t_stop; t += p->dt) nrows++;

@@ -155,6 +155,15 @@ def test_bad_inputs_are_rejected():
         genot.mino_worldline(a, eta, insp, LTi, LTf, insp[0, 2] + 1.0)
     with pytest.raises(ValueError):
         genot.synthetic_inspiral(0.7, 3.0)
+    twice = np.array(insp)
+    twice[5, 1] = twice[4, 1]  # a repeated Mino time
+    with pytest.raises(bhr.BhrError, match="increase"):
+        genot.mino_worldline(a, eta, twice, LTi, LTf, r_start)
+    mino = _mino(name)
+    back = np.array(mino[:50])
+    back[10, 0] = back[9, 0]
+    with pytest.raises(bhr.BhrError, match="increase"):
+        genot.bl_worldline(back, a, float(back[2, 0]), 1.0)
 
 
 @pytest.mark.gpu
