@@ -243,3 +243,41 @@ def test_tiny_grids_every_tiling(tiling, N, M, monkeypatch):
     o.step(20)
     assert rel_field_err(s.get_state(), o.get_state()) <= FIELD_TOL
     s.close()
+
+
+_PREFETCH_RUN = """
+import sys
+import numpy as np
+import bh_ringdown_b200 as bhr
+from bh_ringdown_b200.trajectory import synthetic_plunge
+N, M, Xmin, Xmax, a = 1024, 64, -50.0, 50.0, 0.7
+dt = 0.25 * (Xmax - Xmin) / N
+prm = bhr.Params(N=N, M=M, Xmin=Xmin, Xmax=Xmax, a=a, m=2.0, dt=dt, Fr=5, T=100.0, out_start=0.0, ext_col=640)
+with bhr.Solver(prm) as s:
+    assert s.info()["tiling"] == "block8n", s.info()
+    s.set_trajectory(synthetic_plunge(a, dt / 2.0, duration=100.0))
+    s.step(60)
+    t, h, _ = s.waveform()
+    np.savez(sys.argv[1], state=np.array(s.get_state()), h=h, ahead=s.info()["prefetch_ahead"])
+"""
+
+
+def test_l2_prefetch_distance_does_not_change_results(tmp_path):
+    """The L2 prefetch is only a hint: a sourced block8n solve with it off,
+    at the default distance and past the end of the grid gives bit-identical
+    fields and waveform (each in its own process: the distance override is
+    read once per process)."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    runs = {}
+    for ahead in ("0", "296", "100000"):
+        env = dict(os.environ, BHR_STAGE_TILING="block8n", BHR_PREFETCH_AHEAD=ahead)
+        f = tmp_path / f"run{ahead}.npz"
+        subprocess.run([sys.executable, "-c", _PREFETCH_RUN, str(f)], env=env, cwd=root, check=True, timeout=600)
+        runs[ahead] = np.load(f)
+        assert int(runs[ahead]["ahead"]) == int(ahead)
+    for ahead in ("296", "100000"):
+        assert np.array_equal(runs[ahead]["state"], runs["0"]["state"])
+        assert np.array_equal(runs[ahead]["h"], runs["0"]["h"])
