@@ -6,8 +6,10 @@ linked to libbhr.so (oracle/build_ref.py, tag "dropin": 256 x 32 on
 [-50, 50], T = 270, Fr = 50).
 
 It reads its trajectory where body() does, ../Trajectories/
-a0.0_thi000_thf090.0_n.traj (HighOrder/body.cu:77), here a synthetic
-Schwarzschild plunge sampled at dt/2, and writes one waveform file per m.
+a0.0_thi000_thf090.0_n.traj (HighOrder/body.cu:77), here written as the
+reference's workflow writes it: GenOT's transition-to-plunge worldline
+(bh_ringdown_b200.genot, a = 1e-8, mass ratio 1e-3) sampled at dt/2; it
+writes one waveform file per m.
 The test checks the eleven files' names and row format (the columns
 QNM_Extraction's loadwaveforms reads: time, then h+ and hx for
 l = |m|..|m|+6, QNM_Extraction/Library/ringdownlib.py:102-109), that the
@@ -22,7 +24,7 @@ import numpy as np
 import pytest
 
 import bh_ringdown_b200 as bhr
-from bh_ringdown_b200.trajectory import synthetic_plunge
+from bh_ringdown_b200.genot import transition_plunge
 
 pytestmark = pytest.mark.gpu
 
@@ -42,8 +44,8 @@ def dropin_run(tmp_path_factory):
     (work / "Trajectories").mkdir()
     (work / "run").mkdir()
     traj = work / "Trajectories" / f"{NAME}.traj"
-    # started well inside the ISCO, so the particle plunges within the run
-    np.savetxt(traj, synthetic_plunge(AA, DT / 2.0, duration=T, r_offset=1.0), fmt="%.17g")
+    # from the start of the transition near the ISCO through the plunge
+    np.savetxt(traj, transition_plunge(AA, 1e-3, DT / 2.0, T), fmt="%.17g")
     env = dict(os.environ, BHR_STAGE_TILING=TILING)
     out = subprocess.run([EXE], cwd=work / "run", capture_output=True, text=True, timeout=900, env=env)
     assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
