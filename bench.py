@@ -721,8 +721,14 @@ def run_serve(args):
     dev_pts = sum(replicas.gather_objects(st["point_updates"], dist))
     dev_ms = replicas.max_over_ranks(st["device_ms"], dist, device="cuda")
 
-    # the plain path: the same requests one at a time through bhr_solver (one per GPU)
+    # the plain path: the same requests one at a time through bhr_solver (one per GPU);
+    # each grid shape's one-time autotuning is done first, untimed, as a
+    # long-running plain server would have done it long before
     nplain = min(len(reqs), max(1, args.plain_requests // world))
+    for shape in sorted({(r.params.N, r.params.M) for r in reqs[:nplain]}):
+        warm = next(r for r in reqs[:nplain] if (r.params.N, r.params.M) == shape)
+        with bhr.Solver(dataclasses.replace(warm.params, precision=bhr.BHR_FP64)):
+            pass
     service = []
     for r in reqs[:nplain]:
         t0 = time.perf_counter()
@@ -762,7 +768,8 @@ def run_serve(args):
         "device_pt_updates_per_s": dev_pts / (dev_ms / 1e3),
         "plain": {"capacity_solves_per_s": plain_capacity, "p50_s": float(np.percentile(plat, 50)),
                   "p99_s": float(np.percentile(plat, 99)), "measured_requests": nplain,
-                  "note": "bhr_solver one request at a time, wall-clock service times, FCFS queue"},
+                  "note": "bhr_solver one request at a time, wall-clock service times (each grid shape "
+                          "autotuned beforehand, untimed), FCFS queue"},
         "capacity_vs_plain": engine_capacity / plain_capacity,
         "e2e": {"value": len(lat) / makespan, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                 "note": "wall clock of the whole stream through bhr_engine_submit/step/poll"},
