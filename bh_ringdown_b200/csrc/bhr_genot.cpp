@@ -292,6 +292,8 @@ int bhr_genot_mino(const bhr_genot_params *p, const double *insp, int n_insp, co
     return fail(BHR_INVALID_ARG, "bhr_genot_mino: r_start is outside the inspiral table");
   const double lstart = I.lambda_at(p->r_start) - off;
   const double lend = lTf + 100.0, dl = p->dl, r_stop = 1.0 + std::sqrt((1.0 - a) * (1.0 + a)) - 0.5;
+  if (!((lend - lstart) / dl < 2e8))
+    return fail(BHR_INVALID_ARG, "bhr_genot_mino: more than 2e8 rows (eta too small or dl too fine)");
   double rh = 0, vh = 0, thih = 0, eh = 0, lh = 0, qh = 0;
   bool in_trans = false;
   int n = 0;
@@ -353,6 +355,7 @@ int bhr_genot_bl(const bhr_genot_bl_params *p, const double *mino, int n_mino, i
   if (!(p->dt > 0.0) || !(std::fabs(p->a) < 1.0)) return fail(BHR_INVALID_ARG, "bhr_genot_bl: need dt > 0, |a| < 1");
   if (!increasing(mino + 6, n_mino - 1, 6, 0))
     return fail(BHR_INVALID_ARG, "bhr_genot_bl: the worldline's Mino time must increase");
+  if (!(p->t_stop / p->dt < 2e8)) return fail(BHR_INVALID_ARG, "bhr_genot_bl: more than 2e8 rows");
   // rows of BL time: t = 0, dt, 2 dt, ... (accumulated) while t <= t_stop
   int nrows = 0;
   for (double t = 0.0; t <= p->t_stop; t += p->dt) nrows++;
