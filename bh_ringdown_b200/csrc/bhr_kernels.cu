@@ -486,6 +486,15 @@ __device__ __forceinline__ void tile_prefetch(const StageMaps &T, const int c0, 
   if (STAGE != 1) tma_prefetch_3d(&T.u, c0, b0, 0);
 }
 
+// Thread 0: prefetch into L2 what the next stage reads of a tile: this
+// stage's output there (the next stage's input; its halo is the
+// neighbouring tiles' outputs), u^n and the bb window.
+__device__ __forceinline__ void tile_prefetch_next(const StageMaps &T, const int c0, const int b0) {
+  tma_prefetch_3d(&T.o, c0, b0, 0);
+  tma_prefetch_3d(&T.u, c0, b0, 0);
+  tma_prefetch_3d(&T.coef_bb, c0 - 4, b0, 0);
+}
+
 // One tile per block (grid N/64 x M/ROWS, two blocks per SM).  Thread 0
 // prefetches the tile `ahead` names, if any (after the grid dependency).
 template <int STAGE, int ROWS, int THREADS, class Ahead>
@@ -509,7 +518,9 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
     tile_note_source(S, A);
     const StageMaps *pm;
     int pc0, pb0;
-    if (ahead(pm, pc0, pb0)) tile_prefetch<STAGE>(*pm, pc0, pb0);
+    const int kind = ahead(pm, pc0, pb0);
+    if (kind == 1) tile_prefetch<STAGE>(*pm, pc0, pb0);
+    if (kind == 2) tile_prefetch_next(*pm, pc0, pb0);
   }
   const bool ok = mbar_wait_bounded(&S.bar, 0);
   if (!__syncthreads_and(ok)) {
@@ -523,34 +534,45 @@ __device__ __forceinline__ void stage_tile(const StageMaps &T, const StageArgs &
 }
 
 // Single solve: the block's tile is blockIdx.y * gridDim.x + blockIdx.x in
-// launch order; the tile `n` places later (n = A.ahead, 0: none).
+// launch order; the tile `n` places later (kind 1; n = A.ahead, 0: none).
+// The last n blocks name instead the next stage's first n tiles (kind 2):
+// their input, this stage's output and u^n, was written long before and has
+// left L2.
 template <int ROWS>
 struct GridAhead {
   const StageMaps *T;
   int n;
-  __device__ __forceinline__ bool operator()(const StageMaps *&pm, int &c0, int &b0) const {
-    const int L = blockIdx.y * gridDim.x + blockIdx.x + n;
-    if (n <= 0 || L >= static_cast<int>(gridDim.x * gridDim.y)) return false;
+  __device__ __forceinline__ int operator()(const StageMaps *&pm, int &c0, int &b0) const {
+    const int ntiles = static_cast<int>(gridDim.x * gridDim.y);
+    int L = blockIdx.y * gridDim.x + blockIdx.x + n, kind = 1;
+    if (n <= 0) return 0;
+    if (L >= ntiles) {
+      L -= ntiles;
+      kind = 2;
+      if (L >= n || L >= ntiles) return 0;
+    }
     pm = T;
     c0 = (L % gridDim.x) * TC;
     b0 = (L / gridDim.x) * ROWS;
-    return true;
+    return kind;
   }
 };
-// Batch: the work item `n` places later in the list.
+// Batch: the work item `n` places later in the list.  (Prefetching the
+// next stage's first items from the last blocks, as the single-solve
+// kernels do, measured no gain here.)
 template <int STAGE>
 struct ListAhead {
   const BatchSolve *solves;
   const BatchTile *tiles;
   int n;
-  __device__ __forceinline__ bool operator()(const StageMaps *&pm, int &c0, int &b0) const {
+  __device__ __forceinline__ int operator()(const StageMaps *&pm, int &c0, int &b0) const {
     const int L = blockIdx.x + n;
-    if (n <= 0 || L >= static_cast<int>(gridDim.x)) return false;
+    if (n <= 0 || L >= static_cast<int>(gridDim.x)) return 0;
     const BatchTile w = tiles[L];
     pm = &solves[w.solve].maps[STAGE - 1];
     c0 = w.c0;
     b0 = w.b0;
-    return true;
+    return 1;
   }
 };
 
