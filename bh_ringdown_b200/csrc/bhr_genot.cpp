@@ -425,6 +425,60 @@ int bhr_genot_bl(const bhr_genot_bl_params *p, const double *mino, int n_mino, i
   return BHR_OK;
 }
 
+int bhr_genot_ot_table(double T0, double dT, int rows, double T_start, double *X) {
+  if (!X || rows < 1 || !(dT > 0.0) || !(T_start < 0.0) || !(T_start <= T0))
+    return fail(BHR_INVALID_ARG, "bhr_genot_ot_table: need rows >= 1, dT > 0 and T_start <= T0, T_start < 0");
+  // X'' = -X^2 - T as (X, V); start on the asymptotic series
+  // X = u^(1/2) + u^(-2)/8 - (49/128) u^(-9/2), u = -T (order by order in u^(-5/2))
+  const double u = -T_start;
+  double y[2] = {std::sqrt(u) + 0.125 / (u * u) - 49.0 / 128.0 * std::pow(u, -4.5),
+                 -(0.5 / std::sqrt(u) - 0.25 / (u * u * u) + 49.0 / 128.0 * 4.5 * std::pow(u, -5.5))};
+  auto rk4 = [](double t, const double *y0, double h, double *y1) {
+    auto f = [](double tt, const double *yy, double *d) {
+      d[0] = yy[1];
+      d[1] = -yy[0] * yy[0] - tt;
+    };
+    double k1[2], k2[2], k3[2], k4[2], w[2];
+    f(t, y0, k1);
+    for (int i = 0; i < 2; i++) w[i] = y0[i] + 0.5 * h * k1[i];
+    f(t + 0.5 * h, w, k2);
+    for (int i = 0; i < 2; i++) w[i] = y0[i] + 0.5 * h * k2[i];
+    f(t + 0.5 * h, w, k3);
+    for (int i = 0; i < 2; i++) w[i] = y0[i] + h * k3[i];
+    f(t + h, w, k4);
+    for (int i = 0; i < 2; i++) y1[i] = y0[i] + h / 6.0 * (k1[i] + 2.0 * k2[i] + 2.0 * k3[i] + k4[i]);
+  };
+  // Adaptive classical RK4 with step doubling (a step against two half
+  // steps, their difference / 15 as the error, the Richardson-extrapolated
+  // result kept), landing exactly on each table point.
+  const double rtol = 1e-13, atol = 1e-13;
+  double t = T_start, h = 1e-3;
+  long long steps = 0;
+  for (int k = 0; k < rows; k++) {
+    const double target = T0 + dT * k;
+    while (t < target) {
+      if (++steps > 200000000LL) return fail(BHR_INVALID_ARG, "bhr_genot_ot_table: step limit (blow-up?)");
+      const double hh = std::min(h, target - t);
+      double y1[2], yh[2], y2[2];
+      rk4(t, y, hh, y1);
+      rk4(t, y, 0.5 * hh, yh);
+      rk4(t + 0.5 * hh, yh, 0.5 * hh, y2);
+      double err = 0.0;
+      for (int i = 0; i < 2; i++) err = std::max(err, std::fabs(y2[i] - y1[i]) / 15.0 / (atol + rtol * std::fabs(y2[i])));
+      if (!std::isfinite(err)) return fail(BHR_INVALID_ARG, "bhr_genot_ot_table: the solution is not finite there");
+      if (err <= 1.0) {
+        for (int i = 0; i < 2; i++) y[i] = y2[i] + (y2[i] - y1[i]) / 15.0;
+        t = (hh == target - t) ? target : t + hh;
+        h = hh * std::min(4.0, 0.9 * std::pow(std::max(err, 1e-10), -0.2));
+      } else {
+        h = hh * std::max(0.1, 0.9 * std::pow(err, -0.25));
+      }
+    }
+    X[k] = y[0];
+  }
+  return BHR_OK;
+}
+
 int bhr_genot_traj_name(double a, double thi0_deg, double thf_deg, int thdot_pos, char *buf, int buflen) {
   if (!buf || buflen < 1) return fail(BHR_INVALID_ARG, "bhr_genot_traj_name: no buffer");
   // a, theta_inc of the first row (truncated) with zeros to three digits,

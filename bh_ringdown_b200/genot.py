@@ -11,8 +11,9 @@ feeds them:
 
 * `ot_table` -- the universal Ori-Thorne function X(T), the solution of
   X'' = -X^2 - T that approaches sqrt(-T) as T -> -infinity, integrated
-  here from its asymptotic series (the reference ships it as a table,
-  GenOT/OT_X_vs_L.dat, on the same grid T = -40 + 0.001 k up to 3.41);
+  from its asymptotic series (`bhr_genot_ot_table`; the reference ships it
+  as a table, GenOT/OT_X_vs_L.dat, on the same grid T = -40 + 0.001 k up
+  to 3.41);
 * `synthetic_inspiral` -- a stand-in for the GREMLIN inspiral tables, which
   are not part of the reference tree: circular prograde Kerr orbits from
   r_start down to the ISCO (equatorial, or tilted as in Schwarzschild),
@@ -27,7 +28,7 @@ from __future__ import annotations
 import ctypes as C
 import functools
 import os
-from typing import Optional, Tuple
+from typing import Optional
 
 import numpy as np
 
@@ -57,6 +58,8 @@ def _lib():
                                  C.c_char_p]
     lib.bhr_genot_traj_name.restype = I
     lib.bhr_genot_traj_name.argtypes = [D, D, D, I, C.c_char_p, I]
+    lib.bhr_genot_ot_table.restype = I
+    lib.bhr_genot_ot_table.argtypes = [D, D, I, D, dp]
     lib._genot_sigs = True
     return lib
 
@@ -65,30 +68,18 @@ def _lib():
 OT_T0, OT_DT, OT_ROWS = -40.0, 0.001, 43411  # the reference table's grid: T = -40 .. 3.41
 
 
-def _ot_asymptotic(T: float) -> Tuple[float, float]:
-    """X and dX/dT from the series X = u^(1/2) + u^(-2)/8 - (49/128) u^(-9/2)
-    (u = -T), which solves X'' = -X^2 - T order by order in u^(-5/2)."""
-    u = -T
-    X = u ** 0.5 + u ** -2 / 8.0 - 49.0 / 128.0 * u ** -4.5
-    dXdu = 0.5 * u ** -0.5 - 0.25 * u ** -3 + 49.0 / 128.0 * 4.5 * u ** -5.5
-    return X, -dXdu
-
-
 @functools.lru_cache(maxsize=4)
 def ot_table(T0: float = OT_T0, dT: float = OT_DT, rows: int = OT_ROWS, T_start: float = -400.0) -> np.ndarray:
     """Rows (T, X(T)) of the Ori-Thorne function on T = T0 + k dT.
 
-    X'' = -X^2 - T is integrated from its asymptotic series at T_start with
-    the 8th-order Dormand-Prince method (rtol 1e-13); the result does not
-    change with T_start (checked from -40 to -4000).  Returned read-only."""
-    from scipy.integrate import solve_ivp
+    X'' = -X^2 - T is integrated from its asymptotic series at T_start
+    (bhr_genot_ot_table: adaptive classical RK4 with step doubling, relative
+    tolerance 1e-13); the result does not change with T_start.  Returned
+    read-only."""
     T = T0 + dT * np.arange(rows, dtype=np.float64)
-    X0, V0 = _ot_asymptotic(T_start)
-    sol = solve_ivp(lambda t, y: [y[1], -y[0] * y[0] - t], (T_start, float(T[-1])), [X0, V0], method="DOP853",
-                    rtol=1e-13, atol=1e-14, dense_output=True)
-    if not sol.success:
-        raise RuntimeError(f"Ori-Thorne integration failed: {sol.message}")
-    out = np.ascontiguousarray(np.column_stack([T, sol.sol(T)[0]]))
+    X = np.zeros(rows)
+    _check(_lib().bhr_genot_ot_table(T0, dT, rows, T_start, _ptr(X)))
+    out = np.ascontiguousarray(np.column_stack([T, X]))
     out.setflags(write=False)
     return out
 

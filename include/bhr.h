@@ -353,6 +353,12 @@ typedef struct bhr_genot_bl_params {
  * *n_out is set (the rows out would receive). */
 int bhr_genot_bl(const bhr_genot_bl_params *p, const double *mino, int n_mino, int stride, double *out, int max_rows,
                  int *n_out, double *thf_deg, int *thdot_pos, const char *path);
+/* The Ori-Thorne function on T = T0 + k dT, k < rows (X[k]): the solution
+ * of X'' = -X^2 - T that approaches sqrt(-T) as T -> -infinity, integrated
+ * from its asymptotic series at T_start (< 0, <= T0) by adaptive classical
+ * RK4 with step doubling (relative tolerance 1e-13).  Replaces the table
+ * GenOT ships (GenOT/OT_X_vs_L.dat, T0 = -40, dT = 0.001, 43411 rows). */
+int bhr_genot_ot_table(double T0, double dT, int rows, double T_start, double *X);
 /* The reference's .traj file name, a<a>_thi<theta_inc>_thf<theta_f>_<p|n>.traj
  * (GenOT/WL_BL.cc:101-153). */
 int bhr_genot_traj_name(double a, double thi0_deg, double thf_deg, int thdot_pos, char *buf, int buflen);

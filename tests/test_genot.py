@@ -53,6 +53,16 @@ def test_ot_table_solves_the_ori_thorne_equation_and_matches_the_reference_table
     assert abs(X[0] - (40.0 ** 0.5 + 1 / (8 * 1600.0))) < 1e-7
     other = genot.ot_table(T_start=-100.0)
     assert np.max(np.abs(other[T <= 2.5, 1] - X[T <= 2.5])) < 1e-9
+    # an independent integration (8th-order Dormand-Prince, scipy) of the same equation
+    from scipy.integrate import solve_ivp
+    u = 400.0
+    X0 = u ** 0.5 + u ** -2 / 8 - 49 / 128 * u ** -4.5
+    V0 = -(0.5 * u ** -0.5 - 0.25 * u ** -3 + 49 / 128 * 4.5 * u ** -5.5)
+    sol = solve_ivp(lambda t, y: [y[1], -y[0] ** 2 - t], (-u, T[-1]), [X0, V0], method="DOP853", rtol=1e-13,
+                    atol=1e-14, dense_output=True)
+    Xd = sol.sol(T)[0]
+    m = T <= 3.3
+    assert np.max(np.abs(Xd[m] - X[m]) / np.maximum(1.0, np.abs(X[m]))) < 1e-10
 
 
 @pytest.mark.parametrize("name", CASES)
