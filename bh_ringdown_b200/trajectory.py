@@ -1,14 +1,14 @@
-"""Trajectory files: the 10-column .traj format and a synthetic plunge.
+"""Trajectory files: the 10-column .traj format and a geodesic plunge.
 
 The reference takes its source worldline from GenOT
 (GenOT/README:113-123: columns t r theta dr/dt dtheta/dt dphi/dt phi E Lz
-Q).  GenOT's adiabatic inspiral inputs are not part of the reference tree,
-so workloads here use a stand-in: a prograde equatorial Kerr geodesic that
-starts just inside the ISCO with the ISCO energy and angular momentum and
-plunges; it is integrated in Boyer-Lindquist time with the 8th-order
-Dormand-Prince method (scipy's DOP853, dense output) and sampled on a
-uniform time grid (body.cu consumes two rows per step, so a run with step
-dt wants rows every dt/2).
+Q); bh_ringdown_b200.genot restates GenOT and makes the workloads'
+worldlines.  `synthetic_plunge` here is a simpler worldline for tests: a
+prograde equatorial Kerr geodesic that starts just inside the ISCO with the
+ISCO energy and angular momentum and plunges; it is integrated in
+Boyer-Lindquist time with the 8th-order Dormand-Prince method (scipy's
+DOP853, dense output) and sampled on a uniform time grid (body.cu consumes
+two rows per step, so a run with step dt wants rows every dt/2).
 """
 from __future__ import annotations
 
