@@ -124,23 +124,32 @@ class ClockSampler:
         except Exception:
             return pynvml.nvmlDeviceGetHandleByIndex(self.dev)
 
-    def __enter__(self):
-        import threading
+    def sample(self):
+        """One sample now (also called at fixed points of the timed region,
+        so a starved sampling thread still leaves a record)."""
+        if getattr(self, "h", None) is None:
+            return
         try:
             import pynvml
-            h = self._handle()
-            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            mhz = pynvml.nvmlDeviceGetClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            rs = pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+            self.samples.append((mhz, rs))
+        except Exception:
+            pass
+
+    def __enter__(self):
+        import threading
+        self.h = None
+        try:
+            import pynvml
+            self.h = self._handle()
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
             self.stop = threading.Event()
 
             def run():
                 while not self.stop.is_set():
-                    try:
-                        mhz = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
-                        rs = pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(h)
-                        self.samples.append((mhz, rs))
-                    except Exception:
-                        pass
-                    time.sleep(0.002)
+                    self.sample()
+                    time.sleep(0.001)
             self.thread = threading.Thread(target=run, daemon=True)
             self.thread.start()
         except Exception:
@@ -258,6 +267,7 @@ def run_ours(args, rank, local_rank, world):
             if resident:
                 flush_l2()
             solver.time_steps(1)
+            clk.sample()
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
@@ -266,8 +276,10 @@ def run_ours(args, rank, local_rank, world):
             for _ in range(args.steps):
                 flush_l2()
                 total_ms += solver.time_steps(1)
+                clk.sample()
         else:
             total_ms = solver.time_steps(args.steps)
+            clk.sample()
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
@@ -281,6 +293,7 @@ def run_ours(args, rank, local_rank, world):
                 flush_l2()
             avg, _tot = solver.profile(1)
             per_kernel += avg
+            clk.sample()
         torch.cuda.synchronize()
     clocks = clk.summary()
     solver.close()
