@@ -187,6 +187,34 @@ def test_engine_request_matches_oracle():
     assert np.linalg.norm(h - ho) <= 1e-10 * np.linalg.norm(ho)
 
 
+def test_genot_worldline_request_matches_the_oracle():
+    """A served plunge request with a GenOT transition-to-plunge worldline
+    (inclined, so theta moves), in a batch with a source-free request, is
+    bit-identical to the same request alone and matches the oracle."""
+    from bh_ringdown_b200 import genot
+    from tests.test_source import product_coef_fn
+    N, M, Xmin, Xmax, a = 256, 32, -50.0, 50.0, 0.3
+    dt = 0.25 * (Xmax - Xmin) / N
+    prm = bhr.Params(N=N, M=M, Xmin=Xmin, Xmax=Xmax, a=a, m=2.0, dt=dt, Fr=5, T=25.0, out_start=0.0,
+                     ext_col=N * 6 // 10)
+    rows = genot.transition_plunge(a, 1e-3, dt / 2.0, 30.0, inclination_deg=30.0, chi0_deg=40.0)
+    assert np.ptp(rows[:, 2]) > 0.05
+    alone = run_alone(prm, rows)
+    with bhr.Engine() as e:
+        rid = e.submit(prm, rows)
+        other = e.submit(gauss(512, 64, -50.0, 50.0, 0.9, -3.0, 25.0, center=3.0))
+        e.run_all()
+        t, h, d = e.result(rid)
+        assert e.poll(other)["state"] == bhr.Engine.DONE
+    assert np.array_equal(t, alone[0]) and np.array_equal(h, alone[1])
+    o = pyoracle.Oracle(N, M, Xmin, Xmax, a, 2.0, dt, T=prm.T, Fr=prm.Fr, out_start=0.0, ext_col=prm.ext_col)
+    with bhr.Solver(prm) as s:
+        nt = s.info()["nt"]
+    to, ho, _, _, _, _ = o.run(traj=rows, coef_fn=product_coef_fn(), nsteps=nt)
+    assert np.array_equal(t, to) and np.max(np.abs(ho)) > 0
+    assert np.linalg.norm(h - ho) <= 1e-10 * np.linalg.norm(ho)
+
+
 def test_budget_admits_one_at_a_time_when_tight():
     reqs = requests()[:2]
     alone = [run_alone(p, t) for p, t in reqs]
