@@ -98,6 +98,24 @@ def test_particle_inside_the_horizon_is_rejected():
 
 
 @pytest.mark.gpu
+def test_source_at_zero_spin_is_rejected():
+    """a = 0 exactly: the source's Kerr tortoise formula takes 0 ln(inf)
+    (HighOrder/kern.cu:1198-1199; the reference runs with aa = 1e-8), so the
+    trajectory is refused instead of depositing NaN; a = 1e-8 runs."""
+    from bh_ringdown_b200.trajectory import synthetic_plunge
+    rows = synthetic_plunge(1e-8, 0.025, duration=10.0)
+    with bhr.Solver(small_params(dt=0.05, T=10.0, a=0.0)) as s:
+        with pytest.raises(bhr.BhrError) as e:
+            s.set_trajectory(rows)
+        assert e.value.status == 1
+    with bhr.Solver(small_params(dt=0.05, T=10.0, a=1e-8)) as s:
+        s.set_trajectory(rows)
+        s.step(5)
+        t, h, _ = s.waveform()
+        assert np.all(np.isfinite(h))
+
+
+@pytest.mark.gpu
 def test_non_finite_state_is_detected_at_the_extraction():
     """A NaN planted in the state where the extraction column's closure reads
     it: the extraction flags BHR_NAN_DETECTED, which the step call that runs
