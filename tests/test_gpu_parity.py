@@ -281,3 +281,24 @@ def test_l2_prefetch_distance_does_not_change_results(tmp_path):
     for ahead in ("296", "100000"):
         assert np.array_equal(runs[ahead]["state"], runs["0"]["state"])
         assert np.array_equal(runs[ahead]["h"], runs["0"]["h"])
+
+
+@pytest.mark.parametrize("tiling", ["block8n", "block16", "block8"])
+@pytest.mark.parametrize("N,M,a,m", [(320, 48, 0.3, 1.0), (448, 80, 0.95, -2.0), (1088, 112, 0.6, 3.0)])
+def test_odd_tile_counts_with_a_source(tiling, N, M, a, m, monkeypatch):
+    """Grids whose tile counts are odd and not multiples of the SM count
+    (5, 7 or 17 column tiles, 3, 5 or 7 of 16 rows; a partial last wave,
+    the L2 prefetch reaching past the end and into the next stage's tiles),
+    with a plunge source crossing tile edges: each tiling against the
+    oracle."""
+    monkeypatch.setenv("BHR_STAGE_TILING", tiling)
+    s, o, rows, coef = traj_pair(N, M, -50.0, 50.0, a, m, ext_col=N * 6 // 10)
+    assert s.info()["tiling"] == tiling
+    n = 60
+    s.step(n)
+    t, h, _, _, _, _ = o.run(traj=rows, coef_fn=coef, nsteps=n)
+    ts, hs, _ = s.waveform()
+    assert np.array_equal(ts, t)
+    assert rel_field_err(s.get_state(), o.get_state()) <= FIELD_TOL
+    assert np.linalg.norm(hs - h) <= WAVE_TOL * np.linalg.norm(h)
+    s.close()
