@@ -1,7 +1,8 @@
 // bhr_device.cuh -- device helpers shared by the kernel translation units:
 // the reference's constants, PTX wrappers (mbarrier, TMA, bulk groups,
-// programmatic dependent launch), the 6th-order stencils and the
-// Newton-refined reciprocal and square root.
+// programmatic dependent launch), the 6th-order stencils, the
+// Newton-refined reciprocal and square root, and the work-item lookup of
+// batch launch groups.
 #pragma once
 
 #include <cuda.h>
@@ -9,6 +10,8 @@
 
 #include <cstdint>
 #include <utility>
+
+#include "bhr_internal.h"
 
 namespace bhr {
 namespace {
@@ -130,6 +133,24 @@ __device__ __forceinline__ double sqrt_nr(double x) {
 
 // 1/bir = 1/(B0 + B1 sin^2 theta) (HighOrder/kern.cu:132-149).
 __device__ __forceinline__ double inv_bir(double b0, double b1, double s2) { return rcp_nr(fma(b1, s2, b0)); }
+
+// Work item t of a launch group: the index of its solve in the group and
+// the tile corner (tiles of `rows` rows).  Every value read comes from the
+// kernel's parameter space and depends on t alone, so all of a block's
+// threads compute the same result.
+template <class Args>
+__device__ __forceinline__ int group_item(const WorkGroup<Args> &G, const int t, const int rows, int &c0, int &b0) {
+  int lo = 0, hi = G.nsolves - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (G.first[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  const int k = t - G.first[lo], nx = G.tiles_x[lo];
+  c0 = (k % nx) * TC;
+  b0 = (k / nx) * rows;
+  return lo;
+}
 
 // Launch with programmatic stream serialisation allowed (pdl): the kernel
 // may begin while its predecessor on the stream drains, and holds every

@@ -112,17 +112,18 @@ struct bhr_engine {
   std::mutex mu;
   std::vector<Running> active;
   BatchSolve *d_solves = nullptr;
-  BatchTile *d_tiles = nullptr;
   ExtractArgs *d_ext = nullptr;
   SourceArgs *d_src = nullptr;
   MixedBatch *d_mixed = nullptr;  // mixed-precision solves' stage 2/3 tables
-  int cap_solves = 0, cap_tiles = 0, ntiles = 0, nsrc = 0, max_ptsx = 1, max_ptsy = 1;
-  // The work-list: FP64 solves' tiles (ntiles64), then mixed solves' tiles
-  // of the same height for their FP64 stage 1 (up to ntiles1), then mixed
-  // solves' kMixTileRows-high tiles for the FP32 stages 2 and 3 (nmix).
-  int ntiles64 = 0, ntiles1 = 0, nmix = 0;
+  int cap_solves = 0, ntiles = 0, nsrc = 0, max_ptsx = 1, max_ptsy = 1;
+  // The work-lists, as launch groups: for FP64 stage s, groups64[s - 1]
+  // (stage 1: every solve, FP64 solves first; stages 2 and 3: the FP64
+  // solves); for the FP32 stages 2 and 3 of mixed solves, mixgroups[s - 2]
+  // (kMixTileRows-high tiles).  ntiles counts every stage's tiles.
+  std::vector<BatchGroup> groups64[3];
+  std::vector<MixedGroup> mixgroups[2];
   int *d_err = nullptr;     // BHR_TIMEOUT from a bounded wait in a stage kernel
-  cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph = nullptr;  // one batch step
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool dirty = true;
   long long batch_steps = 0;
@@ -140,15 +141,14 @@ int set_fail(int status, const std::string &msg) {
 void release_tables(bhr_engine *e) {
   if (e->graph) cudaGraphExecDestroy(e->graph);
   e->graph = nullptr;
-  for (void *q : {static_cast<void *>(e->d_solves), static_cast<void *>(e->d_tiles), static_cast<void *>(e->d_ext),
-                  static_cast<void *>(e->d_src), static_cast<void *>(e->d_mixed)})
+  for (void *q : {static_cast<void *>(e->d_solves), static_cast<void *>(e->d_ext), static_cast<void *>(e->d_src),
+                  static_cast<void *>(e->d_mixed)})
     if (q) cudaFreeAsync(q, e->stream);
   e->d_solves = nullptr;
-  e->d_tiles = nullptr;
   e->d_ext = nullptr;
   e->d_src = nullptr;
   e->d_mixed = nullptr;
-  e->cap_solves = e->cap_tiles = 0;
+  e->cap_solves = 0;
 }
 
 // One batch step: sources of the sourced solves, three stages over the
@@ -163,10 +163,12 @@ int enqueue_batch_step(bhr_engine *e) {
   // tiles through the FP64 kernels and mixed solves' tiles through the
   // FP32 ones.
   for (int stage = 1; stage <= 3; stage++) {
-    const int n64 = stage == 1 ? e->ntiles1 : e->ntiles64;
-    cudaError_t err = launch_stage_batch(stage, e->tiling, e->d_solves, e->d_tiles, n64, e->d_err, e->stream);
-    if (err == cudaSuccess && stage > 1 && e->nmix > 0)
-      err = launch_mixed_batch(stage, e->d_mixed, e->d_tiles + e->ntiles1, e->nmix, e->stream);
+    cudaError_t err = cudaSuccess;
+    for (const BatchGroup &g : e->groups64[stage - 1])
+      if (err == cudaSuccess) err = launch_stage_batch(stage, e->tiling, e->d_solves, g, e->d_err, e->stream);
+    if (stage > 1)
+      for (const MixedGroup &g : e->mixgroups[stage - 2])
+        if (err == cudaSuccess) err = launch_mixed_batch(stage, e->d_mixed, g, e->stream);
     if (err != cudaSuccess) return set_fail(BHR_CUDA_ERROR, std::string("stage batch: ") + cudaGetErrorString(err));
   }
   cudaError_t err = launch_extract_batch(e->d_ext, n, e->stream);
@@ -184,14 +186,16 @@ int rebuild(bhr_engine *e) {
   }
   e->dirty = false;
   if (n == 0) {
-    e->ntiles = e->ntiles64 = e->ntiles1 = e->nmix = 0;
+    e->ntiles = 0;
+    for (auto &g : e->groups64) g.clear();
+    for (auto &g : e->mixgroups) g.clear();
     return BHR_OK;
   }
   std::vector<BatchSolve> solves(n);
-  std::vector<BatchTile> tiles, m1tiles, mtiles;
   std::vector<ExtractArgs> ext(n);
   std::vector<SourceArgs> src;
   std::vector<MixedBatch> mixed;
+  std::vector<int> fp64, mix, mix_index(n, -1);
   e->max_ptsx = 1;
   e->max_ptsy = 1;
   for (int i = 0; i < n; i++) {
@@ -205,7 +209,6 @@ int rebuild(bhr_engine *e) {
       B.args[k].un = s->u0;
       B.args[k].out = out[k];
     }
-    int mix_index = 0;
     if (s->mixed) {
       B.args[0].dout = s->d1f;
       MixedBatch X{};
@@ -214,15 +217,12 @@ int rebuild(bhr_engine *e) {
       X.args[0] = X.args[1] = solver_mixed_args(s);
       X.args[0].e_out = s->e2f;
       X.args[1].u_out = s->u0;
-      mix_index = static_cast<int>(mixed.size());
+      mix_index[i] = static_cast<int>(mixed.size());
       mixed.push_back(X);
+      mix.push_back(i);
+    } else {
+      fp64.push_back(i);
     }
-    std::vector<BatchTile> &dst = s->mixed ? m1tiles : tiles;
-    for (int b0 = 0; b0 < s->p.M; b0 += e->rows)
-      for (int c0 = 0; c0 < s->p.N; c0 += TC) dst.push_back({i, c0, b0, mix_index});
-    if (s->mixed)
-      for (int b0 = 0; b0 < s->p.M; b0 += kMixTileRows)
-        for (int c0 = 0; c0 < s->p.N; c0 += TC) mtiles.push_back({i, c0, b0, mix_index});
     ext[i] = solver_extract_args(s);
     ext[i].set_ks = 1;  // stages and extraction run in sequence here
     if (s->has_source) {
@@ -231,16 +231,45 @@ int rebuild(bhr_engine *e) {
       e->max_ptsy = std::max(e->max_ptsy, s->p.PTSY);
     }
   }
-  // Blocks are ordered solve by solve, row block by row block, FP64 solves
-  // first.
-  e->ntiles64 = static_cast<int>(tiles.size());
-  tiles.insert(tiles.end(), m1tiles.begin(), m1tiles.end());
-  e->ntiles1 = static_cast<int>(tiles.size());
-  tiles.insert(tiles.end(), mtiles.begin(), mtiles.end());
-  e->nmix = static_cast<int>(mtiles.size());
-  e->ntiles = static_cast<int>(tiles.size());
+  // The launch groups: blocks are ordered solve by solve, row band by row
+  // band; stage 1 takes the FP64 solves, then the mixed ones.
+  auto add = [](auto &groups, int row, int N, int M, int rows, const auto &args) {
+    if (groups.empty() || groups.back().nsolves == kGroupSolves) {
+      groups.emplace_back();
+      std::memset(&groups.back(), 0, sizeof(groups.back()));
+    }
+    auto &g = groups.back();
+    const int j = g.nsolves++;
+    g.first[j] = g.ntiles;
+    g.tiles_x[j] = N / TC;
+    g.solve[j] = row;
+    g.args[j] = args;
+    g.ntiles += (N / TC) * (M / rows);
+    g.first[j + 1] = g.ntiles;
+  };
+  std::vector<int> order1 = fp64;
+  order1.insert(order1.end(), mix.begin(), mix.end());
+  e->ntiles = 0;
+  for (int stage = 1; stage <= 3; stage++) {
+    std::vector<BatchGroup> &G = e->groups64[stage - 1];
+    G.clear();
+    for (int i : stage == 1 ? order1 : fp64) {
+      const bhr_params &p = e->active[i].s->p;
+      add(G, i, p.N, p.M, e->rows, solves[i].args[stage - 1]);
+      if (stage == 1) e->ntiles += (p.N / TC) * (p.M / e->rows);
+    }
+  }
+  for (int stage = 2; stage <= 3; stage++) {
+    std::vector<MixedGroup> &G = e->mixgroups[stage - 2];
+    G.clear();
+    for (int i : mix) {
+      const bhr_params &p = e->active[i].s->p;
+      add(G, mix_index[i], p.N, p.M, kMixTileRows, mixed[mix_index[i]].args[stage - 2]);
+      if (stage == 2) e->ntiles += (p.N / TC) * (p.M / kMixTileRows);
+    }
+  }
   e->nsrc = static_cast<int>(src.size());
-  // The per-solve tables share one capacity; the work-list has its own.
+  // The per-solve tables share one capacity.
   cudaError_t err = cudaSuccess;
   if (n > e->cap_solves) {
     const int c = std::max(n, 2 * e->cap_solves);
@@ -259,18 +288,7 @@ int rebuild(bhr_engine *e) {
       return set_fail(BHR_OUT_OF_MEMORY, std::string("engine tables: ") + cudaGetErrorString(err));
     e->cap_solves = c;
   }
-  if (e->ntiles > e->cap_tiles) {
-    const int c = std::max(e->ntiles, 2 * e->cap_tiles);
-    if (e->d_tiles) cudaFreeAsync(e->d_tiles, e->stream);
-    e->d_tiles = nullptr;
-    e->cap_tiles = 0;
-    if ((err = cudaMallocAsync(&e->d_tiles, sizeof(BatchTile) * c, e->stream)))
-      return set_fail(BHR_OUT_OF_MEMORY, std::string("engine work-list: ") + cudaGetErrorString(err));
-    e->cap_tiles = c;
-  }
   if ((err = cudaMemcpyAsync(e->d_solves, solves.data(), sizeof(BatchSolve) * n, cudaMemcpyHostToDevice, e->stream)) ||
-      (err = cudaMemcpyAsync(e->d_tiles, tiles.data(), sizeof(BatchTile) * tiles.size(), cudaMemcpyHostToDevice,
-                             e->stream)) ||
       (err = cudaMemcpyAsync(e->d_ext, ext.data(), sizeof(ExtractArgs) * n, cudaMemcpyHostToDevice, e->stream)) ||
       (e->nsrc > 0 && (err = cudaMemcpyAsync(e->d_src, src.data(), sizeof(SourceArgs) * e->nsrc,
                                              cudaMemcpyHostToDevice, e->stream))) ||

@@ -127,6 +127,25 @@ struct StageMaps {
   CUtensorMap o;  // stage output planes, box {TC, rows, 4} (TMA stores)
 };
 
+// One launch's share of a batch work-list: up to kGroupSolves solves whose
+// tiles follow one another in launch order, each solve's row band by row
+// band (TC columns by the kernel's tile height).  The stage arguments travel
+// in the kernel's parameter space, where the stage kernels read them as
+// they read a lone solve's (constant-bank operands, no loads from global
+// memory in the row loops); each block finds its solve by a binary search
+// over `first`.  The tensor maps stay in the batch's solve table.
+constexpr int kGroupSolves = 112;
+template <class Args>
+struct WorkGroup {
+  int nsolves, ntiles;
+  int first[kGroupSolves + 1];  // each solve's first work item; first[nsolves] = ntiles
+  int tiles_x[kGroupSolves];    // TC-column tiles per row band (N / TC)
+  int solve[kGroupSolves];      // the solve's row in the batch's solve table
+  Args args[kGroupSolves];
+};
+using BatchGroup = WorkGroup<StageArgs>;
+static_assert(sizeof(BatchGroup) + 64 <= 32764, "a kernel's parameters are limited to 32764 bytes");
+
 // Fused stages 1 and 2 over column strips (tiling kTilingStrip12): the state
 // and bb planes read in 136-column x 4-row boxes.
 struct StripMaps {
@@ -168,12 +187,13 @@ struct MixedBatch {
   MixedMaps maps[2];    // stages 2 and 3
   MixedArgs args[2];
 };
+using MixedGroup = WorkGroup<MixedArgs>;
+static_assert(sizeof(MixedGroup) + 64 <= 32764, "a kernel's parameters are limited to 32764 bytes");
 cudaError_t encode_mixed_maps(const float *in, const float *bbf, const float *colf, const float *rowf,
                               const double *u1, int N, int M, MixedMaps *maps);
 cudaError_t launch_mixed_stage(int stage, const MixedMaps &maps, const MixedArgs &a, cudaStream_t st);
-struct BatchTile;
-cudaError_t launch_mixed_batch(int stage, const MixedBatch *solves, const BatchTile *tiles, int ntiles,
-                               cudaStream_t st);
+// One launch of a mixed stage over a group of mixed solves (16-row tiles).
+cudaError_t launch_mixed_batch(int stage, const MixedBatch *solves, const MixedGroup &g, cudaStream_t st);
 cudaError_t launch_to_float(const double *src, float *dst, size_t n, cudaStream_t st);
 // kc[4][M][N] (FP32): bb, ee, d_re, d_im formed in FP64 from the tables.
 cudaError_t launch_mixed_coef(const double *coltab, const double *rowtab, const double *bbt, float *kc, int N, int M,
@@ -181,13 +201,11 @@ cudaError_t launch_mixed_coef(const double *coltab, const double *rowtab, const 
 cudaError_t prepare_mixed_kernels();
 
 // A batch of solves advanced together: per solve, the tensor maps and
-// arguments of its three stages; per block, one (solve, tile) work item.
+// arguments of its three stages (the arguments are copied into the launch
+// groups).
 struct BatchSolve {
   StageMaps maps[3];
   StageArgs args[3];
-};
-struct BatchTile {
-  int solve, c0, b0, pad;
 };
 
 // Tensor maps of one state (four M x N planes): q planes with the +-3 row
@@ -224,8 +242,10 @@ constexpr int tiling_rows(int tiling) {
 }
 // Tile height of the mixed-precision FP32 stage kernels.
 constexpr int kMixTileRows = 16;
-cudaError_t launch_stage_batch(int stage, int tiling, const BatchSolve *solves, const BatchTile *tiles,
-                               int ntiles, int *err, cudaStream_t st);
+// One launch of an FP64 stage over a group of a batch's solves (tiles of the
+// tiling's height).
+cudaError_t launch_stage_batch(int stage, int tiling, const BatchSolve *solves, const BatchGroup &g, int *err,
+                               cudaStream_t st);
 cudaError_t launch_source_batch(const SourceArgs *args, int nsolves, int max_ptsy, int max_ptsx, cudaStream_t st);
 cudaError_t launch_extract_batch(const ExtractArgs *args, int nsolves, cudaStream_t st);
 cudaError_t launch_extract(const ExtractArgs &a, cudaStream_t st);

@@ -557,21 +557,18 @@ struct GridAhead {
     return kind;
   }
 };
-// Batch: the work item `n` places later in the list.  (Prefetching the
+// Batch: the work item `n` places later in the group.  (Prefetching the
 // next stage's first items from the last blocks, as the single-solve
 // kernels do, measured no gain here.)
-template <int STAGE>
-struct ListAhead {
+template <int STAGE, int ROWS>
+struct GroupAhead {
   const BatchSolve *solves;
-  const BatchTile *tiles;
+  const BatchGroup *G;
   int n;
   __device__ __forceinline__ int operator()(const StageMaps *&pm, int &c0, int &b0) const {
     const int L = blockIdx.x + n;
-    if (n <= 0 || L >= static_cast<int>(gridDim.x)) return 0;
-    const BatchTile w = tiles[L];
-    pm = &solves[w.solve].maps[STAGE - 1];
-    c0 = w.c0;
-    b0 = w.b0;
+    if (n <= 0 || L >= G->ntiles) return 0;
+    pm = &solves[G->solve[group_item(*G, L, ROWS, c0, b0)]].maps[STAGE - 1];
     return 1;
   }
 };
@@ -591,14 +588,15 @@ __global__ void __launch_bounds__(kNarrowThreads, 4)
   stage_tile<STAGE, 8, kNarrowThreads>(T, A, blockIdx.x * TC, blockIdx.y * 8, GridAhead<8>{&T, A.ahead});
 }
 
-// Several solves advanced together: block -> (solve, tile) from the work-list.
+// Several solves advanced together: block -> (solve, tile), work item
+// blockIdx.x of the launch group.
 template <int STAGE, int ROWS>
 __global__ void __launch_bounds__(STAGE_THREADS, 2)
-    stage_batch_kernel(const BatchSolve *solves, const BatchTile *tiles, int ahead) {
-  const BatchTile t = tiles[blockIdx.x];
-  const BatchSolve &B = solves[t.solve];
-  stage_tile<STAGE, ROWS, STAGE_THREADS>(B.maps[STAGE - 1], B.args[STAGE - 1], t.c0, t.b0,
-                                        ListAhead<STAGE>{solves, tiles, ahead});
+    stage_batch_kernel(const BatchSolve *solves, const __grid_constant__ BatchGroup G, int ahead) {
+  int c0, b0;
+  const int i = group_item(G, blockIdx.x, ROWS, c0, b0);
+  stage_tile<STAGE, ROWS, STAGE_THREADS>(solves[G.solve[i]].maps[STAGE - 1], G.args[i], c0, b0,
+                                        GroupAhead<STAGE, ROWS>{solves, &G, ahead});
 }
 
 // ---- persistent stage kernels -------------------------------------------
@@ -634,18 +632,16 @@ struct SingleWork {
     b0 = (t / tiles_x) * rows;
   }
 };
-template <int STAGE>
-struct BatchWork {
+// Batch: work item t of the launch group.
+template <int STAGE, int ROWS>
+struct GroupWork {
   const BatchSolve *solves;
-  const BatchTile *tiles;
-  int ntiles;
-  __device__ __forceinline__ int count() const { return ntiles; }
+  const BatchGroup *G;
+  __device__ __forceinline__ int count() const { return G->ntiles; }
   __device__ __forceinline__ void get(int t, const StageMaps *&tm, const StageArgs *&ta, int &c0, int &b0) const {
-    const BatchTile w = tiles[t];
-    tm = &solves[w.solve].maps[STAGE - 1];
-    ta = &solves[w.solve].args[STAGE - 1];
-    c0 = w.c0;
-    b0 = w.b0;
+    const int i = group_item(*G, t, ROWS, c0, b0);
+    tm = &solves[G->solve[i]].maps[STAGE - 1];
+    ta = &G->args[i];
   }
 };
 
@@ -781,26 +777,26 @@ __global__ void __launch_bounds__(kRingThreads, kRingBlocksPerSM)
 
 template <int STAGE>
 __global__ void __launch_bounds__(kPersistThreads, 1)
-    stage_persistent_batch_kernel(const BatchSolve *solves, const BatchTile *tiles, int ntiles, int *err) {
-  BatchWork<STAGE> W{solves, tiles, ntiles};
+    stage_persistent_batch_kernel(const BatchSolve *solves, const __grid_constant__ BatchGroup G, int *err) {
+  GroupWork<STAGE, kPersistRows> W{solves, &G};
   stage_persistent<STAGE, kPersistRows, kPersistThreads, 2, true>(W, err);
 }
 
 // The 8-row tilings over a batch work-list (tiles of 8 rows).
 template <int STAGE>
 __global__ void __launch_bounds__(kRingThreads, kRingBlocksPerSM)
-    stage_ring_batch_kernel(const BatchSolve *solves, const BatchTile *tiles, int ntiles, int *err) {
-  BatchWork<STAGE> W{solves, tiles, ntiles};
+    stage_ring_batch_kernel(const BatchSolve *solves, const __grid_constant__ BatchGroup G, int *err) {
+  GroupWork<STAGE, kRingRows> W{solves, &G};
   stage_persistent<STAGE, kRingRows, kRingThreads, kRingBufs, false>(W, err);
 }
 
 template <int STAGE>
 __global__ void __launch_bounds__(kNarrowThreads, 4)
-    stage_narrow_batch_kernel(const BatchSolve *solves, const BatchTile *tiles, int ahead) {
-  const BatchTile t = tiles[blockIdx.x];
-  const BatchSolve &B = solves[t.solve];
-  stage_tile<STAGE, 8, kNarrowThreads>(B.maps[STAGE - 1], B.args[STAGE - 1], t.c0, t.b0,
-                                       ListAhead<STAGE>{solves, tiles, ahead});
+    stage_narrow_batch_kernel(const BatchSolve *solves, const __grid_constant__ BatchGroup G, int ahead) {
+  int c0, b0;
+  const int i = group_item(G, blockIdx.x, 8, c0, b0);
+  stage_tile<STAGE, 8, kNarrowThreads>(solves[G.solve[i]].maps[STAGE - 1], G.args[i], c0, b0,
+                                       GroupAhead<STAGE, 8>{solves, &G, ahead});
 }
 
 // ---- stages 1 and 2 fused over column strips (the strip12 tiling) --------
@@ -1564,8 +1560,9 @@ cudaError_t prepare_kernels() {
   return cudaSuccess;
 }
 
-cudaError_t launch_stage_batch(int stage, int tiling, const BatchSolve *solves, const BatchTile *tiles, int ntiles,
-                               int *err, cudaStream_t st) {
+cudaError_t launch_stage_batch(int stage, int tiling, const BatchSolve *solves, const BatchGroup &g, int *err,
+                               cudaStream_t st) {
+  const int ntiles = g.ntiles;
   if (ntiles <= 0) return cudaSuccess;
   if (stage < 1 || stage > 3) return cudaErrorInvalidValue;
   return by_stage(stage, [&](auto sc) {
@@ -1573,19 +1570,19 @@ cudaError_t launch_stage_batch(int stage, int tiling, const BatchSolve *solves, 
     switch (tiling) {
       case kTilingPersistent:
         return launch_pdl(stage_persistent_batch_kernel<S>, dim3(std::min(ntiles, sm_count())),
-                          dim3(32, kPersistThreads / 32), persist_smem_bytes(), st, solves, tiles, ntiles, err);
+                          dim3(32, kPersistThreads / 32), persist_smem_bytes(), st, solves, g, err);
       case kTilingRing:
         return launch_pdl(stage_ring_batch_kernel<S>, dim3(std::min(ntiles, kRingBlocksPerSM * sm_count())),
-                          dim3(32, kRingThreads / 32), ring_smem_bytes(), st, solves, tiles, ntiles, err);
+                          dim3(32, kRingThreads / 32), ring_smem_bytes(), st, solves, g, err);
       case kTilingBlock8n:
         return launch_pdl(stage_narrow_batch_kernel<S>, dim3(ntiles), dim3(32, kNarrowThreads / 32),
-                          sizeof(StageSmem<8>) + 128, st, solves, tiles, stage_prefetch_ahead());
+                          sizeof(StageSmem<8>) + 128, st, solves, g, stage_prefetch_ahead());
       case kTilingBlock8:
         return launch_pdl(stage_batch_kernel<S, 8>, dim3(ntiles), dim3(32, STAGE_THREADS / 32),
-                          sizeof(StageSmem<8>) + 128, st, solves, tiles, stage_prefetch_ahead());
+                          sizeof(StageSmem<8>) + 128, st, solves, g, stage_prefetch_ahead());
       default:
         return launch_pdl(stage_batch_kernel<S, 16>, dim3(ntiles), dim3(32, STAGE_THREADS / 32),
-                          sizeof(StageSmem<16>) + 128, st, solves, tiles, stage_prefetch_ahead());
+                          sizeof(StageSmem<16>) + 128, st, solves, g, stage_prefetch_ahead());
     }
   });
 }

@@ -75,23 +75,19 @@ struct MixGridAhead {
     return true;
   }
 };
-// Batch: the work item `n` places later in the list.
+// Batch: the work item `n` places later in the launch group.
 template <int STAGE>
-struct MixListAhead {
+struct MixGroupAhead {
   const MixedBatch *solves;
-  const BatchTile *tiles;
+  const MixedGroup *G;
   int n;
   __device__ __forceinline__ bool operator()(const MixedMaps *&pm, int &c0, int &b0) const {
     const int L = blockIdx.x + n;
-    if (n <= 0 || L >= static_cast<int>(gridDim.x)) return false;
-    const BatchTile w = tiles[L];
-    pm = &solves[w.pad].maps[STAGE - 2];
-    c0 = w.c0;
-    b0 = w.b0;
+    if (n <= 0 || L >= G->ntiles) return false;
+    pm = &solves[G->solve[group_item(*G, L, kMixRows, c0, b0)]].maps[STAGE - 2];
     return true;
   }
 };
-
 // One 64 x 16 tile (columns c0.., rows b0..) of stage 2 or 3.  Thread 0
 // prefetches into L2 the input of the later tile `ahead` names, so that the
 // block which takes it finds its loads there.
@@ -336,14 +332,15 @@ __global__ void __launch_bounds__(kMixThreads, 3)
   mixed_tile<STAGE>(T, A, blockIdx.x * TC, blockIdx.y * kMixRows, MixGridAhead{&T, ahead});
 }
 
-// Mixed-precision solves of a batch: block -> (solve, tile); the tile's pad
-// field indexes the MixedBatch array.
+// Mixed-precision solves of a batch: block -> (solve, tile), work item
+// blockIdx.x of the launch group (its `solve` entries index the MixedBatch
+// array).
 template <int STAGE>
 __global__ void __launch_bounds__(kMixThreads, 3)
-    mixed_batch_kernel(const MixedBatch *solves, const BatchTile *tiles, int ahead) {
-  const BatchTile t = tiles[blockIdx.x];
-  const MixedBatch &B = solves[t.pad];
-  mixed_tile<STAGE>(B.maps[STAGE - 2], B.args[STAGE - 2], t.c0, t.b0, MixListAhead<STAGE>{solves, tiles, ahead});
+    mixed_batch_kernel(const MixedBatch *solves, const __grid_constant__ MixedGroup G, int ahead) {
+  int c0, b0;
+  const int i = group_item(G, blockIdx.x, kMixRows, c0, b0);
+  mixed_tile<STAGE>(solves[G.solve[i]].maps[STAGE - 2], G.args[i], c0, b0, MixGroupAhead<STAGE>{solves, &G, ahead});
 }
 
 // bb, ee = Ataurho + bb, d_re = (Brho_re - bb Btau_re) - bb' ee and
@@ -448,13 +445,12 @@ cudaError_t launch_mixed_stage(int stage, const MixedMaps &maps, const MixedArgs
   return launch_pdl(mixed_stage_kernel<3>, grid, block, mix_smem_bytes<3>(), st, maps, a, ahead);
 }
 
-cudaError_t launch_mixed_batch(int stage, const MixedBatch *solves, const BatchTile *tiles, int ntiles,
-                               cudaStream_t st) {
-  if (ntiles <= 0) return cudaSuccess;
-  const dim3 grid(ntiles), block(32, kMixThreads / 32);
+cudaError_t launch_mixed_batch(int stage, const MixedBatch *solves, const MixedGroup &g, cudaStream_t st) {
+  if (g.ntiles <= 0) return cudaSuccess;
+  const dim3 grid(g.ntiles), block(32, kMixThreads / 32);
   const int ahead = stage_prefetch_ahead();
-  if (stage == 2) return launch_pdl(mixed_batch_kernel<2>, grid, block, mix_smem_bytes<2>(), st, solves, tiles, ahead);
-  return launch_pdl(mixed_batch_kernel<3>, grid, block, mix_smem_bytes<3>(), st, solves, tiles, ahead);
+  if (stage == 2) return launch_pdl(mixed_batch_kernel<2>, grid, block, mix_smem_bytes<2>(), st, solves, g, ahead);
+  return launch_pdl(mixed_batch_kernel<3>, grid, block, mix_smem_bytes<3>(), st, solves, g, ahead);
 }
 
 cudaError_t launch_mixed_coef(const double *coltab, const double *rowtab, const double *bbt, float *kc, int N, int M,
