@@ -4,11 +4,13 @@
 // m modes; TD_GPU_code/run.sh submits one job per trajectory).  The engine
 // keeps every admitted solve's fields and tables resident, admits queued
 // requests while the HBM budget allows, and advances all running solves with
-// one launch per RK stage over a work-list of (solve, tile) pairs, captured
-// as a CUDA graph.  Requests arriving while others run join at the next
-// step boundary (continuous batching); finished solves leave with their
-// waveform.  Each tile is computed by the same code as a lone solve, so a
-// request's result does not depend on what it shares the GPU with.
+// one launch per RK stage over a work-list of (solve, tile) pairs (one
+// launch per group of up to kGroupSolves solves, whose stage arguments
+// travel in the launch's parameters), captured as a CUDA graph.  Requests
+// arriving while others run join at the next step boundary (continuous
+// batching); finished solves leave with their waveform.  Each tile is
+// computed by the same code as a lone solve, so a request's result does not
+// depend on what it shares the GPU with.
 //
 // Host work per request (grid, tables, initial data, trajectory records,
 // device allocations; waveform readback and release at the end) runs on a

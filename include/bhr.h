@@ -259,8 +259,9 @@ int bhr_step_noalloc(const bhr_params *p, double *state, int nsteps, void *strea
  * engine queues requests, admits them in arrival order while their device
  * memory fits `hbm_budget_bytes` (one is always admitted when none runs;
  * while the oldest does not fit, later ones that do are admitted ahead of
- * it, at most 64 of them), and advances every running solve with one launch per RK stage over a
- * (solve, tile) work-list.  Requests submitted while others run join at the
+ * it, at most 64 of them), and advances every running solve with one
+ * launch per RK stage (per group of up to 112 solves) over a (solve, tile)
+ * work-list.  Requests submitted while others run join at the
  * next bhr_engine_step (continuous batching).  A request's waveform does
  * not depend on the other requests in the batch: it is bit-identical to the
  * same request run alone in an engine, and matches bhr_solver_step's to

@@ -1,5 +1,5 @@
 """Batch engine (bhr_engine_*): many solves advanced by one launch per RK
-stage over a (solve, tile) work-list.
+stage (per group of up to 112 solves) over a (solve, tile) work-list.
 
 A request's waveform must not depend on what it shares the GPU with: the
 same request run alone in an engine and in a mixed batch (other grids,
