@@ -26,6 +26,12 @@ namespace {
 
 constexpr int kMixRows = kMixTileRows;
 constexpr int kMixThreads = 256;
+// Blocks per SM: stage 2 fits in 64 registers a thread and ~50 KB of shared
+// memory, so four; stage 3 (80 registers, its FP64 u1 tile: ~74 KB) three.
+template <int STAGE>
+constexpr int mix_blocks_per_sm() {
+  return STAGE == 2 ? 4 : 3;
+}
 
 // Every TMA destination starts on a 128-byte boundary.
 template <int STAGE>
@@ -327,7 +333,7 @@ __device__ __forceinline__ void mixed_tile(const MixedMaps &T, const MixedArgs &
 }
 
 template <int STAGE>
-__global__ void __launch_bounds__(kMixThreads, 3)
+__global__ void __launch_bounds__(kMixThreads, mix_blocks_per_sm<STAGE>())
     mixed_stage_kernel(const __grid_constant__ MixedMaps T, const MixedArgs A, int ahead) {
   mixed_tile<STAGE>(T, A, blockIdx.x * TC, blockIdx.y * kMixRows, MixGridAhead{&T, ahead});
 }
@@ -336,7 +342,7 @@ __global__ void __launch_bounds__(kMixThreads, 3)
 // blockIdx.x of the launch group (its `solve` entries index the MixedBatch
 // array).
 template <int STAGE>
-__global__ void __launch_bounds__(kMixThreads, 3)
+__global__ void __launch_bounds__(kMixThreads, mix_blocks_per_sm<STAGE>())
     mixed_batch_kernel(const MixedBatch *solves, const __grid_constant__ MixedGroup G, int ahead) {
   int c0, b0;
   const int i = group_item(G, blockIdx.x, kMixRows, c0, b0);
