@@ -117,29 +117,36 @@ def test_more_solves_than_one_launch_group(tiling, monkeypatch):
     in its parameters, so every stage runs as several launch groups (stage 1:
     three; FP64 stages 2 and 3: two; the FP32 stages of the mixed requests:
     two).  Four kinds of request (grids, spins, m, FP64 and mixed precision)
-    alternate, so a block that took a neighbouring solve's arguments would
-    change a result: each must be bit-identical to its kind run alone."""
+    alternate, and every 29th request is a sourced plunge (its source patch
+    and step records are arguments too), so a block that took a neighbouring
+    solve's arguments would change a result: each must be bit-identical to
+    its kind run alone."""
     monkeypatch.setenv("BHR_ENGINE_TILING", tiling)
-    kinds = [gauss(128, 16, -40.0, 40.0, 0.0, 1.0, 6.0), gauss(192, 32, -40.0, 40.0, 0.5, 2.0, 6.0, center=4.0),
-             gauss(128, 16, -40.0, 40.0, 0.3, -2.0, 6.0), gauss(192, 32, -40.0, 40.0, 0.8, 3.0, 6.0, center=4.0)]
-    kinds[2].precision = bhr.BHR_MIXED
-    kinds[3].precision = bhr.BHR_MIXED
-    alone = [run_alone(p, None) for p in kinds]
+    kinds = [(gauss(128, 16, -40.0, 40.0, 0.0, 1.0, 6.0), None),
+             (gauss(192, 32, -40.0, 40.0, 0.5, 2.0, 6.0, center=4.0), None),
+             (gauss(128, 16, -40.0, 40.0, 0.3, -2.0, 6.0), None),
+             (gauss(192, 32, -40.0, 40.0, 0.8, 3.0, 6.0, center=4.0), None),
+             plunge(256, 32, -50.0, 50.0, 0.6, 2.0, 8.0)]
+    kinds[2][0].precision = bhr.BHR_MIXED
+    kinds[3][0].precision = bhr.BHR_MIXED
+    alone = [run_alone(p, t) for p, t in kinds]
     for (_, h0, _), (_, h1, _) in zip(alone, alone[1:]):
         assert not np.array_equal(h0, h1)
     n = 232
+    kind = [4 if i % 29 == 7 else i % 4 for i in range(n)]
+    # stage-1 tiles (8 rows) of every solve plus the mixed solves' 16-row FP32 tiles
+    tiles = {0: 2 * 2, 1: 3 * 4, 2: 2 * 2 + 2 * 1, 3: 3 * 4 + 3 * 2, 4: 4 * 4}
     with bhr.Engine() as e:
-        ids = [e.submit(kinds[i % 4], None) for i in range(n)]
+        ids = [e.submit(*kinds[k]) for k in kind]
         while e.stats()["queued"] > 0:  # every request prepared, so all join the first batch step
             e.step(0)
         e.step(1)
         st = e.stats()
-        # stage-1 tiles (8 rows) of every solve plus the mixed solves' 16-row FP32 tiles
-        assert st["running"] == n and st["tiles"] == (n // 4) * (4 + 12 + 4 + 12 + 2 + 6)
+        assert st["running"] == n and st["tiles"] == sum(tiles[k] for k in kind)
         e.run_all()
         for i, rid in enumerate(ids):
             t, h, d = e.result(rid)
-            t0, h0, d0 = alone[i % 4]
+            t0, h0, d0 = alone[kind[i]]
             assert np.array_equal(t, t0) and np.array_equal(h, h0) and np.array_equal(d, d0), i
 
 
